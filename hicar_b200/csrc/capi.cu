@@ -1,0 +1,952 @@
+// capi.cu -- the C ABI of include/hicarw.h: per-nest handle, control flow of
+// calc_iter_winds (wind_iterative.F90:295-532), probing (:1096-1248,
+// wind.F90:1010-1099) and the device-driven BiCGStab loop.
+//
+// The loop: one CUDA graph holds `check_every` BiCGStab iterations (the kernel
+// schedule of k_krylov.cu, or the fused schedule of k_fused.cu).  The host
+// replays it and, one graph behind, reads the device-side `stop` flag through
+// pinned memory, so the GPU never waits for the host inside a solve.  Kernels
+// of an ended solve return immediately.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/hicarw.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "fused.h"
+
+using namespace hw;
+
+namespace hw {
+static std::atomic<long long> g_launches{0};
+static thread_local int g_capturing = 0;
+static thread_local int g_capture_nodes = 0;
+void count_launch(int n)
+{
+    if (g_capturing) g_capture_nodes += n;
+    else g_launches += n;
+}
+}  // namespace hw
+
+#define CK(call)                                                                                                       \
+    do {                                                                                                               \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess) {                                                                                       \
+            set_err(h, #call, e_);                                                                                     \
+            return HICARW_ERR_CUDA;                                                                                    \
+        }                                                                                                              \
+    } while (0)
+
+static thread_local std::string g_err_noh;
+
+struct GraphKey {
+    int prec, sweeps, chunk, solver, replace;
+    bool operator<(const GraphKey &o) const
+    {
+        if (prec != o.prec) return prec < o.prec;
+        if (sweeps != o.sweeps) return sweeps < o.sweeps;
+        if (chunk != o.chunk) return chunk < o.chunk;
+        if (solver != o.solver) return solver < o.solver;
+        return replace < o.replace;
+    }
+};
+struct GraphRec {
+    cudaGraphExec_t exec;
+    int nodes;
+};
+
+enum { V_X = 0, V_R, V_RHAT, V_P, V_PHAT, V_V, V_S, V_SHAT, V_T, V_RHS, V_DINV, V_PRES, NVEC };
+
+struct hicarw_handle {
+    Dims d;
+    hicarw_options opt;
+    int nest = 1;
+    cudaStream_t cap = nullptr;
+    // metric fields, caller layout
+    float *mjac = nullptr, *mju = nullptr, *mjv = nullptr, *mjw = nullptr, *mdzdx = nullptr, *mdzdy = nullptr,
+          *mdzdx_u = nullptr, *mdzdy_v = nullptr, *madz = nullptr, *mnterr = nullptr;
+    float *mf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float *dz_if = nullptr, *dzdx_surf = nullptr, *dzdy_surf = nullptr, *adz_col = nullptr;
+    float *alpha = nullptr, *div = nullptr;
+    float *coef = nullptr;
+    BcCol *bc = nullptr;
+    int vprec = -1; // precision of the allocated Krylov vectors
+    void *vec[NVEC] = {};
+    SolveState *st = nullptr;
+    SolveState *hst = nullptr; // pinned host mirror
+    int *hflag = nullptr;      // pinned stop flags (2 slots)
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    double *hist = nullptr;
+    int hist_cap = 0;
+    double *partials = nullptr;
+    int red_blocks = 0;
+    unsigned int *scan = nullptr; // nan count, alpha min, alpha max, probe leak
+    unsigned int *hscan = nullptr;
+    // staging for host pointers
+    float *su = nullptr, *sv = nullptr, *sw = nullptr, *sT = nullptr, *srho = nullptr, *sdiv = nullptr;
+    float *sprobe_u = nullptr, *sprobe_v = nullptr, *sprobe_w = nullptr;
+    int structure_uploaded = 0, operator_probed = 0, precond_n_sweeps = 2;
+    std::map<GraphKey, GraphRec> graphs;
+    FusedBufs fb;
+    std::string err;
+    long long launches_at_call = 0;
+};
+
+static void set_err(hicarw_handle *h, const char *what, cudaError_t e)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    if (h) h->err = buf;
+    else g_err_noh = buf;
+}
+
+static const int BASE_PREC_SWEEPS = 2; // wind_iterative.F90:75
+static const int MAX_PREC_SWEEPS = 4;  // wind_iterative.F90:76
+
+extern "C" void hicarw_default_options(hicarw_options *o)
+{
+    memset(o, 0, sizeof(*o));
+    o->max_iters = 1500;
+    o->verbose = 0;
+    o->tol_rel = 1.0e-5;
+    o->tol_abs = 1.0e-10;
+    o->krylov_precision = HICARW_KRYLOV_F64;
+    o->solver = HICARW_SOLVER_REFERENCE;
+    o->criterion = HICARW_CRIT_RECURRENCE;
+    o->replace_every = 50;
+    o->check_every = 8;
+}
+
+static Metrics metrics_of(const hicarw_handle *h)
+{
+    Metrics m;
+    m.jac = h->mjac; m.ju = h->mju; m.jv = h->mjv; m.jw = h->mjw; m.dzdx = h->mdzdx; m.dzdy = h->mdzdy;
+    m.dzdx_u = h->mdzdx_u; m.dzdy_v = h->mdzdy_v; m.adz = h->madz; m.nterr = h->mnterr;
+    m.mf_mx_u = h->mf[0]; m.mf_my_v = h->mf[1]; m.mf_my_u = h->mf[2]; m.mf_mx_v = h->mf[3]; m.mf_mxy = h->mf[4];
+    m.dz_if = h->dz_if; m.dzdx_surf = h->dzdx_surf; m.dzdy_surf = h->dzdy_surf; m.adz_col = h->adz_col;
+    return m;
+}
+
+static OpCtx opctx(const hicarw_handle *h)
+{
+    OpCtx c;
+    c.d = h->d;
+    c.coef = h->coef;
+    c.bc = h->bc;
+    c.probed = h->operator_probed;
+    return c;
+}
+
+static size_t n_cell(const Dims &d) { return (size_t)d.nx * d.nz * d.ny; }
+static size_t n_u(const Dims &d) { return (size_t)(d.nx + 1) * d.nz * d.ny; }
+static size_t n_v(const Dims &d) { return (size_t)d.nx * d.nz * (d.ny + 1); }
+
+static cudaError_t dalloc(void **p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    return e;
+}
+
+static int ensure_vectors(hicarw_handle *h, int prec)
+{
+    const Dims &d = h->d;
+    if (h->vprec == prec) return 0;
+    size_t es = prec == HICARW_KRYLOV_F64 ? 8 : 4;
+    void *nv[NVEC] = {};
+    for (int q = 0; q < NVEC; q++) CK(dalloc(&nv[q], (size_t)d.npad * es));
+    if (h->vprec >= 0) { // carry the warm-start lambda across a precision change
+        if (prec == HICARW_KRYLOV_F64) launch_convert<float, double>(d.npad, (const float *)h->vec[V_X], (double *)nv[V_X], 0);
+        else launch_convert<double, float>(d.npad, (const double *)h->vec[V_X], (float *)nv[V_X], 0);
+        CK(cudaDeviceSynchronize());
+        for (int q = 0; q < NVEC; q++) cudaFree(h->vec[q]);
+    }
+    for (int q = 0; q < NVEC; q++) h->vec[q] = nv[q];
+    h->vprec = prec;
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    return 0;
+}
+
+template <typename T>
+static T *V(hicarw_handle *h, int q) { return (T *)h->vec[q]; }
+
+// Stage a caller array to the device when it lives in host memory.
+static int stage_in(hicarw_handle *h, const float *src, float **buf, size_t n, int mem_kind, cudaStream_t s,
+                    const float **out)
+{
+    if (mem_kind == HICARW_MEM_DEVICE || src == nullptr) { *out = src; return 0; }
+    if (!*buf) CK(cudaMalloc((void **)buf, n * sizeof(float)));
+    CK(cudaMemcpyAsync(*buf, src, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    *out = *buf;
+    return 0;
+}
+
+extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options *opt, const hicarw_metrics *m,
+                                      int mem_kind, void *stream, hicarw_handle **out)
+{
+    if (!g || !m || !out || g->nx < 3 || g->ny < 3 || g->nz < 2 || !(g->dx > 0.0f)) return HICARW_ERR_ARG;
+    hicarw_handle *h = new hicarw_handle();
+    Dims &d = h->d;
+    d.nx = g->nx; d.ny = g->ny; d.nz = g->nz;
+    d.mx = d.nx + 2; d.my = d.ny + 2; d.mz = d.nz + 2;
+    d.P = ((d.nx + 1 + XO + 1) + 7) / 8 * 8;
+    d.plane = (long long)d.P * d.mz;
+    d.npad = d.plane * d.my;
+    d.dx = g->dx;
+    h->nest = g->nest;
+    if (opt) h->opt = *opt;
+    else hicarw_default_options(&h->opt);
+    if (h->opt.check_every <= 0) h->opt.check_every = 8;
+    if (h->opt.replace_every <= 0) h->opt.replace_every = 50;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = 0;
+#define ALLOC(p, n) do { cudaError_t e_ = dalloc((void **)&(p), (n)); if (e_ != cudaSuccess) { set_err(h, "cudaMalloc", e_); hicarw_finalize_iter_winds(h); return HICARW_ERR_CUDA; } } while (0)
+    ALLOC(h->mjac, n_cell(d) * 4); ALLOC(h->mju, n_u(d) * 4); ALLOC(h->mjv, n_v(d) * 4); ALLOC(h->mjw, n_cell(d) * 4);
+    ALLOC(h->mdzdx, n_cell(d) * 4); ALLOC(h->mdzdy, n_cell(d) * 4); ALLOC(h->mdzdx_u, n_u(d) * 4);
+    ALLOC(h->mdzdy_v, n_v(d) * 4); ALLOC(h->madz, n_cell(d) * 4); ALLOC(h->mnterr, (size_t)d.nx * d.ny * 4);
+    ALLOC(h->mf[0], (size_t)(d.nx + 1) * d.ny * 4); ALLOC(h->mf[1], (size_t)d.nx * (d.ny + 1) * 4);
+    ALLOC(h->mf[2], (size_t)(d.nx + 1) * d.ny * 4); ALLOC(h->mf[3], (size_t)d.nx * (d.ny + 1) * 4);
+    ALLOC(h->mf[4], (size_t)d.nx * d.ny * 4);
+    ALLOC(h->dz_if, (size_t)d.nx * (d.nz + 1) * d.ny * 4); ALLOC(h->dzdx_surf, (size_t)d.nx * d.ny * 4);
+    ALLOC(h->dzdy_surf, (size_t)d.nx * d.ny * 4); ALLOC(h->adz_col, (size_t)d.nz * 4);
+    ALLOC(h->alpha, n_cell(d) * 4); ALLOC(h->div, n_cell(d) * 4);
+    ALLOC(h->coef, (size_t)NCOEF * d.npad * 4);
+    ALLOC(h->bc, (size_t)d.mx * d.my * sizeof(BcCol));
+    ALLOC(h->st, sizeof(SolveState));
+    h->red_blocks = 148 * 4;
+    ALLOC(h->partials, (size_t)h->red_blocks * 8 * sizeof(double));
+    ALLOC(h->scan, 8 * sizeof(unsigned int));
+    h->hist_cap = h->opt.max_iters + 2;
+    ALLOC(h->hist, (size_t)h->hist_cap * sizeof(double));
+#undef ALLOC
+    if (cudaMallocHost((void **)&h->hst, sizeof(SolveState)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->hflag, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost((void **)&h->hscan, 8 * sizeof(unsigned int)) != cudaSuccess) {
+        hicarw_finalize_iter_winds(h);
+        return HICARW_ERR_CUDA;
+    }
+    cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&h->ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->ev[1], cudaEventDisableTiming);
+    cudaEventCreate(&h->t0);
+    cudaEventCreate(&h->t1);
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    struct { float *dst; const float *src; size_t n; } cp[] = {
+        {h->mjac, m->jacobian, n_cell(d)}, {h->mju, m->jacobian_u, n_u(d)}, {h->mjv, m->jacobian_v, n_v(d)},
+        {h->mjw, m->jacobian_w, n_cell(d)}, {h->mdzdx, m->dzdx, n_cell(d)}, {h->mdzdy, m->dzdy, n_cell(d)},
+        {h->mdzdx_u, m->dzdx_u, n_u(d)}, {h->mdzdy_v, m->dzdy_v, n_v(d)}, {h->madz, m->advection_dz, n_cell(d)},
+        {h->mnterr, m->neighbor_terrain, (size_t)d.nx * d.ny},
+        {h->mf[0], m->mapfac_mx_u, (size_t)(d.nx + 1) * d.ny}, {h->mf[1], m->mapfac_my_v, (size_t)d.nx * (d.ny + 1)},
+        {h->mf[2], m->mapfac_my_u, (size_t)(d.nx + 1) * d.ny}, {h->mf[3], m->mapfac_mx_v, (size_t)d.nx * (d.ny + 1)},
+        {h->mf[4], m->mapfac_mxy, (size_t)d.nx * d.ny}};
+    for (auto &c : cp) {
+        if (!c.src) { h->err = "missing metric field"; hicarw_finalize_iter_winds(h); return HICARW_ERR_ARG; }
+        cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.n * sizeof(float), kind, s);
+        if (e != cudaSuccess) { set_err(h, "metric copy", e); hicarw_finalize_iter_winds(h); return HICARW_ERR_CUDA; }
+    }
+    launch_module_vars(d, h->madz, h->mdzdx, h->mdzdy, h->mnterr, h->dz_if, h->dzdx_surf, h->dzdy_surf, h->adz_col, s);
+    if ((rc = ensure_vectors(h, h->opt.krylov_precision)) != 0) { hicarw_finalize_iter_winds(h); return rc; }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_err(h, "init", e); hicarw_finalize_iter_winds(h); return HICARW_ERR_CUDA; }
+    *out = h;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
+{
+    if (!h) return HICARW_ERR_ARG;
+    cudaDeviceSynchronize();
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    fused_free(h->fb);
+    void *ptrs[] = {h->mjac, h->mju, h->mjv, h->mjw, h->mdzdx, h->mdzdy, h->mdzdx_u, h->mdzdy_v, h->madz, h->mnterr,
+                    h->mf[0], h->mf[1], h->mf[2], h->mf[3], h->mf[4], h->dz_if, h->dzdx_surf, h->dzdy_surf, h->adz_col,
+                    h->alpha, h->div, h->coef, h->bc, h->st, h->hist, h->partials, h->scan, h->su, h->sv, h->sw,
+                    h->sT, h->srho, h->sdiv, h->sprobe_u, h->sprobe_v, h->sprobe_w};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int q = 0; q < NVEC; q++)
+        if (h->vec[q]) cudaFree(h->vec[q]);
+    if (h->hst) cudaFreeHost(h->hst);
+    if (h->hflag) cudaFreeHost(h->hflag);
+    if (h->hscan) cudaFreeHost(h->hscan);
+    for (int q = 0; q < 2; q++)
+        if (h->ev[q]) cudaEventDestroy(h->ev[q]);
+    if (h->t0) cudaEventDestroy(h->t0);
+    if (h->t1) cudaEventDestroy(h->t1);
+    if (h->cap) cudaStreamDestroy(h->cap);
+    delete h;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
+{
+    if (!h || !opt) return HICARW_ERR_ARG;
+    h->opt = *opt;
+    if (h->opt.check_every <= 0) h->opt.check_every = 8;
+    if (h->opt.replace_every <= 0) h->opt.replace_every = 50;
+    if (h->opt.max_iters + 2 > h->hist_cap) {
+        cudaFree(h->hist);
+        h->hist_cap = h->opt.max_iters + 2;
+        CK(dalloc((void **)&h->hist, (size_t)h->hist_cap * sizeof(double)));
+    }
+    int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    int rc = ensure_vectors(h, prec);
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// One BiCGStab iteration, enqueued on stream s (captured into the graphs).
+// ---------------------------------------------------------------------------
+template <typename VT>
+static void enqueue_precond(hicarw_handle *h, const VT *in, VT *out, int sweeps, SolveState *gate, int set_halt,
+                            cudaStream_t s)
+{
+    OpCtx c = opctx(h);
+    VT *Dinv = V<VT>(h, V_DINV), *pres = V<VT>(h, V_PRES);
+    launch_precond_scale<VT>(h->d, in, out, Dinv, gate, set_halt, s);
+    for (int sw = 2; sw <= sweeps; sw++) {
+        launch_spmv<VT>(c, out, pres, gate, s);
+        launch_rich<VT>(h->d, in, out, pres, Dinv, gate, s);
+    }
+}
+
+template <typename VT, typename XT>
+static void enqueue_iteration(hicarw_handle *h, XT *x, int sweeps, cudaStream_t s)
+{
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    SolveState *st = h->st;
+    VT *r = V<VT>(h, V_R), *rhat = V<VT>(h, V_RHAT), *p = V<VT>(h, V_P), *phat = V<VT>(h, V_PHAT), *v = V<VT>(h, V_V),
+       *sv = V<VT>(h, V_S), *shat = V<VT>(h, V_SHAT), *t = V<VT>(h, V_T), *Dinv = V<VT>(h, V_DINV),
+       *pres = V<VT>(h, V_PRES);
+    enqueue_precond<VT>(h, p, phat, sweeps, st, 1, s);                 // :649
+    launch_spmv_sigma<VT>(c, phat, v, rhat, st, rb, s);                // :657-688
+    launch_s_precond<VT>(h->d, r, v, sv, shat, Dinv, st, s);           // :690 + sweep 1 of :695
+    for (int sw = 2; sw <= sweeps; sw++) {
+        launch_spmv<VT>(c, shat, pres, st, s);
+        launch_rich<VT>(h->d, sv, shat, pres, Dinv, st, s);
+    }
+    launch_spmv_dot5<VT>(c, shat, t, sv, rhat, st, h->hist, rb, s);    // :703-750
+    launch_update_xrp<VT, XT>(h->d, x, phat, shat, r, sv, t, p, v, st, s); // :755-783
+}
+
+static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec **out)
+{
+    GraphKey key{prec, sweeps, chunk, h->opt.solver, h->opt.replace_every};
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) { *out = &it->second; return 0; }
+    cudaGraph_t graph;
+    g_capturing = 1;
+    g_capture_nodes = 0;
+    CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+    for (int q = 0; q < chunk; q++) {
+        if (h->opt.solver == HICARW_SOLVER_REFERENCE) {
+            if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), sweeps, h->cap);
+            else enqueue_iteration<float, float>(h, V<float>(h, V_X), sweeps, h->cap);
+        } else {
+            FusedCtx fc = fused_ctx(h);
+            fused_enqueue_iteration(fc, sweeps, h->opt.solver == HICARW_SOLVER_MIXED, h->cap);
+        }
+    }
+    cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+    g_capturing = 0;
+    if (e != cudaSuccess) { set_err(h, "cudaStreamEndCapture", e); return HICARW_ERR_CUDA; }
+    GraphRec rec;
+    rec.nodes = g_capture_nodes;
+    e = cudaGraphInstantiate(&rec.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { set_err(h, "cudaGraphInstantiate", e); return HICARW_ERR_CUDA; }
+    auto res = h->graphs.emplace(key, rec);
+    *out = &res.first->second;
+    return 0;
+}
+
+// Run the BiCGStab loop until the device says stop.  Returns the reference
+// status (0/1/2) in h->hst after the call.
+static int run_loop(hicarw_handle *h, int prec, int sweeps, cudaStream_t s)
+{
+    GraphRec *g = nullptr;
+    int chunk = h->opt.check_every;
+    int rc = get_graph(h, prec, sweeps, chunk, &g);
+    if (rc) return rc;
+    const int max_chunks = (h->opt.max_iters + chunk - 1) / chunk + 2;
+    h->hflag[0] = h->hflag[1] = 0;
+    for (int n = 0; n < max_chunks; n++) {
+        CK(cudaGraphLaunch(g->exec, s));
+        g_launches += g->nodes;
+        CK(cudaMemcpyAsync(&h->hflag[n & 1], &h->st->stop, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(h->ev[n & 1], s));
+        if (n >= 1) {
+            CK(cudaEventSynchronize(h->ev[(n - 1) & 1]));
+            if (h->hflag[(n - 1) & 1]) break;
+        }
+    }
+    return 0;
+}
+
+// The device state after a solve, copied to the pinned mirror.
+static int fetch_state(hicarw_handle *h, cudaStream_t s)
+{
+    CK(cudaMemcpyAsync(h->hst, h->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// bicgstab_solve (:555-791) on the current x / rhs.  Fills st (pinned mirror).
+static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
+{
+    const int solver = h->opt.solver;
+    const int prec = solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    int rc = ensure_vectors(h, prec);
+    if (rc) return rc;
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, s);
+    CK(cudaEventRecord(h->t0, s));
+    if (solver == HICARW_SOLVER_REFERENCE) {
+        if (prec == HICARW_KRYLOV_F64)
+            launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
+                                         V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+        else
+            launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R),
+                                       V<float>(h, V_RHAT), V<float>(h, V_P), h->st, h->hist, rb, s);
+        rc = run_loop(h, prec, sweeps, s);
+        if (rc) return rc;
+    } else {
+        if ((rc = fused_prepare(h->fb, h->d, s)) != 0) { h->err = "fused buffers"; return HICARW_ERR_CUDA; }
+        FusedCtx fc = fused_ctx(h);
+        fused_setup(fc, solver == HICARW_SOLVER_MIXED, s);
+        rc = run_loop(h, prec, sweeps, s);
+        if (rc) return rc;
+        // true-residual stopping rule: restart from the FP64 solution while the
+        // FP64 residual is above target (MIXED only; the iterate is in x64)
+        if (solver == HICARW_SOLVER_MIXED && h->opt.criterion == HICARW_CRIT_TRUE) {
+            for (int rs = 0; rs < 20; rs++) {
+                if ((rc = fetch_state(h, s)) != 0) return rc;
+                if (h->hst->status != 0) break;
+                fused_true_residual(fc, 0, s);
+                if ((rc = fetch_state(h, s)) != 0) return rc;
+                if (h->hst->true_res <= h->hst->target || h->hst->it >= h->opt.max_iters) break;
+                fused_restart(fc, s);
+                rc = run_loop(h, prec, sweeps, s);
+                if (rc) return rc;
+            }
+        }
+    }
+    CK(cudaEventRecord(h->t1, s));
+    // final FP64 true residual of the solution (diagnostic; reference has none)
+    if (solver == HICARW_SOLVER_REFERENCE) {
+        if (prec == HICARW_KRYLOV_F64)
+            launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+        else
+            launch_true_residual<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+    } else {
+        FusedCtx fc = fused_ctx(h);
+        fused_true_residual(fc, 0, s);
+    }
+    return fetch_state(h, s);
+}
+
+static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retries)
+{
+    if (!o) return;
+    const SolveState *st = h->hst;
+    o->status = st->status;
+    o->iterations = st->it;
+    o->sweeps = sweeps;
+    o->retries = retries;
+    o->res0 = st->res0;
+    o->res_final = st->rnorm;
+    o->b_norm = sqrt(st->bnorm2);
+    o->target = st->target;
+    o->true_res = st->true_res;
+    o->replacements = st->replacements;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->t0, h->t1);
+    o->solve_ms = ms;
+    o->launches = (int)(g_launches.load() - h->launches_at_call);
+}
+
+// lambda used by the wind correction: x (REFERENCE) or the FP64 accumulator.
+static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float *u, float *v, float *w, cudaStream_t s)
+{
+    Metrics m = metrics_of(h);
+    if (h->opt.solver == HICARW_SOLVER_REFERENCE) {
+        if (h->vprec == HICARW_KRYLOV_F64) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
+        else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
+    } else {
+        FusedCtx fc = fused_ctx(h);
+        if (h->opt.solver == HICARW_SOLVER_MIXED) launch_winds<double>(h->d, m, fc.x64, h->alpha, rho, u, v, w, adv_den, s);
+        else launch_winds<float>(h->d, m, fc.x, h->alpha, rho, u, v, w, adv_den, s);
+    }
+    return 0;
+}
+
+static int zero_solution(hicarw_handle *h, cudaStream_t s)
+{
+    size_t es = h->vprec == HICARW_KRYLOV_F64 ? 8 : 4;
+    CK(cudaMemsetAsync(h->vec[V_X], 0, (size_t)h->d.npad * es, s));
+    if (h->fb.ready) CK(cudaMemsetAsync(h->fb.x64, 0, (size_t)h->d.npad * 8, s));
+    return 0;
+}
+
+extern "C" int hicarw_reset_solution(hicarw_handle *h, void *stream)
+{
+    if (!h) return HICARW_ERR_ARG;
+    return zero_solution(h, (cudaStream_t)stream);
+}
+
+// extract_diagonal + compute_rhs_3d (:430, :433) for the current state.
+static void prepare_system(hicarw_handle *h, cudaStream_t s)
+{
+    const Dims &d = h->d;
+    if (h->vprec == HICARW_KRYLOV_F64) {
+        launch_diag<double>(d, h->coef, h->dz_if, V<double>(h, V_DINV), h->operator_probed, s);
+        launch_rhs<double>(d, h->div, V<double>(h, V_RHS), s);
+    } else {
+        launch_diag<float>(d, h->coef, h->dz_if, V<float>(h, V_DINV), h->operator_probed, s);
+        launch_rhs<float>(d, h->div, V<float>(h, V_RHS), s);
+    }
+}
+
+extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, const float *div, const float *density,
+                                      int adv_den, float *u, float *v, float *w, int mem_kind, void *stream,
+                                      hicarw_stats *stats)
+{
+    if (!h || !alpha || !div || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    h->launches_at_call = g_launches.load();
+    int rc;
+    const int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    if ((rc = ensure_vectors(h, prec)) != 0) return rc;
+    // module copies of alpha and div (:308-317)
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(h->alpha, alpha, n_cell(d) * 4, kind, s));
+    CK(cudaMemcpyAsync(h->div, div, n_cell(d) * 4, kind, s));
+    const float *rho = nullptr, *du = nullptr, *dv = nullptr, *dw = nullptr;
+    if (adv_den && (rc = stage_in(h, density, &h->srho, n_cell(d), mem_kind, s, &rho)) != 0) return rc;
+    if ((rc = stage_in(h, u, &h->su, n_u(d), mem_kind, s, &du)) != 0) return rc;
+    if ((rc = stage_in(h, v, &h->sv, n_v(d), mem_kind, s, &dv)) != 0) return rc;
+    if ((rc = stage_in(h, w, &h->sw, n_cell(d), mem_kind, s, &dw)) != 0) return rc;
+    // NaN scan of div and alpha min/max (:319-329, :411-421): one pass, read back once
+    CK(cudaMemsetAsync(h->scan, 0, 3 * sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(h->scan + 1, 0xff, sizeof(unsigned int), s));
+    launch_scan_inputs((long long)n_cell(d), h->div, h->alpha, h->scan, s);
+    CK(cudaMemcpyAsync(h->hscan, h->scan, 3 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    if (!h->structure_uploaded) { // first call: analytic coefficients (:351-407)
+        launch_coefs(d, metrics_of(h), h->alpha, h->coef, 0, s);
+        launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
+        if ((rc = zero_solution(h, s)) != 0) return rc;
+        h->structure_uploaded = 1;
+        CK(cudaStreamSynchronize(s));
+    } else {
+        CK(cudaStreamSynchronize(s));
+        unsigned int bmn = h->hscan[1], bmx = h->hscan[2];
+        if (bmx > bmn && !h->operator_probed) { // varying alpha -> update_coefs_gpu (:423-426)
+            launch_coefs(d, metrics_of(h), h->alpha, h->coef, 1, s);
+            launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
+        }
+    }
+    if (h->hscan[0] > 0 && h->opt.verbose)
+        fprintf(stderr, "HICAR wind solver: NaN in input divergence (count=%u)\n", h->hscan[0]);
+    prepare_system(h, s);
+    int sweeps = h->precond_n_sweeps;
+    if ((rc = bicgstab_solve(h, sweeps, s)) != 0) return rc;
+    int retries = 0;
+    double res0 = h->hst->res0, resf = h->hst->rnorm;
+    int status = h->hst->status, iters = h->hst->it;
+    if (h->opt.verbose)
+        fprintf(stderr, " HICAR BiCGStab status=%d iterations=%d precond_n_sweeps=%d res0=%g res_final=%g\n", status,
+                iters, sweeps, res0, resf);
+    // adaptive sweep retry (:479-503)
+    if (status != 0 && iters > 0 && resf > 0.01 * res0) {
+        while (status != 0 && resf > 0.01 * res0 && h->precond_n_sweeps < MAX_PREC_SWEEPS) {
+            h->precond_n_sweeps++;
+            sweeps = h->precond_n_sweeps;
+            if ((rc = zero_solution(h, s)) != 0) return rc;
+            if ((rc = bicgstab_solve(h, sweeps, s)) != 0) return rc;
+            retries++;
+            res0 = h->hst->res0; resf = h->hst->rnorm; status = h->hst->status; iters = h->hst->it;
+            if (h->opt.verbose)
+                fprintf(stderr, "  Retry status=%d iterations=%d sweeps=%d\n", status, iters, sweeps);
+        }
+        h->precond_n_sweeps = BASE_PREC_SWEEPS;
+        if (status != 0 && resf > res0) { // the reference stops the model here (:506-528)
+            fill_stats(h, stats, sweeps, retries);
+            h->err = "BiCGStab diverged after every preconditioner retry";
+            return HICARW_ERR_DIVERGED;
+        }
+    }
+    enqueue_winds(h, rho, adv_den, (float *)du, (float *)dv, (float *)dw, s); // :531
+    if (mem_kind == HICARW_MEM_HOST) {
+        CK(cudaMemcpyAsync(u, du, n_u(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(v, dv, n_v(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(w, dw, n_cell(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    fill_stats(h, stats, sweeps, retries);
+    return status;
+}
+
+extern "C" int hicarw_calc_divergence(hicarw_handle *h, const float *u, const float *v, const float *w,
+                                      const float *density, float *div, int adv_den, int horz_only, int use_dqdt,
+                                      int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !w || !div || (adv_den && !density)) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    const float *du, *dv, *dw, *rho = nullptr;
+    int rc;
+    if ((rc = stage_in(h, u, &h->su, n_u(d), mem_kind, s, &du)) != 0) return rc;
+    if ((rc = stage_in(h, v, &h->sv, n_v(d), mem_kind, s, &dv)) != 0) return rc;
+    if ((rc = stage_in(h, w, &h->sw, n_cell(d), mem_kind, s, &dw)) != 0) return rc;
+    if (adv_den && (rc = stage_in(h, density, &h->srho, n_cell(d), mem_kind, s, &rho)) != 0) return rc;
+    float *ddiv = div;
+    if (mem_kind == HICARW_MEM_HOST) {
+        if (!h->sdiv) CK(cudaMalloc((void **)&h->sdiv, n_cell(d) * 4));
+        ddiv = h->sdiv;
+    }
+    launch_divergence(d, metrics_of(h), du, dv, dw, rho, ddiv, adv_den, horz_only, use_dqdt, s);
+    if (mem_kind == HICARW_MEM_HOST) {
+        CK(cudaMemcpyAsync(div, ddiv, n_cell(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    return HICARW_OK;
+}
+
+// ---- probing -------------------------------------------------------------
+extern "C" int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int cc, void *stream)
+{
+    if (!h || ca < 0 || ca > 2 || cb < 0 || cb > 2 || cc < 0 || cc > 2) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (h->vprec == HICARW_KRYLOV_F64) launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
+    else launch_probe_pattern<float>(h->d, V<float>(h, V_X), ca, cb, cc, s);
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_probe_zero_corrections(hicarw_handle *h, float *u, float *v, float *w, int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !w) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    if (mem_kind == HICARW_MEM_HOST) {
+        memset(u, 0, n_u(d) * 4); memset(v, 0, n_v(d) * 4); memset(w, 0, n_cell(d) * 4);
+        return HICARW_OK;
+    }
+    CK(cudaMemsetAsync(u, 0, n_u(d) * 4, s));
+    CK(cudaMemsetAsync(v, 0, n_v(d) * 4, s));
+    CK(cudaMemsetAsync(w, 0, n_cell(d) * 4, s));
+    return HICARW_OK;
+}
+
+// calc_updated_winds from the current x_sol (probe_apply_corrections, :1158-1163).
+extern "C" int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alpha, const float *density, int adv_den,
+                                              float *u, float *v, float *w, int mem_kind, void *stream)
+{
+    if (!h || !alpha || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(h->alpha, alpha, n_cell(d) * 4, kind, s));
+    const float *rho = nullptr, *du, *dv, *dw;
+    int rc;
+    if (adv_den && (rc = stage_in(h, density, &h->srho, n_cell(d), mem_kind, s, &rho)) != 0) return rc;
+    if ((rc = stage_in(h, u, &h->su, n_u(d), mem_kind, s, &du)) != 0) return rc;
+    if ((rc = stage_in(h, v, &h->sv, n_v(d), mem_kind, s, &dv)) != 0) return rc;
+    if ((rc = stage_in(h, w, &h->sw, n_cell(d), mem_kind, s, &dw)) != 0) return rc;
+    Metrics m = metrics_of(h);
+    if (h->vprec == HICARW_KRYLOV_F64) launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
+    else launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
+    if (mem_kind == HICARW_MEM_HOST) {
+        CK(cudaMemcpyAsync(u, du, n_u(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(v, dv, n_v(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(w, dw, n_cell(d) * 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_probe_record(hicarw_handle *h, const float *Tfield, int ca, int cb, int cc, float *max_leak,
+                                   int mem_kind, void *stream)
+{
+    if (!h || !Tfield || !max_leak) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float *T;
+    int rc;
+    if ((rc = stage_in(h, Tfield, &h->sT, n_cell(h->d), mem_kind, s, &T)) != 0) return rc;
+    unsigned int bits;
+    memcpy(&bits, max_leak, 4);
+    h->hscan[3] = bits;
+    CK(cudaMemcpyAsync(h->scan + 3, &h->hscan[3], 4, cudaMemcpyHostToDevice, s));
+    launch_probe_record(h->d, T, h->coef, ca, cb, cc, h->scan + 3, s);
+    CK(cudaMemcpyAsync(&h->hscan[3], h->scan + 3, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    memcpy(max_leak, &h->hscan[3], 4);
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_probe_finalize(hicarw_handle *h, float max_leak, void *stream)
+{
+    if (!h) return HICARW_ERR_ARG;
+    h->operator_probed = 1;
+    h->structure_uploaded = 1;
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    if (h->opt.verbose)
+        fprintf(stderr, "Projection operator calibrated by probing (A = 2*D o G); off-stencil leakage max |T| = %g\n",
+                (double)max_leak);
+    return zero_solution(h, (cudaStream_t)stream); // :1243
+}
+
+extern "C" int hicarw_calibrate_projection_operator(hicarw_handle *h, const float *alpha, const float *density,
+                                                    int adv_den, float *u, float *v, float *w, float *max_leak,
+                                                    int mem_kind, void *stream)
+{
+    if (!h || !alpha || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    int rc;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(h->alpha, alpha, n_cell(d) * 4, kind, s));
+    const float *rho = nullptr;
+    if (adv_den && (rc = stage_in(h, density, &h->srho, n_cell(d), mem_kind, s, &rho)) != 0) return rc;
+    // scratch winds (the reference saves u/v/w dqdt, probes in them and restores them;
+    // probing in separate buffers leaves the caller's arrays untouched, same result)
+    if (!h->sprobe_u) {
+        CK(cudaMalloc((void **)&h->sprobe_u, n_u(d) * 4));
+        CK(cudaMalloc((void **)&h->sprobe_v, n_v(d) * 4));
+        CK(cudaMalloc((void **)&h->sprobe_w, n_cell(d) * 4));
+    }
+    if (!h->sT) CK(cudaMalloc((void **)&h->sT, n_cell(d) * 4));
+    if (!h->structure_uploaded) { // the analytic coefficients fill the rows a probe never reaches
+        launch_coefs(d, metrics_of(h), h->alpha, h->coef, 0, s);
+        launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
+        h->structure_uploaded = 1;
+    }
+    CK(cudaMemsetAsync(h->scan + 3, 0, 4, s));
+    Metrics m = metrics_of(h);
+    for (int cc = 0; cc < 3; cc++)
+        for (int cb = 0; cb < 3; cb++)
+            for (int ca = 0; ca < 3; ca++) {
+                if (h->vprec == HICARW_KRYLOV_F64) launch_probe_pattern<double>(d, V<double>(h, V_X), ca, cb, cc, s);
+                else launch_probe_pattern<float>(d, V<float>(h, V_X), ca, cb, cc, s);
+                CK(cudaMemsetAsync(h->sprobe_u, 0, n_u(d) * 4, s));
+                CK(cudaMemsetAsync(h->sprobe_v, 0, n_v(d) * 4, s));
+                CK(cudaMemsetAsync(h->sprobe_w, 0, n_cell(d) * 4, s));
+                if (h->vprec == HICARW_KRYLOV_F64)
+                    launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
+                else
+                    launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
+                launch_divergence(d, m, h->sprobe_u, h->sprobe_v, h->sprobe_w, rho, h->sT, adv_den, 0, 1, s);
+                launch_probe_record(d, h->sT, h->coef, ca, cb, cc, h->scan + 3, s);
+            }
+    CK(cudaMemcpyAsync(&h->hscan[3], h->scan + 3, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float leak;
+    memcpy(&leak, &h->hscan[3], 4);
+    if (max_leak) *max_leak = leak;
+    (void)u; (void)v; (void)w;
+    return hicarw_probe_finalize(h, leak, stream);
+}
+
+// ---- extensions ----------------------------------------------------------
+extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind, void *stream)
+{
+    if (!h || !lambda) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    size_t n = (size_t)d.mx * d.mz * d.my;
+    double *conv = nullptr, *gath = nullptr;
+    CK(cudaMalloc((void **)&conv, (size_t)d.npad * 8));
+    CK(cudaMalloc((void **)&gath, n * 8));
+    const double *src64 = nullptr;
+    if (h->opt.solver == HICARW_SOLVER_MIXED && h->fb.ready) src64 = h->fb.x64;
+    else if (h->vprec == HICARW_KRYLOV_F64) src64 = V<double>(h, V_X);
+    else {
+        launch_convert<float, double>(d.npad, V<float>(h, V_X), conv, s);
+        src64 = conv;
+    }
+    // gather the padded rows into the (nx+2, nz+2, ny+2) Fortran layout
+    cudaError_t e = cudaMemcpy2DAsync(gath, sizeof(double) * d.mx, src64 + XO, sizeof(double) * d.P,
+                                      sizeof(double) * d.mx, (size_t)d.mz * d.my, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lambda, gath, n * 8,
+                            mem_kind == HICARW_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(conv);
+    cudaFree(gath);
+    if (e != cudaSuccess || e2 != cudaSuccess) { set_err(h, "get_lambda", e != cudaSuccess ? e : e2); return HICARW_ERR_CUDA; }
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_get_coefs(hicarw_handle *h, float *coefs, int mem_kind, void *stream)
+{
+    if (!h || !coefs) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    for (int c = 0; c < NCOEF; c++) {
+        // interior rows (1..nx, 1..nz, 1..ny) -> (nx, nz, ny)
+        for (int j = 1; j <= d.ny; j++)
+            CK(cudaMemcpy2DAsync(coefs + (size_t)c * n_cell(d) + (size_t)(j - 1) * d.nx * d.nz, sizeof(float) * d.nx,
+                                 h->coef + (size_t)c * d.npad + kidx(d, 1, 1, j), sizeof(float) * d.P,
+                                 sizeof(float) * d.nx, d.nz, kind, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed, int mem_kind, void *stream)
+{
+    if (!h || !coefs) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int c = 0; c < NCOEF; c++)
+        for (int j = 1; j <= d.ny; j++)
+            CK(cudaMemcpy2DAsync(h->coef + (size_t)c * d.npad + kidx(d, 1, 1, j), sizeof(float) * d.P,
+                                 coefs + (size_t)c * n_cell(d) + (size_t)(j - 1) * d.nx * d.nz, sizeof(float) * d.nx,
+                                 sizeof(float) * d.nx, d.nz, kind, s));
+    h->operator_probed = probed ? 1 : 0;
+    h->structure_uploaded = 1;
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    CK(cudaStreamSynchronize(s));
+    return HICARW_OK;
+}
+
+// Copy a (nx+2, nz+2, ny+2) FP64 array into / out of a padded device vector.
+static int put_padded(hicarw_handle *h, const double *src, double *dst, int mem_kind, cudaStream_t s)
+{
+    const Dims &d = h->d;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpy2DAsync(dst + XO, sizeof(double) * d.P, src, sizeof(double) * d.mx, sizeof(double) * d.mx,
+                         (size_t)d.mz * d.my, kind, s));
+    return 0;
+}
+static int get_padded(hicarw_handle *h, const double *src, double *dst, int mem_kind, cudaStream_t s)
+{
+    const Dims &d = h->d;
+    cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpy2DAsync(dst, sizeof(double) * d.mx, src + XO, sizeof(double) * d.P, sizeof(double) * d.mx,
+                         (size_t)d.mz * d.my, kind, s));
+    return 0;
+}
+
+extern "C" int hicarw_apply_operator(hicarw_handle *h, const double *x, double *y, int mem_kind, void *stream)
+{
+    if (!h || !x || !y) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    double *bx, *by;
+    CK(dalloc((void **)&bx, (size_t)d.npad * 8));
+    CK(dalloc((void **)&by, (size_t)d.npad * 8));
+    int rc = put_padded(h, x, bx, mem_kind, s);
+    if (!rc) {
+        launch_spmv<double>(opctx(h), bx, by, nullptr, s);
+        rc = get_padded(h, by, y, mem_kind, s);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(bx);
+    cudaFree(by);
+    return rc;
+}
+
+extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream)
+{
+    if (!h || !x || !y || sweeps < 1) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    double *bx, *by, *bd, *bp;
+    CK(dalloc((void **)&bx, (size_t)d.npad * 8));
+    CK(dalloc((void **)&by, (size_t)d.npad * 8));
+    CK(dalloc((void **)&bd, (size_t)d.npad * 8));
+    CK(dalloc((void **)&bp, (size_t)d.npad * 8));
+    int rc = put_padded(h, x, bx, mem_kind, s);
+    if (!rc) {
+        launch_diag<double>(d, h->coef, h->dz_if, bd, h->operator_probed, s);
+        OpCtx c = opctx(h);
+        launch_precond_scale<double>(d, bx, by, bd, nullptr, 0, s);
+        for (int sw = 2; sw <= sweeps; sw++) {
+            launch_spmv<double>(c, by, bp, nullptr, s);
+            launch_rich<double>(d, bx, by, bp, bd, nullptr, s);
+        }
+        rc = get_padded(h, by, y, mem_kind, s);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(bx); cudaFree(by); cudaFree(bd); cudaFree(bp);
+    return rc;
+}
+
+extern "C" int hicarw_solve_rhs(hicarw_handle *h, const double *rhs, int mem_kind, void *stream, hicarw_stats *stats)
+{
+    if (!h || !rhs) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Dims &d = h->d;
+    h->launches_at_call = g_launches.load();
+    const int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    int rc = ensure_vectors(h, prec);
+    if (rc) return rc;
+    double *b;
+    CK(dalloc((void **)&b, (size_t)d.npad * 8));
+    rc = put_padded(h, rhs, b, mem_kind, s);
+    if (!rc) {
+        if (h->vprec == HICARW_KRYLOV_F64) {
+            CK(cudaMemcpyAsync(V<double>(h, V_RHS), b, (size_t)d.npad * 8, cudaMemcpyDeviceToDevice, s));
+            launch_diag<double>(d, h->coef, h->dz_if, V<double>(h, V_DINV), h->operator_probed, s);
+        } else {
+            launch_convert<double, float>(d.npad, b, V<float>(h, V_RHS), s);
+            launch_diag<float>(d, h->coef, h->dz_if, V<float>(h, V_DINV), h->operator_probed, s);
+        }
+        rc = bicgstab_solve(h, h->precond_n_sweeps, s);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(b);
+    if (rc) return rc;
+    fill_stats(h, stats, h->precond_n_sweeps, 0);
+    return h->hst->status;
+}
+
+extern "C" int hicarw_get_history(hicarw_handle *h, double *out, int cap)
+{
+    if (!h) return HICARW_ERR_ARG;
+    int n = h->hst->it + 1;
+    if (out && cap > 0) {
+        int m = n < cap ? n : cap;
+        if (cudaMemcpy(out, h->hist, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return HICARW_ERR_CUDA;
+    }
+    return n;
+}
+
+extern "C" const char *hicarw_last_error(hicarw_handle *h) { return h ? h->err.c_str() : g_err_noh.c_str(); }
+
+extern "C" long long hicarw_kernel_launches(void) { return g_launches.load(); }
+
+// ---- pieces shared with the fused schedule ----
+FusedCtx fused_ctx(hicarw_handle *h)
+{
+    FusedCtx c;
+    c.op = opctx(h);
+    c.rb = RedBuf{h->partials, h->red_blocks};
+    c.st = h->st;
+    c.hist = h->hist;
+    c.div = h->div;
+    c.fb = &h->fb;
+    c.x64 = (h->opt.solver == HICARW_SOLVER_MIXED && h->fb.ready) ? h->fb.x64 : nullptr;
+    c.replace_every = h->opt.replace_every;
+    float **slots[] = {&c.x, &c.r, &c.rhat, &c.p, &c.phat, &c.v, &c.s, &c.shat, &c.t, &c.rhs, &c.Dinv, &c.pres};
+    for (int q = 0; q < NVEC; q++) *slots[q] = h->vprec == HICARW_KRYLOV_F32 ? (float *)h->vec[q] : nullptr;
+    return c;
+}

@@ -1,0 +1,405 @@
+// k_krylov.cu -- the 15-point operator, the Jacobi-Richardson preconditioner and
+// the BiCGStab steps of bicgstab_solve (wind_iterative.F90:555-791), templated on
+// the Krylov vector type V (double = reference precision, float = FP32 vectors).
+//
+// Schedule per BiCGStab iteration with n Richardson sweeps (reference order):
+//   precond_scale(p -> p^)  [n-1 x (spmv(p^) ; rich)]   spmv_sigma(p^ -> v, <r^,v>)
+//   s_precond(s = r - a v ; s^ = D^-1 s) [n-1 x (spmv ; rich)]
+//   spmv_dot5(s^ -> t, <t,s> <t,t> <r^,s> <r^,t> <s,s>)   update_xrp(x, r, p)
+// Every reduction is FP64 and single pass: each CTA writes one partial per value,
+// the last CTA to arrive (atomic ticket) adds the partials in CTA order and runs
+// the scalar recurrences of the reference on the device (alpha, omega, beta, the
+// recurrence norm, the stopping and breakdown tests), so an iteration needs no
+// host synchronisation.  Kernels read the `stop`/`halt` flags and return at once
+// when the solve has ended, which lets the host replay a fixed CUDA graph of
+// several iterations and read the flag only once per graph.
+#include "common.cuh"
+#include "kernels.h"
+#include "krylov_dev.cuh"
+
+namespace hw {
+
+static int row_grid(const Dims &d, int cap)
+{
+    long long n = nsegs(d);
+    return (int)(n < cap ? n : cap);
+}
+
+// ---- y = A x ----
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_kernel(OpCtx c, const V *__restrict__ x, V *__restrict__ y,
+                                                    const SolveState *gate)
+{
+    if (gated(gate)) return;
+    const long long n = nsegs(c.d);
+    for (long long s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = seg_of(c.d, s);
+        if (g.ok) y[kidx(c.d, g.i, g.k, g.j)] = (V)spmv_row(c, x, g.i, g.k, g.j);
+    }
+}
+
+template <typename V>
+void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaStream_t st)
+{
+    spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
+    count_launch(1);
+}
+
+// ---- setup: r = b - A x0, r^ = r, p = r, <r^,r>, <r,r>, <b,b> (:585-645) ----
+// X is the type of the solution (FP64 accumulator in the MIXED schedule).
+template <typename V, typename X>
+__global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restrict__ x, const V *__restrict__ rhs,
+                                                     V *__restrict__ r, V *__restrict__ rhat, V *__restrict__ p,
+                                                     SolveState *stt, double *hist, double *partials)
+{
+    double acc[3] = {0.0, 0.0, 0.0};
+    const long long n = nsegs(c.d);
+    for (long long s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = seg_of(c.d, s);
+        if (!g.ok) continue;
+        long long o = kidx(c.d, g.i, g.k, g.j);
+        double bd = (double)rhs[o];
+        V rv = (V)(bd - spmv_row(c, x, g.i, g.k, g.j)); // t = A x0 ; r = 1*b + (-1)*t
+        r[o] = rv;
+        rhat[o] = rv;
+        p[o] = rv;
+        acc[0] += (double)rv * (double)rv; // <r^, r>
+        acc[1] += (double)rv * (double)rv; // <r, r>
+        acc[2] += bd * bd;                 // <b, b>
+    }
+    double tot[3];
+    if (!grid_reduce<3>(acc, partials, &stt->ticket[0], tot)) return;
+    if (threadIdx.x == 0) {
+        stt->rho = tot[0];
+        double rn = sqrt(tot[1]);
+        stt->rnorm = rn;
+        stt->res0 = rn;
+        stt->bnorm2 = tot[2];
+        stt->target = fmax(stt->tol_abs, stt->tol_rel * sqrt(tot[2])); // :633
+        stt->omega = 1.0;
+        stt->alpha = 1.0;
+        stt->it = 0;
+        hist[0] = rn;
+        if (rn <= stt->target) { stt->status = 0; stt->stop = 1; stt->halt = 1; }
+        else if (stt->max_iters <= 0) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
+    }
+}
+
+template <typename V, typename X>
+void launch_setup(const OpCtx &c, const X *x, const V *rhs, V *r, V *rhat, V *p, SolveState *stt, double *hist,
+                  const RedBuf &rb, cudaStream_t st)
+{
+    setup_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r, rhat, p, stt, hist, rb.partials);
+    count_launch(1);
+}
+
+// ---- v = A p^ and sigma = <r^, v> (:657-688) ----
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_sigma_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
+                                                          const V *__restrict__ rhat, SolveState *stt, double *partials)
+{
+    if (gated(stt)) return;
+    double acc[1] = {0.0};
+    const long long n = nsegs(c.d);
+    for (long long s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = seg_of(c.d, s);
+        if (!g.ok) continue;
+        long long o = kidx(c.d, g.i, g.k, g.j);
+        V vv = (V)spmv_row(c, phat, g.i, g.k, g.j);
+        v[o] = vv;
+        acc[0] += (double)rhat[o] * (double)vv;
+    }
+    double tot[1];
+    if (!grid_reduce<1>(acc, partials, &stt->ticket[1], tot)) return;
+    if (threadIdx.x == 0) {
+        double sigma = tot[0];
+        stt->sigma = sigma;
+        stt->it += 1;
+        if (fabs(sigma) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; }
+        else stt->alpha = stt->rho / sigma;
+    }
+}
+
+template <typename V>
+void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, SolveState *stt, const RedBuf &rb,
+                       cudaStream_t st)
+{
+    spmv_sigma_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, phat, v, rhat, stt, rb.partials);
+    count_launch(1);
+}
+
+// ---- t = A s^ and the packed reduction <t,s> <t,t> <r^,s> <r^,t> <s,s> (:703-783) ----
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_dot5_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
+                                                         const V *__restrict__ sv, const V *__restrict__ rhat,
+                                                         SolveState *stt, double *hist, double *partials)
+{
+    if (gated(stt)) return;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const long long n = nsegs(c.d);
+    for (long long s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = seg_of(c.d, s);
+        if (!g.ok) continue;
+        long long o = kidx(c.d, g.i, g.k, g.j);
+        V tv = (V)spmv_row(c, shat, g.i, g.k, g.j);
+        t[o] = tv;
+        double td = (double)tv, sd = (double)sv[o], rd = (double)rhat[o];
+        acc[0] += td * sd;
+        acc[1] += td * td;
+        acc[2] += rd * sd;
+        acc[3] += rd * td;
+        acc[4] += sd * sd;
+    }
+    double tot[5];
+    if (!grid_reduce<5>(acc, partials, &stt->ticket[2], tot)) return;
+    if (threadIdx.x == 0) {
+        double ts = tot[0], tt = tot[1], rs = tot[2], rt = tot[3], ss = tot[4];
+        stt->upd_r = 0;
+        stt->upd_p = 0;
+        if (tt < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; return; } // :737
+        double omega = ts / tt;
+        double rho_new = rs - omega * rt;
+        double rn2 = ss - 2.0 * omega * ts + omega * omega * tt; // :748
+        if (rn2 < 0.0) rn2 = 0.0;
+        double rn = sqrt(rn2);
+        stt->omega = omega;
+        stt->rnorm = rn;
+        hist[stt->it] = rn;
+        if (rn <= stt->target) { stt->status = 0; stt->stop = 1; return; }         // :758 (after x update)
+        if (fabs(omega) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :763
+        stt->upd_r = 1;
+        if (fabs(stt->rho) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :774
+        stt->beta = (rho_new / stt->rho) * (stt->alpha / omega);
+        stt->upd_p = 1;
+        stt->rho = rho_new;
+        if (stt->it >= stt->max_iters) { stt->status = 1; stt->stop = 1; } // loop ends after this iteration
+    }
+}
+
+template <typename V>
+void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *rhat, SolveState *stt, double *hist,
+                      const RedBuf &rb, cudaStream_t st)
+{
+    spmv_dot5_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, shat, t, s, rhat, stt, hist, rb.partials);
+    count_launch(1);
+}
+
+// ---- elementwise kernels over the padded vectors (padding stays zero) ----
+constexpr int EWT = 256;
+static int ew_grid(long long n)
+{
+    long long b = (n + EWT - 1) / EWT;
+    return (int)(b < 148 * 16 ? b : 148 * 16);
+}
+
+// out = D^-1 in (sweep 1 of apply_precond, :1289-1297).  The first kernel of an
+// iteration also converts a pending `stop` into `halt` for the next iteration.
+template <typename V>
+__global__ void precond_scale_kernel(long long n, const V *__restrict__ in, V *__restrict__ out,
+                                     const V *__restrict__ Dinv, SolveState *gate, int set_halt)
+{
+    if (gated(gate)) {
+        if (set_halt && blockIdx.x == 0 && threadIdx.x == 0) gate->halt = 1;
+        return;
+    }
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        out[q] = Dinv[q] * in[q];
+}
+
+template <typename V>
+void launch_precond_scale(const Dims &d, const V *in, V *out, const V *Dinv, SolveState *gate, int set_halt,
+                          cudaStream_t st)
+{
+    precond_scale_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, in, out, Dinv, gate, set_halt);
+    count_launch(1);
+}
+
+// s = r - alpha v (:690) fused with s^ = D^-1 s (sweep 1 of the second apply)
+template <typename V>
+__global__ void s_precond_kernel(long long n, const V *__restrict__ r, const V *__restrict__ v, V *__restrict__ s,
+                                 V *__restrict__ shat, const V *__restrict__ Dinv, const SolveState *stt)
+{
+    if (gated(stt)) return;
+    const double a = stt->alpha;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        V sv = (V)(1.0 * (double)r[q] + (-a) * (double)v[q]);
+        s[q] = sv;
+        shat[q] = Dinv[q] * sv;
+    }
+}
+
+template <typename V>
+void launch_s_precond(const Dims &d, const V *r, const V *v, V *s, V *shat, const V *Dinv, SolveState *stt,
+                      cudaStream_t st)
+{
+    s_precond_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, r, v, s, shat, Dinv, stt);
+    count_launch(1);
+}
+
+// out += D^-1 (in - A out) with pres = A out (sweeps 2..n, :1301-1313)
+template <typename V>
+__global__ void rich_kernel(long long n, const V *__restrict__ in, V *__restrict__ out, const V *__restrict__ pres,
+                            const V *__restrict__ Dinv, const SolveState *gate)
+{
+    if (gated(gate)) return;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        out[q] = out[q] + Dinv[q] * (in[q] - pres[q]);
+}
+
+template <typename V>
+void launch_rich(const Dims &d, const V *in, V *out, const V *pres, const V *Dinv, const SolveState *gate,
+                 cudaStream_t st)
+{
+    rich_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, in, out, pres, Dinv, gate);
+    count_launch(1);
+}
+
+// x += alpha p^ + omega s^ (:755); r = s - omega t (:771); p = r + beta (p - omega v) (:781)
+template <typename V, typename X>
+__global__ void update_xrp_kernel(long long n, X *__restrict__ x, const V *__restrict__ phat, const V *__restrict__ shat,
+                                  V *__restrict__ r, const V *__restrict__ s, const V *__restrict__ t, V *__restrict__ p,
+                                  const V *__restrict__ v, const SolveState *stt)
+{
+    if (*(volatile const int *)&stt->halt) return;
+    const double a = stt->alpha, w = stt->omega, b = stt->beta;
+    const int ur = stt->upd_r, up = stt->upd_p;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        x[q] = (X)((double)x[q] + a * (double)phat[q] + w * (double)shat[q]);
+        if (ur) {
+            V rv = (V)(1.0 * (double)s[q] + (-w) * (double)t[q]);
+            r[q] = rv;
+            if (up) p[q] = (V)((double)rv + b * ((double)p[q] - w * (double)v[q]));
+        }
+    }
+}
+
+template <typename V, typename X>
+void launch_update_xrp(const Dims &d, X *x, const V *phat, const V *shat, V *r, const V *s, const V *t, V *p, const V *v,
+                       const SolveState *stt, cudaStream_t st)
+{
+    update_xrp_kernel<V, X><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, x, phat, shat, r, s, t, p, v, stt);
+    count_launch(1);
+}
+
+__global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs, int max_iters)
+{
+    s->rho = s->alpha = s->omega = s->beta = s->sigma = 0.0;
+    s->rnorm = s->res0 = s->bnorm2 = s->target = 0.0;
+    s->tol_rel = tol_rel;
+    s->tol_abs = tol_abs;
+    s->true_res = -1.0;
+    s->it = 0;
+    s->max_iters = max_iters;
+    s->status = 1;
+    s->stop = 0;
+    s->halt = 0;
+    s->upd_r = s->upd_p = 0;
+    s->replacements = 0;
+    for (int q = 0; q < 8; q++) s->ticket[q] = 0u;
+    s->err = 0;
+}
+
+void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, cudaStream_t st)
+{
+    state_reset_kernel<<<1, 1, 0, st>>>(stt, tol_rel, tol_abs, max_iters);
+    count_launch(1);
+}
+
+// ---- FP64 true residual b - A x.  mode 0: norm only (-> true_res);
+// mode 1: also r_out = (V)(b - A x) and rho = <r^, r_out> (residual replacement);
+// mode 2: restart, r_out = r^ = b - A x, rho = <r, r>, rnorm = ||r||.
+template <typename V, typename X>
+__global__ void __launch_bounds__(ROWT) true_residual_kernel(OpCtx c, const X *__restrict__ x, const V *__restrict__ rhs,
+                                                             V *__restrict__ r_out, V *__restrict__ rhat,
+                                                             SolveState *stt, int mode, double *partials)
+{
+    double acc[2] = {0.0, 0.0};
+    const long long n = nsegs(c.d);
+    for (long long s = blockIdx.x; s < n; s += gridDim.x) {
+        Seg g = seg_of(c.d, s);
+        if (!g.ok) continue;
+        long long o = kidx(c.d, g.i, g.k, g.j);
+        double e = (double)rhs[o] - spmv_row(c, x, g.i, g.k, g.j);
+        acc[0] += e * e;
+        if (mode >= 1) {
+            V ev = (V)e;
+            r_out[o] = ev;
+            if (mode == 2) {
+                rhat[o] = ev;
+                acc[1] += (double)ev * (double)ev;
+            } else acc[1] += (double)rhat[o] * (double)ev;
+        }
+    }
+    double tot[2];
+    if (!grid_reduce<2>(acc, partials, &stt->ticket[3], tot)) return;
+    if (threadIdx.x == 0) {
+        stt->true_res = sqrt(tot[0]);
+        if (mode >= 1) {
+            stt->rho = tot[1];
+            stt->replacements += 1;
+        }
+        if (mode == 2) stt->rnorm = sqrt(tot[0]);
+    }
+}
+
+template <typename V, typename X>
+void launch_true_residual(const OpCtx &c, const X *x, const V *rhs, V *r_out, const V *rhat, SolveState *stt, int mode,
+                          const RedBuf &rb, cudaStream_t st)
+{
+    true_residual_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r_out, const_cast<V *>(rhat), stt, mode, rb.partials);
+    count_launch(1);
+}
+
+template <typename A, typename B>
+__global__ void convert_kernel(long long n, const A *__restrict__ in, B *__restrict__ out)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        out[q] = (B)in[q];
+}
+
+template <typename A, typename B>
+void launch_convert(long long n, const A *in, B *out, cudaStream_t st)
+{
+    convert_kernel<A, B><<<ew_grid(n), EWT, 0, st>>>(n, in, out);
+    count_launch(1);
+}
+
+// ---- explicit instantiations ----
+#define INST_V(V)                                                                                                      \
+    template void launch_spmv<V>(const OpCtx &, const V *, V *, const SolveState *, cudaStream_t);                    \
+    template void launch_precond_scale<V>(const Dims &, const V *, V *, const V *, SolveState *, int, cudaStream_t);  \
+    template void launch_s_precond<V>(const Dims &, const V *, const V *, V *, V *, const V *, SolveState *,          \
+                                      cudaStream_t);                                                                   \
+    template void launch_rich<V>(const Dims &, const V *, V *, const V *, const V *, const SolveState *, cudaStream_t); \
+    template void launch_spmv_sigma<V>(const OpCtx &, const V *, V *, const V *, SolveState *, const RedBuf &,        \
+                                       cudaStream_t);                                                                  \
+    template void launch_spmv_dot5<V>(const OpCtx &, const V *, V *, const V *, const V *, SolveState *, double *,    \
+                                      const RedBuf &, cudaStream_t);
+INST_V(double)
+INST_V(float)
+template void launch_update_xrp<double, double>(const Dims &, double *, const double *, const double *, double *,
+                                                const double *, const double *, double *, const double *,
+                                                const SolveState *, cudaStream_t);
+template void launch_update_xrp<float, float>(const Dims &, float *, const float *, const float *, float *,
+                                              const float *, const float *, float *, const float *, const SolveState *,
+                                              cudaStream_t);
+template void launch_update_xrp<float, double>(const Dims &, double *, const float *, const float *, float *,
+                                               const float *, const float *, float *, const float *, const SolveState *,
+                                               cudaStream_t);
+template void launch_setup<double, double>(const OpCtx &, const double *, const double *, double *, double *,
+                                           double *, SolveState *, double *, const RedBuf &, cudaStream_t);
+template void launch_setup<float, float>(const OpCtx &, const float *, const float *, float *, float *, float *,
+                                         SolveState *, double *, const RedBuf &, cudaStream_t);
+template void launch_setup<float, double>(const OpCtx &, const double *, const float *, float *, float *, float *,
+                                          SolveState *, double *, const RedBuf &, cudaStream_t);
+template void launch_true_residual<double, double>(const OpCtx &, const double *, const double *, double *,
+                                                   const double *, SolveState *, int, const RedBuf &, cudaStream_t);
+template void launch_true_residual<float, float>(const OpCtx &, const float *, const float *, float *, const float *,
+                                                 SolveState *, int, const RedBuf &, cudaStream_t);
+template void launch_true_residual<float, double>(const OpCtx &, const double *, const float *, float *,
+                                                  const float *, SolveState *, int, const RedBuf &, cudaStream_t);
+template void launch_convert<double, float>(long long, const double *, float *, cudaStream_t);
+template void launch_convert<float, double>(long long, const float *, double *, cudaStream_t);
+template void launch_convert<double, double>(long long, const double *, double *, cudaStream_t);
+
+}  // namespace hw

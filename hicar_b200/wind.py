@@ -1,0 +1,80 @@
+"""Host mirror of the solver-facing part of HICAR's ``wind.F90``:
+``calc_divergence`` (wind.F90:250-523), ``calibrate_projection_operator``
+(:1010-1099) and the iterative-winds branch of ``update_winds`` (:765-823).
+All arithmetic runs in the CUDA library; this module only orders the calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _capi
+from . import wind_iterative as wi
+from .domain import DeviceDomain, mem_kind, ptr
+
+_operator_calibrated: dict = {}  # per nest (wind.F90 operator_calibrated)
+
+
+def calc_divergence(div, domain: DeviceDomain, advect_density: bool = True, horz_only: bool = False,
+                    use_dqdt: bool = False) -> None:
+    """div = D(u, v, w) (wind.F90:250-523).  use_dqdt selects the dqdt winds."""
+    h = wi.handle(domain.nest_indx)
+    u, v, w = (domain.u_dqdt, domain.v_dqdt, domain.w_dqdt) if use_dqdt else (domain.u, domain.v, domain.w)
+    if u is None:
+        raise ValueError("data_3d winds are not set on this domain (use_dqdt=False)")
+    rc = _capi.load().hicarw_calc_divergence(h, ptr(u), ptr(v), ptr(w), ptr(domain.density) if advect_density else None,
+                                             ptr(div), int(bool(advect_density)), int(bool(horz_only)),
+                                             int(bool(use_dqdt)), mem_kind(u), wi._stream[0])
+    _capi.check(rc, h)
+
+
+def calibrate_projection_operator(domain: DeviceDomain, options: wi.WindOptions, div=None,
+                                  on_device: bool = True) -> float:
+    """Calibrate A = 2 D o G by the 27-colouring probe (wind.F90:1010-1099).
+
+    on_device=True runs all 27 probes inside the library (no host round trip);
+    on_device=False drives the reference's probe hooks one by one, exactly as
+    wind.F90:1055-1067 does (``div`` is the probe's scratch divergence)."""
+    lib = _capi.load()
+    h = wi.handle(domain.nest_indx)
+    adv = bool(options.advect_density)
+    if on_device:
+        leak = C.c_float(0.0)
+        rc = lib.hicarw_calibrate_projection_operator(h, ptr(domain.wind_alpha), ptr(domain.density) if adv else None,
+                                                      int(adv), ptr(domain.u_dqdt), ptr(domain.v_dqdt),
+                                                      ptr(domain.w_dqdt), C.byref(leak), mem_kind(domain.u_dqdt),
+                                                      wi._stream[0])
+        _capi.check(rc, h)
+        return float(leak.value)
+    saved = [a.clone() if hasattr(a, "clone") else a.copy() for a in (domain.u_dqdt, domain.v_dqdt, domain.w_dqdt)]
+    max_leak = 0.0
+    for cc in range(3):
+        for cb in range(3):
+            for ca in range(3):
+                wi.probe_lambda_pattern(ca, cb, cc)
+                wi.probe_zero_corrections(domain)
+                wi.probe_apply_corrections(domain, adv)
+                calc_divergence(div, domain, advect_density=adv, horz_only=False, use_dqdt=True)
+                max_leak = wi.probe_record(domain, div, ca, cb, cc, max_leak)
+    wi.probe_finalize(max_leak)
+    domain.set_winds(*saved)
+    return max_leak
+
+
+def update_winds_iterative(domain: DeviceDomain, options: wi.WindOptions, div) -> list:
+    """The iterative-winds branch of update_winds (wind.F90:765-823) for a
+    constant alpha already stored in domain.wind_alpha: first update = analytic
+    solve, calibration, polishing solve; later updates = one solve."""
+    nest = domain.nest_indx
+    stats = []
+    calc_divergence(div, domain, horz_only=False, use_dqdt=True)                              # :805
+    stats.append(wi.calc_iter_winds(domain, domain.wind_alpha, div, options.advect_density))  # :807
+    if not _operator_calibrated.get(nest, False):                                             # :813
+        calibrate_projection_operator(domain, options, div)                                   # :814
+        _operator_calibrated[nest] = True
+        calc_divergence(div, domain, horz_only=False, use_dqdt=True)                          # :817
+        stats.append(wi.calc_iter_winds(domain, domain.wind_alpha, div, options.advect_density))
+    return stats
+
+
+def reset() -> None:
+    _operator_calibrated.clear()

@@ -1,0 +1,213 @@
+/*
+ * hicarw.h -- C ABI of the B200 iterative wind solver.
+ *
+ * Drop-in replacement for HICAR's Fortran module `wind_iterative`
+ * (src/physics/wind_iterative.F90).  Each entry point below names the
+ * reference routine it replaces.  The Fortran side binds these functions
+ * with ISO_C_BINDING; every argument is a plain pointer,
+ * an int or a float/double, every array uses the reference's Fortran layout
+ * (i fastest, then k, then j), and every function returns an int status:
+ *
+ *     0  HICARW_OK                 converged / done
+ *     1  HICARW_ITER_CAP           iteration cap reached (reference status 1)
+ *     2  HICARW_BREAKDOWN          BiCGStab breakdown (reference status 2)
+ *     3  HICARW_FELL_BACK          flexible/learned solve fell back to plain BiCGStab
+ *    <0  an error (argument, state, CUDA, or the reference's fatal `stop`);
+ *        the library never aborts the caller.
+ *
+ * Array pointers are device pointers (mem_kind = HICARW_MEM_DEVICE, e.g. an
+ * OpenACC `host_data use_device` region) or host pointers
+ * (HICARW_MEM_HOST: the library stages them through its own device buffers).
+ * Work is ordered on the CUDA stream passed in (NULL = legacy default stream);
+ * entry points return after the work is enqueued unless they hand a result
+ * back to host memory (stats, leakage), in which case they synchronise the stream.
+ *
+ * Threading: one handle per nest; a handle is not thread-safe.
+ *
+ * Array extents at one rank (nx = ide, ny = jde, nz = kde):
+ *   cell     (nx, nz, ny)     alpha, div, density, jacobian, jacobian_w, dzdx,
+ *                             dzdy, advection_dz, w (w%dqdt_3d)
+ *   u-face   (nx+1, nz, ny)   u (u%dqdt_3d), jacobian_u, dzdx_u
+ *   v-face   (nx, nz, ny+1)   v (v%dqdt_3d), jacobian_v, dzdy_v
+ *   2-D      (nx, ny)         neighbor_terrain, mapfac_mxy
+ *            (nx+1, ny)       mapfac_mx_u, mapfac_my_u
+ *            (nx, ny+1)       mapfac_my_v, mapfac_mx_v
+ */
+#ifndef HICARW_H
+#define HICARW_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HICARW_ABI_VERSION 1
+
+enum {
+    HICARW_OK = 0,
+    HICARW_ITER_CAP = 1,
+    HICARW_BREAKDOWN = 2,
+    HICARW_FELL_BACK = 3,
+    HICARW_ERR_ARG = -1,
+    HICARW_ERR_STATE = -2,
+    HICARW_ERR_CUDA = -3,
+    HICARW_ERR_DIVERGED = -4, /* the reference executes `stop` here (wind_iterative.F90:506-528) */
+    HICARW_ERR_NAN = -5,
+    HICARW_ERR_TIMEOUT = -6   /* a bounded device-side wait gave up */
+};
+
+enum { HICARW_MEM_DEVICE = 0, HICARW_MEM_HOST = 1 };
+
+/* Krylov vector precision. */
+enum {
+    HICARW_KRYLOV_F64 = 0, /* reference precision: FP64 vectors, FP64 reductions */
+    HICARW_KRYLOV_F32 = 1  /* FP32 vectors, FP64 reductions */
+};
+
+/* Solve schedule. */
+enum {
+    HICARW_SOLVER_REFERENCE = 0, /* right-preconditioned BiCGStab, reference kernel schedule */
+    HICARW_SOLVER_FUSED = 1,     /* same method, fused FP32 kernels (temporal blocking of the
+                                    Jacobi-Richardson sweeps with the outer matvec) */
+    HICARW_SOLVER_MIXED = 2      /* FUSED + FP64 solution accumulation and periodic FP64
+                                    true-residual replacement (iterative refinement of lambda) */
+};
+
+/* Stopping rule. */
+enum {
+    HICARW_CRIT_RECURRENCE = 0, /* ||s - w t|| <= max(tol_abs, tol_rel ||b||) (wind_iterative.F90:633,758) */
+    HICARW_CRIT_TRUE = 1        /* additionally ||b - A x|| (FP64) <= max(tol_abs, tol_rel ||b||) */
+};
+
+typedef struct hicarw_grid {
+    int nx, ny, nz; /* ide, jde, kde at one rank */
+    float dx;       /* domain%dx */
+    int nest;       /* domain%nest_indx (1..4) */
+} hicarw_grid;
+
+typedef struct hicarw_options {
+    int max_iters;        /* wind%wind_solver_iterations (default 1500) */
+    int verbose;          /* general%debug .or. windtype == kITERATIVE_WINDS */
+    double tol_rel;       /* reference: 1e-5 (wind_iterative.F90:60) */
+    double tol_abs;       /* reference: 1e-10 (wind_iterative.F90:59) */
+    int krylov_precision; /* HICARW_KRYLOV_* */
+    int solver;           /* HICARW_SOLVER_* */
+    int criterion;        /* HICARW_CRIT_* */
+    int replace_every;    /* MIXED: FP64 true-residual replacement period (iterations) */
+    int check_every;      /* iterations between host reads of the device-side stop flag */
+} hicarw_options;
+
+/* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),
+ * wind_iterative.F90:2320-2331 and wind.F90:272-287. */
+typedef struct hicarw_metrics {
+    const float *jacobian, *jacobian_u, *jacobian_v, *jacobian_w;
+    const float *dzdx, *dzdy, *dzdx_u, *dzdy_v;
+    const float *advection_dz;
+    const float *neighbor_terrain;
+    const float *mapfac_mx_u, *mapfac_my_v, *mapfac_my_u, *mapfac_mx_v, *mapfac_mxy;
+} hicarw_metrics;
+
+typedef struct hicarw_stats {
+    int status;        /* 0 converged, 1 iteration cap, 2 breakdown, 3 fell back */
+    int iterations;    /* BiCGStab iterations of the accepted solve */
+    int sweeps;        /* Jacobi-Richardson sweeps of the accepted solve */
+    int retries;       /* adaptive sweep retries (wind_iterative.F90:479-503) */
+    double res0;       /* ||r0|| */
+    double res_final;  /* recurrence norm at exit */
+    double b_norm;     /* ||b|| */
+    double target;     /* max(tol_abs, tol_rel ||b||) */
+    double true_res;   /* ||b - A x|| in FP64 at exit (negative when not computed) */
+    int replacements;  /* FP64 residual replacements (MIXED) */
+    int launches;      /* kernels launched by this call (incl. graph nodes) */
+    double solve_ms;   /* device time of the Krylov solve (CUDA events) */
+} hicarw_stats;
+
+typedef struct hicarw_handle hicarw_handle;
+
+/* Default options: the reference's constants (max_iters 1500, tol 1e-5/1e-10,
+ * FP64 Krylov vectors, reference schedule, recurrence-norm stop). */
+void hicarw_default_options(hicarw_options *opt);
+
+/* init_iter_winds(domain, options)  (wind_iterative.F90:215-287, init_module_vars :2274-2421).
+ * Copies the metric fields to device-resident solver state (one handle per nest,
+ * the analogue of the reference's per-nest cache, :2613-2851). */
+int hicarw_init_iter_winds(const hicarw_grid *grid, const hicarw_options *opt, const hicarw_metrics *m,
+                           int mem_kind, void *stream, hicarw_handle **out);
+
+/* finalize_iter_winds()  (wind_iterative.F90:2142-2267). Frees every device allocation. */
+int hicarw_finalize_iter_winds(hicarw_handle *h);
+
+/* calc_iter_winds(domain, alpha_in, div_in, adv_den)  (wind_iterative.F90:295-532):
+ * first call builds the analytic coefficients (:351-407), later calls refresh them
+ * when alpha varies and the operator is not probed (:408-427); then the diagonal,
+ * the RHS b = -2 div, the warm-started BiCGStab solve with the adaptive sweep retry,
+ * and the lambda -> (u, v, w_grid) correction (calc_updated_winds, :1742-2071)
+ * applied in place to u, v, w (u%dqdt_3d, v%dqdt_3d, w%dqdt_3d).
+ * density is domain%vars_3d(density); it is read only when adv_den != 0. */
+int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, const float *div, const float *density,
+                           int adv_den, float *u, float *v, float *w, int mem_kind, void *stream,
+                           hicarw_stats *stats);
+
+/* calc_divergence(div, domain, advect_density, horz_only, use_dqdt)  (wind.F90:250-523). */
+int hicarw_calc_divergence(hicarw_handle *h, const float *u, const float *v, const float *w,
+                           const float *density, float *div, int adv_den, int horz_only, int use_dqdt,
+                           int mem_kind, void *stream);
+
+/* Probe hooks (wind_iterative.F90:1096-1248), called in this order for each of
+ * the 27 colourings by calibrate_projection_operator (wind.F90:1055-1067). */
+int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int cc, void *stream);               /* :1096-1115 */
+int hicarw_probe_zero_corrections(hicarw_handle *h, float *u, float *v, float *w, int mem_kind,
+                                  void *stream);                                                       /* :1119-1155 */
+int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alpha, const float *density,
+                                   int adv_den, float *u, float *v, float *w, int mem_kind,
+                                   void *stream);                                                      /* :1158-1163 */
+int hicarw_probe_record(hicarw_handle *h, const float *Tfield, int ca, int cb, int cc,
+                        float *max_leak, int mem_kind, void *stream);                                 /* :1169-1231 */
+int hicarw_probe_finalize(hicarw_handle *h, float max_leak, void *stream);                              /* :1235-1248 */
+
+/* calibrate_projection_operator(domain, options, div)  (wind.F90:1010-1099):
+ * all 27 probes on the device, no host round trip; u, v, w are used as scratch
+ * and restored, as the reference does. */
+int hicarw_calibrate_projection_operator(hicarw_handle *h, const float *alpha, const float *density,
+                                         int adv_den, float *u, float *v, float *w, float *max_leak,
+                                         int mem_kind, void *stream);
+
+/* ---- extensions with no entry point of their own in the reference ---- */
+
+/* Reset the warm-start lambda (x_sol) to zero, as probe_finalize does (:1243). */
+int hicarw_reset_solution(hicarw_handle *h, void *stream);
+
+/* Copy lambda (x_sol, FP64, (nx+2, nz+2, ny+2) Fortran layout) to the caller. */
+int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind, void *stream);
+
+/* Copy the 15 stencil coefficients A..O ((nx, nz, ny) each, 15 consecutive arrays). */
+int hicarw_get_coefs(hicarw_handle *h, float *coefs, int mem_kind, void *stream);
+int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed, int mem_kind, void *stream);
+
+/* y = A x over all rows (spmv, wind_iterative.F90:813-1027); x, y FP64 (nx+2, nz+2, ny+2). */
+int hicarw_apply_operator(hicarw_handle *h, const double *x, double *y, int mem_kind, void *stream);
+
+/* y = M^-1 x (apply_precond, wind_iterative.F90:1268-1315) with the current sweep count. */
+int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream);
+
+/* Solve A lambda = rhs for a caller-given right-hand side ((nx+2, nz+2, ny+2), FP64),
+ * starting from the current lambda; used by manufactured-solution tests. */
+int hicarw_solve_rhs(hicarw_handle *h, const double *rhs, int mem_kind, void *stream, hicarw_stats *stats);
+
+/* Change the solve options of an existing handle (precision, schedule, tolerance). */
+int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt);
+
+/* Recurrence residual norm per iteration of the last solve (FP64). Returns the count. */
+int hicarw_get_history(hicarw_handle *h, double *out, int cap);
+
+/* Last CUDA error string of this handle (static storage). */
+const char *hicarw_last_error(hicarw_handle *h);
+
+/* Number of kernels this library has launched since load (graph nodes included). */
+long long hicarw_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HICARW_H */

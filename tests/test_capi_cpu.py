@@ -1,0 +1,41 @@
+"""CPU checks of the C ABI library: it loads, exports every entry point that
+include/hicarw.h declares, and its default options are the reference's
+constants (no compute call: there is no GPU here)."""
+import ctypes as C
+import os
+import re
+
+from hicar_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "hicarw.h")).read()
+    return sorted(set(re.findall(r"\b(hicarw_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(_capi.EXPORTS) == names
+
+
+def test_default_options_are_reference_constants(lib):
+    o = _capi.default_options()
+    assert o.max_iters == 1500            # namelist_utilities.F90:3871-3876
+    assert o.tol_rel == 1.0e-5            # wind_iterative.F90:60
+    assert o.tol_abs == 1.0e-10           # wind_iterative.F90:59
+    assert o.krylov_precision == _capi.KRYLOV_F64
+    assert o.solver == _capi.SOLVER_REFERENCE
+
+
+def test_bad_arguments_are_errors_not_aborts(lib):
+    h = C.c_void_p()
+    g = _capi.Grid(1, 1, 1, 250.0, 1)     # too small: rejected before any CUDA call
+    rc = lib.hicarw_init_iter_winds(C.byref(g), None, None, 0, None, C.byref(h))
+    assert rc == -1
+    assert lib.hicarw_finalize_iter_winds(None) == -1
+    assert lib.hicarw_calc_iter_winds(None, None, None, None, 0, None, None, None, 0, None, None) == -1
