@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Wind solves/s of the B200 iterative wind solver on a seeded synthetic
+terrain case (the 512 x 512 x 48 plain-BiCGStab workload).
+
+One step = one steady-state wind solve of HICAR's update_winds path
+(wind.F90:805-807): calc_divergence of fresh winds, then calc_iter_winds
+(RHS, BiCGStab to 1e-6 relative residual with the probed operator, lambda ->
+u/v/w correction).  The operator is calibrated once before timing, as HICAR
+does on its first wind update; every step starts from lambda = 0 and the same
+input winds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent subdomain per rank (weak scaling, no collective on
+the data path; torch.distributed only for the barrier and the max-over-ranks
+timing).  --impl reference times the CPU restatement of the reference solver
+(the reference itself cannot be compiled here) on a bounded sample of the same
+workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "wind solves/s to 1e-6 rel. residual, learned+mixed vs plain BiCGStab, 1 B200"
+UNIT = "solves/s"
+WORKLOADS = {
+    "plain512": dict(nx=512, ny=512, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    "cpu64": dict(nx=64, ny=64, nz=20, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    # a smaller case whose inputs still exceed L2, for ncu captures
+    "mid256": dict(nx=256, ny=256, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+}
+# BiCGStab iterations the reference method (2-sweep Jacobi-Richardson, FP64
+# Krylov, probed operator, 1e-6 recurrence norm) needs on each workload's
+# seed-1 case, measured with the FP64 reference-schedule solve; the CPU sample
+# extrapolates one solve from these.
+REF_ITERS = {"plain512": 719, "cpu64": 78, "mid256": None}
+# DRAM bytes per launch of the dominant kernel from one ncu capture
+# (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
+TRAFFIC = {}
+TOL = 1.0e-6
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def solver_options(name: str):
+    from hicar_b200 import _capi, wind_iterative as wi
+    presets = {
+        # the reference's method and kernel schedule, FP64 Krylov vectors
+        "plain": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64),
+        # same BiCGStab recurrences, FP32 multigrid V-cycle preconditioner, true-residual stop,
+        # the reference solve as the fallback on a 1%-per-50-iterations stall
+        "mg": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64,
+                   precond=_capi.PRECOND_MG, stall_iters=50),
+    }
+    kw = presets[name]
+    return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (never changes a setting)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_inputs(wl: dict, seed: int):
+    from hicar_b200 import cases
+    return cases.build_case(wl["nx"], wl["ny"], wl["nz"], wl["dx"], wl["n_hills"], seed=seed,
+                            adv_den=wl["adv_den"], alpha=wl["alpha"])
+
+
+# --------------------------------------------------------------------------------------
+# CPU restatement, bounded sample (reference arm, and cpu_baseline of our arm)
+# --------------------------------------------------------------------------------------
+class CpuSample:
+    """The CPU oracle (reference precision, OpenMP over j-planes) on one
+    steady-state solve of `case`, sampled: divergence, RHS/diagonal,
+    `sample_iters` BiCGStab iterations and the lambda -> wind correction are
+    timed in full; the solve time is extrapolated to `ref_iters` iterations.
+    The probed operator is calibrated on the CPU (or handed in) before timing."""
+
+    def __init__(self, case, coefs=None, threads=None):
+        import numpy as np
+        from oracle import oracle as O
+        O.build()
+        if threads:
+            O.set_threads(threads)
+        self.np = np
+        self.case = case
+        self.cores = O.lib("ref").orc_get_threads()
+        self.s = O.OracleSolver(case.domain, "ref")
+        self.s.set_alpha(case.alpha)
+        t = time.perf_counter()
+        if coefs is None:
+            u, v, w = (np.ascontiguousarray(a).copy() for a in (case.u, case.v, case.w))
+            self.s.build_analytic(case.alpha)
+            self.s.calibrate(case.adv_den, u, v, w)
+        else:
+            self.s.set_coefs(coefs, probed=True)
+        self.setup_s = time.perf_counter() - t
+
+    def run(self, ref_iters, sample_iters):
+        np, s, case = self.np, self.s, self.case
+        u, v, w = (np.ascontiguousarray(a).copy() for a in (case.u, case.v, case.w))
+        t0 = time.perf_counter()
+        div = s.divergence(u, v, w, adv_den=True)
+        t1 = time.perf_counter()
+        s.prepare(div)
+        s.set_vec("x", np.zeros((s.ny + 2, s.nz + 2, s.nx + 2)))
+        s.set_tolerance(TOL)
+        t2 = time.perf_counter()
+        s.bicgstab(sample_iters)
+        t3 = time.perf_counter()
+        s.updated_winds(case.adv_den, u, v, w)
+        t4 = time.perf_counter()
+        t_iter = (t3 - t2) / sample_iters
+        t_solve = (t1 - t0) + (t2 - t1) + (t4 - t3) + t_iter * ref_iters
+        return {"value": 1.0 / t_solve, "t_iter_s": t_iter, "t_solve_s": t_solve, "cores": self.cores,
+                "sample": f"divergence + RHS/diagonal + {sample_iters} of {ref_iters} BiCGStab iterations + "
+                          f"lambda->winds timed; solve time extrapolated to {ref_iters} iterations "
+                          f"(the count this method needs on this case)"}
+
+
+def run_reference(args, wl):
+    rank, world, local = dist_setup()
+    if rank != 0:
+        return
+    case = build_inputs(wl, seed=1)
+    cs = CpuSample(case)
+    vals, info = [], None
+    for q in range(args.warmup + args.steps):
+        info = cs.run(args.ref_iters, args.cpu_sample_iters)
+        if q >= args.warmup:
+            vals.append(info["value"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, **wl, "tol_rel": TOL,
+                       "method": "BiCGStab + 2-sweep Jacobi-Richardson, probed operator"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------------------
+def run_ours(args, wl):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from hicar_b200 import _capi, wind, wind_iterative as wi
+    from hicar_b200.domain import DeviceDomain
+
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lib = _capi.load()
+    case = build_inputs(wl, seed=1 + rank)
+    dom = DeviceDomain.from_case(case, f"cuda:{local}")
+    u0, v0, w0 = dom.u_dqdt.clone(), dom.v_dqdt.clone(), dom.w_dqdt.clone()
+    stream = torch.cuda.current_stream()
+    wi.set_stream(stream.cuda_stream)
+    opt0 = wi.WindOptions(advect_density=wl["adv_den"])
+    wi.init_iter_winds(dom, opt0)
+    div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device=f"cuda:{local}")
+    wind.update_winds_iterative(dom, opt0, div)          # analytic solve + calibration + polish (untimed)
+    h = wi.handle(dom.nest_indx)
+    # iterations the reference method needs on this system (for the CPU extrapolation)
+    opt = solver_options("plain")
+    wi.set_options(opt)
+    dom.set_winds(u0, v0, w0)
+    lib.hicarw_reset_solution(h, stream.cuda_stream)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    ref_stats = wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
+    ref_iters = ref_stats["iterations"]
+    opt = solver_options(args.solver)
+    wi.set_options(opt)
+
+    def step():
+        dom.set_winds(u0, v0, w0)
+        lib.hicarw_reset_solution(h, stream.cuda_stream)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        return wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = lib.hicarw_kernel_launches()
+    torch.cuda.synchronize()
+    e0.record()
+    stats = []
+    for q in range(args.steps):
+        if q == 0 and args.ncu_range == "step":
+            torch.cuda.cudart().cudaProfilerStart()
+        stats.append(step())
+        if q == 0 and args.ncu_range == "step":
+            torch.cuda.cudart().cudaProfilerStop()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = lib.hicarw_kernel_launches() - l0
+    clocks = sampler.stop()
+    t_ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([t_ms], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * args.steps / (t_ms / 1000.0)
+
+    # ---- e2e: the same step with host (pinned) winds copied in and out every step ----
+    hu, hv, hw_ = (torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in (u0, v0, w0))
+    for src, dst in ((u0, hu), (v0, hv), (w0, hw_)):
+        dst.copy_(src.cpu())
+    ou, ov, ow = (torch.empty_like(a) for a in (hu, hv, hw_))
+    h2d = sum(a.numel() * 4 for a in (hu, hv, hw_))
+    d2h = h2d
+
+    def e2e_step():
+        dom.u_dqdt.copy_(hu, non_blocking=True)
+        dom.v_dqdt.copy_(hv, non_blocking=True)
+        dom.w_dqdt.copy_(hw_, non_blocking=True)
+        lib.hicarw_reset_solution(h, stream.cuda_stream)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
+        ou.copy_(dom.u_dqdt, non_blocking=True)
+        ov.copy_(dom.v_dqdt, non_blocking=True)
+        ow.copy_(dom.w_dqdt, non_blocking=True)
+        return st
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    te = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([te], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = world * e2e_steps / (te / 1000.0)
+
+    # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
+    cap = 32
+    names = C.create_string_buffer(32 * cap)
+    ms = (C.c_double * cap)()
+    by = (C.c_double * cap)()
+    cnt = (C.c_int * cap)()
+    if args.ncu_range == "profile":
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+    n = lib.hicarw_profile_iteration(h, 5, names, ms, by, cnt, cap, stream.cuda_stream)
+    if args.ncu_range == "profile":
+        torch.cuda.cudart().cudaProfilerStop()
+    prof = []
+    for q in range(max(n, 0)):
+        nm = names.raw[32 * q:32 * q + 32].split(b"\0")[0].decode()
+        prof.append({"kernel": nm, "ms": ms[q], "bytes": by[q], "per_iter": cnt[q], "share_ms": ms[q] * cnt[q]})
+    tot = sum(p["share_ms"] for p in prof) or 1.0
+    dom_k = max(prof, key=lambda p: p["share_ms"]) if prof else None
+    peak, peak_kind = peaks()
+    traffic = TRAFFIC.get(f"{args.workload}:{args.solver}:{dom_k['kernel']}") if dom_k else None
+    roofline = None
+    if dom_k:
+        ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
+                    "share": dom_k["share_ms"] / tot,
+                    "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        coefs = np.empty((15, dom.ny, dom.nz, dom.nx), np.float32)
+        lib.hicarw_get_coefs(h, coefs.ctypes.data, _capi.MEM_HOST, stream.cuda_stream)
+        c = CpuSample(case, coefs=coefs).run(ref_iters, args.cpu_sample_iters)
+        cpu = {"value": c["value"], "unit": UNIT, "cores": c["cores"], "kind": "port", "sample": c["sample"],
+               "t_iter_s": c["t_iter_s"]}
+
+    it = [s["iterations"] for s in stats]
+    tr = [s["true_res"] / s["b_norm"] for s in stats]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {wl['nx']}x{wl['ny']}x{wl['nz']} terrain case, "
+                                   f"{wl['n_hills']} hills, alpha={wl['alpha']}, adv_den={wl['adv_den']}",
+                       "solver": args.solver, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
+                       "iterations": it[0], "ref_method_iterations": ref_iters, "true_res_rel": max(tr),
+                       "l2": "inputs larger than L2 (15 FP32 coefficient arrays, 0.8 GB)",
+                       "parallelism": f"{world} independent subdomains" if world > 1 else "1 GPU"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "clocks": clocks, "gpu_launches": int(launches)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    wi.finalize_iter_winds()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain512", choices=sorted(WORKLOADS))
+    ap.add_argument("--solver", default="plain")
+    ap.add_argument("--cpu-sample-iters", type=int, default=10)
+    ap.add_argument("--ref-iters", type=int, default=None,
+                    help="iterations of the reference method on the workload (reference arm)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ncu-range", default="none", choices=["none", "step", "profile"],
+                    help="bracket the first timed step or the per-kernel profiling pass with "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if args.ref_iters is None:
+            args.ref_iters = REF_ITERS[args.workload]
+        run_reference(args, wl)
+    else:
+        run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

@@ -18,6 +18,7 @@ MEM_DEVICE, MEM_HOST = 0, 1
 KRYLOV_F64, KRYLOV_F32 = 0, 1
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED = 0, 1, 2
 CRIT_RECURRENCE, CRIT_TRUE = 0, 1
+PRECOND_JACOBI, PRECOND_MG = 0, 1
 
 # Every exported symbol of include/hicarw.h (checked by the CPU test suite).
 EXPORTS = [
@@ -26,7 +27,7 @@ EXPORTS = [
     "hicarw_probe_apply_corrections", "hicarw_probe_record", "hicarw_probe_finalize",
     "hicarw_calibrate_projection_operator", "hicarw_reset_solution", "hicarw_get_lambda", "hicarw_get_coefs",
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
-    "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches",
+    "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
 ]
 
 
@@ -37,7 +38,8 @@ class Grid(C.Structure):
 class Options(C.Structure):
     _fields_ = [("max_iters", C.c_int), ("verbose", C.c_int), ("tol_rel", C.c_double), ("tol_abs", C.c_double),
                 ("krylov_precision", C.c_int), ("solver", C.c_int), ("criterion", C.c_int),
-                ("replace_every", C.c_int), ("check_every", C.c_int)]
+                ("replace_every", C.c_int), ("check_every", C.c_int), ("precond", C.c_int),
+                ("stall_iters", C.c_int), ("mg_omega", C.c_float)]
 
 
 METRIC_FIELDS = ["jacobian", "jacobian_u", "jacobian_v", "jacobian_w", "dzdx", "dzdy", "dzdx_u", "dzdy_v",
@@ -53,7 +55,7 @@ class Stats(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("sweeps", C.c_int), ("retries", C.c_int),
                 ("res0", C.c_double), ("res_final", C.c_double), ("b_norm", C.c_double), ("target", C.c_double),
                 ("true_res", C.c_double), ("replacements", C.c_int), ("launches", C.c_int),
-                ("solve_ms", C.c_double)]
+                ("precond", C.c_int), ("solve_ms", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -100,6 +102,7 @@ def load(path: str = LIB_PATH):
         "hicarw_get_history": (ci, [vp, vp, ci]),
         "hicarw_last_error": (C.c_char_p, [vp]),
         "hicarw_kernel_launches": (C.c_longlong, []),
+        "hicarw_profile_iteration": (ci, [vp, ci, vp, vp, vp, vp, ci, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

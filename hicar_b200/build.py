@@ -21,6 +21,7 @@ UNITS = {
     "k_model.cu": ["-fmad=false"],
     "k_krylov.cu": [],
     "k_fused.cu": [],
+    "k_mg.cu": [],
     "capi.cu": [],
 }
 

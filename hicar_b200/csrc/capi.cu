@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "fused.h"
+#include "mg.h"
 
 using namespace hw;
 
@@ -31,6 +32,29 @@ void count_launch(int n)
 {
     if (g_capturing) g_capture_nodes += n;
     else g_launches += n;
+}
+
+struct ProfRec {
+    const char *name;
+    double bytes;
+    cudaEvent_t a, b;
+};
+static thread_local int g_prof_on = 0;
+static thread_local std::vector<ProfRec> g_prof;
+
+ProfScope::ProfScope(const char *name, double bytes, cudaStream_t st) : slot(-1), s(st)
+{
+    if (!g_prof_on || g_capturing) return;
+    ProfRec r{name, bytes, nullptr, nullptr};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, s);
+    g_prof.push_back(r);
+    slot = (int)g_prof.size() - 1;
+}
+ProfScope::~ProfScope()
+{
+    if (slot >= 0) cudaEventRecord(g_prof[slot].b, s);
 }
 }  // namespace hw
 
@@ -46,9 +70,10 @@ void count_launch(int n)
 static thread_local std::string g_err_noh;
 
 struct GraphKey {
-    int prec, sweeps, chunk, solver, replace;
+    int prec, sweeps, chunk, solver, replace, precond;
     bool operator<(const GraphKey &o) const
     {
+        if (precond != o.precond) return precond < o.precond;
         if (prec != o.prec) return prec < o.prec;
         if (sweeps != o.sweeps) return sweeps < o.sweeps;
         if (chunk != o.chunk) return chunk < o.chunk;
@@ -95,6 +120,9 @@ struct hicarw_handle {
     int structure_uploaded = 0, operator_probed = 0, precond_n_sweeps = 2;
     std::map<GraphKey, GraphRec> graphs;
     FusedBufs fb;
+    Mg mg;
+    int mg_dirty = 1;     // coefficients changed since the multigrid hierarchy was built
+    int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
     long long launches_at_call = 0;
 };
@@ -122,6 +150,9 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->criterion = HICARW_CRIT_RECURRENCE;
     o->replace_every = 50;
     o->check_every = 8;
+    o->precond = HICARW_PRECOND_JACOBI;
+    o->stall_iters = 0;
+    o->mg_omega = 0.8f;
 }
 
 static Metrics metrics_of(const hicarw_handle *h)
@@ -221,7 +252,7 @@ extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options
     ALLOC(h->coef, (size_t)NCOEF * d.npad * 4);
     ALLOC(h->bc, (size_t)d.mx * d.my * sizeof(BcCol));
     ALLOC(h->st, sizeof(SolveState));
-    h->red_blocks = 148 * 4;
+    h->red_blocks = 148 * 16;
     ALLOC(h->partials, (size_t)h->red_blocks * 8 * sizeof(double));
     ALLOC(h->scan, 8 * sizeof(unsigned int));
     h->hist_cap = h->opt.max_iters + 2;
@@ -267,6 +298,7 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     fused_free(h->fb);
+    mg_free(h->mg);
     void *ptrs[] = {h->mjac, h->mju, h->mjv, h->mjw, h->mdzdx, h->mdzdy, h->mdzdx_u, h->mdzdy_v, h->madz, h->mnterr,
                     h->mf[0], h->mf[1], h->mf[2], h->mf[3], h->mf[4], h->dz_if, h->dzdx_surf, h->dzdy_surf, h->adz_col,
                     h->alpha, h->div, h->coef, h->bc, h->st, h->hist, h->partials, h->scan, h->su, h->sv, h->sw,
@@ -330,6 +362,16 @@ static void enqueue_iteration(hicarw_handle *h, XT *x, int sweeps, cudaStream_t 
     VT *r = V<VT>(h, V_R), *rhat = V<VT>(h, V_RHAT), *p = V<VT>(h, V_P), *phat = V<VT>(h, V_PHAT), *v = V<VT>(h, V_V),
        *sv = V<VT>(h, V_S), *shat = V<VT>(h, V_SHAT), *t = V<VT>(h, V_T), *Dinv = V<VT>(h, V_DINV),
        *pres = V<VT>(h, V_PRES);
+    if (h->use_mg) { // multigrid-preconditioned BiCGStab (same recurrences, M = V-cycle)
+        launch_iteration_begin(st, s);
+        mg_apply<VT>(h->mg, p, phat, st, s);
+        launch_spmv_sigma<VT>(c, phat, v, rhat, st, rb, s);
+        launch_s_update<VT>(h->d, r, v, sv, st, s);
+        mg_apply<VT>(h->mg, sv, shat, st, s);
+        launch_spmv_dot5<VT>(c, shat, t, sv, rhat, st, h->hist, rb, s);
+        launch_update_xrp<VT, XT>(h->d, x, phat, shat, r, sv, t, p, v, st, s);
+        return;
+    }
     enqueue_precond<VT>(h, p, phat, sweeps, st, 1, s);                 // :649
     launch_spmv_sigma<VT>(c, phat, v, rhat, st, rb, s);                // :657-688
     launch_s_precond<VT>(h->d, r, v, sv, shat, Dinv, st, s);           // :690 + sweep 1 of :695
@@ -343,7 +385,7 @@ static void enqueue_iteration(hicarw_handle *h, XT *x, int sweeps, cudaStream_t 
 
 static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec **out)
 {
-    GraphKey key{prec, sweeps, chunk, h->opt.solver, h->opt.replace_every};
+    GraphKey key{prec, sweeps, chunk, h->opt.solver, h->opt.replace_every, h->use_mg};
     auto it = h->graphs.find(key);
     if (it != h->graphs.end()) { *out = &it->second; return 0; }
     cudaGraph_t graph;
@@ -404,15 +446,24 @@ static int fetch_state(hicarw_handle *h, cudaStream_t s)
 }
 
 // bicgstab_solve (:555-791) on the current x / rhs.  Fills st (pinned mirror).
-static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
+static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allow_mg = 1)
 {
+    int rc;
+    h->use_mg = allow_mg && h->opt.precond == HICARW_PRECOND_MG && h->operator_probed &&
+                h->opt.solver == HICARW_SOLVER_REFERENCE;
+    if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
+        h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+        if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
+        h->mg_dirty = 0;
+    }
     const int solver = h->opt.solver;
     const int prec = solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
-    int rc = ensure_vectors(h, prec);
+    rc = ensure_vectors(h, prec);
     if (rc) return rc;
     OpCtx c = opctx(h);
     RedBuf rb{h->partials, h->red_blocks};
-    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, s);
+    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters,
+                       h->use_mg ? h->opt.stall_iters : 0, s);
     CK(cudaEventRecord(h->t0, s));
     if (solver == HICARW_SOLVER_REFERENCE) {
         if (prec == HICARW_KRYLOV_F64)
@@ -472,6 +523,7 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
     o->target = st->target;
     o->true_res = st->true_res;
     o->replacements = st->replacements;
+    o->precond = h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, h->t0, h->t1);
     o->solve_ms = ms;
@@ -550,6 +602,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
         if ((rc = zero_solution(h, s)) != 0) return rc;
         h->structure_uploaded = 1;
+        h->mg_dirty = 1;
         CK(cudaStreamSynchronize(s));
     } else {
         CK(cudaStreamSynchronize(s));
@@ -557,6 +610,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         if (bmx > bmn && !h->operator_probed) { // varying alpha -> update_coefs_gpu (:423-426)
             launch_coefs(d, metrics_of(h), h->alpha, h->coef, 1, s);
             launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
+            h->mg_dirty = 1;
         }
     }
     if (h->hscan[0] > 0 && h->opt.verbose)
@@ -564,6 +618,15 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
     prepare_system(h, s);
     int sweeps = h->precond_n_sweeps;
     if ((rc = bicgstab_solve(h, sweeps, s)) != 0) return rc;
+    int fell_back = 0;
+    if (h->use_mg && h->hst->status != 0) { // preconditioned solve stalled or failed: the reference solve decides
+        if (h->opt.verbose)
+            fprintf(stderr, " HICAR multigrid BiCGStab status=%d after %d iterations: falling back to Jacobi\n",
+                    h->hst->status, h->hst->it);
+        if ((rc = zero_solution(h, s)) != 0) return rc;
+        if ((rc = bicgstab_solve(h, sweeps, s, 0)) != 0) return rc;
+        fell_back = 1;
+    }
     int retries = 0;
     double res0 = h->hst->res0, resf = h->hst->rnorm;
     int status = h->hst->status, iters = h->hst->it;
@@ -597,6 +660,10 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         CK(cudaStreamSynchronize(s));
     }
     fill_stats(h, stats, sweeps, retries);
+    if (fell_back && status == 0) {
+        if (stats) stats->status = HICARW_FELL_BACK;
+        return HICARW_FELL_BACK;
+    }
     return status;
 }
 
@@ -702,6 +769,7 @@ extern "C" int hicarw_probe_finalize(hicarw_handle *h, float max_leak, void *str
     if (!h) return HICARW_ERR_ARG;
     h->operator_probed = 1;
     h->structure_uploaded = 1;
+    h->mg_dirty = 1;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     if (h->opt.verbose)
@@ -821,6 +889,7 @@ extern "C" int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed
                                  sizeof(float) * d.nx, d.nz, kind, s));
     h->operator_probed = probed ? 1 : 0;
     h->structure_uploaded = 1;
+    h->mg_dirty = 1;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     CK(cudaStreamSynchronize(s));
@@ -866,16 +935,27 @@ extern "C" int hicarw_apply_operator(hicarw_handle *h, const double *x, double *
 
 extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream)
 {
-    if (!h || !x || !y || sweeps < 1) return HICARW_ERR_ARG;
+    if (!h || !x || !y) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
+    if (sweeps <= 0 && !h->operator_probed) return HICARW_ERR_STATE; // the V-cycle needs the probed operator
     double *bx, *by, *bd, *bp;
     CK(dalloc((void **)&bx, (size_t)d.npad * 8));
     CK(dalloc((void **)&by, (size_t)d.npad * 8));
     CK(dalloc((void **)&bd, (size_t)d.npad * 8));
     CK(dalloc((void **)&bp, (size_t)d.npad * 8));
     int rc = put_padded(h, x, bx, mem_kind, s);
-    if (!rc) {
+    if (!rc && sweeps <= 0) {
+        if (h->mg_dirty || !h->mg.ready) {
+            h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+            if (mg_build(h->mg, d, h->coef, s) != 0) rc = HICARW_ERR_CUDA;
+            else h->mg_dirty = 0;
+        }
+        if (!rc) {
+            mg_apply<double>(h->mg, bx, by, nullptr, s);
+            rc = get_padded(h, by, y, mem_kind, s);
+        }
+    } else if (!rc) {
         launch_diag<double>(d, h->coef, h->dz_if, bd, h->operator_probed, s);
         OpCtx c = opctx(h);
         launch_precond_scale<double>(d, bx, by, bd, nullptr, 0, s);
@@ -933,6 +1013,74 @@ extern "C" int hicarw_get_history(hicarw_handle *h, double *out, int cap)
 extern "C" const char *hicarw_last_error(hicarw_handle *h) { return h ? h->err.c_str() : g_err_noh.c_str(); }
 
 extern "C" long long hicarw_kernel_launches(void) { return g_launches.load(); }
+
+// ---- per-kernel profile of one solve iteration ------------------------------
+__global__ void prof_state_kernel(SolveState *s, int on)
+{
+    s->profile = on;
+    s->stop = 0;
+    s->halt = 0;
+    s->upd_r = s->upd_p = 1;
+    s->it = 0;
+}
+
+extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms, double *bytes,
+                                        int *per_iter, int cap, void *stream)
+{
+    if (!h || reps < 1 || cap < 1) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int solver = h->opt.solver;
+    const int prec = solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    int rc = ensure_vectors(h, prec);
+    if (rc) return rc;
+    if (solver != HICARW_SOLVER_REFERENCE && (rc = fused_prepare(h->fb, h->d, s)) != 0) return HICARW_ERR_CUDA;
+    h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed && solver == HICARW_SOLVER_REFERENCE;
+    if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
+        if (mg_build(h->mg, h->d, h->coef, s) != 0) return HICARW_ERR_CUDA;
+        h->mg_dirty = 0;
+    }
+    prof_state_kernel<<<1, 1, 0, s>>>(h->st, 1);
+    CK(cudaStreamSynchronize(s));
+    for (auto &r : g_prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    g_prof.clear();
+    g_prof_on = 1;
+    for (int q = 0; q < reps; q++) {
+        if (solver == HICARW_SOLVER_REFERENCE) {
+            if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, s);
+            else enqueue_iteration<float, float>(h, V<float>(h, V_X), h->precond_n_sweeps, s);
+        } else {
+            FusedCtx fc = fused_ctx(h);
+            fused_enqueue_iteration(fc, h->precond_n_sweeps, solver == HICARW_SOLVER_MIXED, s);
+        }
+    }
+    g_prof_on = 0;
+    prof_state_kernel<<<1, 1, 0, s>>>(h->st, 0);
+    CK(cudaStreamSynchronize(s));
+    // aggregate by kernel name, in first-launch order
+    std::vector<std::string> nm;
+    std::vector<double> tot, by;
+    std::vector<int> cnt;
+    for (auto &r : g_prof) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        size_t q = 0;
+        while (q < nm.size() && nm[q] != r.name) q++;
+        if (q == nm.size()) { nm.push_back(r.name); tot.push_back(0.0); by.push_back(r.bytes); cnt.push_back(0); }
+        tot[q] += t;
+        cnt[q] += 1;
+    }
+    for (auto &r : g_prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    g_prof.clear();
+    int n = (int)nm.size() < cap ? (int)nm.size() : cap;
+    for (int q = 0; q < n; q++) {
+        if (names) { strncpy(names + 32 * q, nm[q].c_str(), 31); names[32 * q + 31] = 0; }
+        if (ms) ms[q] = tot[q] / cnt[q];
+        if (bytes) bytes[q] = by[q];
+        if (per_iter) per_iter[q] = cnt[q] / reps;
+    }
+    // the profiling pass overwrote the Krylov state: restart the next solve cold
+    return zero_solution(h, s) ? HICARW_ERR_CUDA : n;
+}
 
 // ---- pieces shared with the fused schedule ----
 FusedCtx fused_ctx(hicarw_handle *h)

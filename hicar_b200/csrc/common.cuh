@@ -77,7 +77,10 @@ struct SolveState {
     int replacements;
     unsigned int ticket[8];
     int err;        // device-side error flag (bounded waits)
-    int pad_;
+    int profile;    // profiling pass: kernels ignore the stop/halt flags
+    int stall_k;    // stall detector window (0 = off)
+    int best_it;    // iteration of the best recurrence norm so far
+    double best_rn; // best recurrence norm so far
 };
 
 constexpr double BREAKDOWN_EPS = 1.0e-30; // wind_iterative.F90:61

@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(ROWT) spmv_kernel(OpCtx c, const V *__restrict
 template <typename V>
 void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaStream_t st)
 {
+    ProfScope ps_("spmv", coef_bytes(c.d) + rows(c.d) * 2.0 * sizeof(V), st);
     spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     count_launch(1);
 }
@@ -79,6 +80,8 @@ __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restric
         stt->omega = 1.0;
         stt->alpha = 1.0;
         stt->it = 0;
+        stt->best_rn = rn;
+        stt->best_it = 0;
         hist[0] = rn;
         if (rn <= stt->target) { stt->status = 0; stt->stop = 1; stt->halt = 1; }
         else if (stt->max_iters <= 0) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
@@ -89,6 +92,7 @@ template <typename V, typename X>
 void launch_setup(const OpCtx &c, const X *x, const V *rhs, V *r, V *rhat, V *p, SolveState *stt, double *hist,
                   const RedBuf &rb, cudaStream_t st)
 {
+    ProfScope ps_("setup", coef_bytes(c.d) + rows(c.d) * (sizeof(X) + 4.0 * sizeof(V)), st);
     setup_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r, rhat, p, stt, hist, rb.partials);
     count_launch(1);
 }
@@ -124,6 +128,7 @@ template <typename V>
 void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, SolveState *stt, const RedBuf &rb,
                        cudaStream_t st)
 {
+    ProfScope ps_("spmv_sigma", coef_bytes(c.d) + rows(c.d) * 3.0 * sizeof(V), st);
     spmv_sigma_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, phat, v, rhat, stt, rb.partials);
     count_launch(1);
 }
@@ -166,6 +171,10 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_kernel(OpCtx c, const V *__res
         stt->rnorm = rn;
         hist[stt->it] = rn;
         if (rn <= stt->target) { stt->status = 0; stt->stop = 1; return; }         // :758 (after x update)
+        if (stt->stall_k > 0) { // stall detector: no 1% decrease within stall_k iterations
+            if (rn < 0.99 * stt->best_rn) { stt->best_rn = rn; stt->best_it = stt->it; }
+            else if (stt->it - stt->best_it >= stt->stall_k) { stt->status = 4; stt->stop = 1; return; }
+        }
         if (fabs(omega) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :763
         stt->upd_r = 1;
         if (fabs(stt->rho) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :774
@@ -180,6 +189,7 @@ template <typename V>
 void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *rhat, SolveState *stt, double *hist,
                       const RedBuf &rb, cudaStream_t st)
 {
+    ProfScope ps_("spmv_dot5", coef_bytes(c.d) + rows(c.d) * 4.0 * sizeof(V), st);
     spmv_dot5_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, shat, t, s, rhat, stt, hist, rb.partials);
     count_launch(1);
 }
@@ -210,6 +220,7 @@ template <typename V>
 void launch_precond_scale(const Dims &d, const V *in, V *out, const V *Dinv, SolveState *gate, int set_halt,
                           cudaStream_t st)
 {
+    ProfScope ps_("precond_scale", rows(d) * 3.0 * sizeof(V), st);
     precond_scale_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, in, out, Dinv, gate, set_halt);
     count_launch(1);
 }
@@ -232,6 +243,7 @@ template <typename V>
 void launch_s_precond(const Dims &d, const V *r, const V *v, V *s, V *shat, const V *Dinv, SolveState *stt,
                       cudaStream_t st)
 {
+    ProfScope ps_("s_precond", rows(d) * 5.0 * sizeof(V), st);
     s_precond_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, r, v, s, shat, Dinv, stt);
     count_launch(1);
 }
@@ -250,6 +262,7 @@ template <typename V>
 void launch_rich(const Dims &d, const V *in, V *out, const V *pres, const V *Dinv, const SolveState *gate,
                  cudaStream_t st)
 {
+    ProfScope ps_("rich", rows(d) * 5.0 * sizeof(V), st);
     rich_kernel<V><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, in, out, pres, Dinv, gate);
     count_launch(1);
 }
@@ -260,7 +273,7 @@ __global__ void update_xrp_kernel(long long n, X *__restrict__ x, const V *__res
                                   V *__restrict__ r, const V *__restrict__ s, const V *__restrict__ t, V *__restrict__ p,
                                   const V *__restrict__ v, const SolveState *stt)
 {
-    if (*(volatile const int *)&stt->halt) return;
+    if (*(volatile const int *)&stt->halt && !stt->profile) return;
     const double a = stt->alpha, w = stt->omega, b = stt->beta;
     const int ur = stt->upd_r, up = stt->upd_p;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -277,12 +290,29 @@ template <typename V, typename X>
 void launch_update_xrp(const Dims &d, X *x, const V *phat, const V *shat, V *r, const V *s, const V *t, V *p, const V *v,
                        const SolveState *stt, cudaStream_t st)
 {
+    ProfScope ps_("update_xrp", rows(d) * (2.0 * sizeof(X) + 8.0 * sizeof(V)), st);
     update_xrp_kernel<V, X><<<ew_grid(d.npad), EWT, 0, st>>>(d.npad, x, phat, shat, r, s, t, p, v, stt);
     count_launch(1);
 }
 
-__global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs, int max_iters)
+// First node of an iteration in schedules whose first kernel is not
+// precond_scale: a pending stop becomes halt (no x update in later iterations).
+__global__ void iteration_begin_kernel(SolveState *s)
 {
+    if (s->stop && !s->profile) s->halt = 1;
+}
+
+void launch_iteration_begin(SolveState *stt, cudaStream_t st)
+{
+    iteration_begin_kernel<<<1, 1, 0, st>>>(stt);
+    count_launch(1);
+}
+
+__global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs, int max_iters, int stall_k)
+{
+    s->stall_k = stall_k;
+    s->best_it = 0;
+    s->best_rn = 1e300;
     s->rho = s->alpha = s->omega = s->beta = s->sigma = 0.0;
     s->rnorm = s->res0 = s->bnorm2 = s->target = 0.0;
     s->tol_rel = tol_rel;
@@ -297,11 +327,12 @@ __global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs
     s->replacements = 0;
     for (int q = 0; q < 8; q++) s->ticket[q] = 0u;
     s->err = 0;
+    s->profile = 0;
 }
 
-void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, cudaStream_t st)
+void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, int stall_k, cudaStream_t st)
 {
-    state_reset_kernel<<<1, 1, 0, st>>>(stt, tol_rel, tol_abs, max_iters);
+    state_reset_kernel<<<1, 1, 0, st>>>(stt, tol_rel, tol_abs, max_iters, stall_k);
     count_launch(1);
 }
 
@@ -346,6 +377,7 @@ template <typename V, typename X>
 void launch_true_residual(const OpCtx &c, const X *x, const V *rhs, V *r_out, const V *rhat, SolveState *stt, int mode,
                           const RedBuf &rb, cudaStream_t st)
 {
+    ProfScope ps_("true_residual", coef_bytes(c.d) + rows(c.d) * (sizeof(X) + 3.0 * sizeof(V)), st);
     true_residual_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r_out, const_cast<V *>(rhat), stt, mode, rb.partials);
     count_launch(1);
 }

@@ -6,6 +6,16 @@ namespace hw {
 
 void count_launch(int n);
 
+// Per-launch profiling hook: when a profiling pass is active (never during graph
+// capture) each launcher brackets its kernel with CUDA events and records its
+// name and algorithmic bytes (compulsory DRAM traffic of one launch).
+struct ProfScope {
+    ProfScope(const char *name, double bytes, cudaStream_t s);
+    ~ProfScope();
+    int slot;
+    cudaStream_t s;
+};
+
 // k_model.cu
 void launch_divergence(const Dims &d, const Metrics &m, const float *u, const float *v, const float *w,
                        const float *rho, float *div, int adv_den, int horz_only, int use_dqdt, cudaStream_t st);
@@ -62,7 +72,8 @@ void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *
 template <typename V, typename X>
 void launch_update_xrp(const Dims &d, X *x, const V *phat, const V *shat, V *r, const V *s, const V *t, V *p,
                        const V *v, const SolveState *stt, cudaStream_t st);
-void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, cudaStream_t st);
+void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, int stall_k, cudaStream_t st);
+void launch_iteration_begin(SolveState *stt, cudaStream_t st);
 template <typename V, typename X>
 void launch_true_residual(const OpCtx &c, const X *x, const V *rhs, V *r_out, const V *rhat, SolveState *stt,
                           int mode, const RedBuf &rb, cudaStream_t st);

@@ -7,6 +7,11 @@
 
 namespace hw {
 
+// Rows of the system, (nx+2)(nz+2)(ny+2), and compulsory coefficient bytes of
+// one operator application (15 FP32 coefficients per interior row).
+inline double rows(const Dims &d) { return (double)d.mx * d.my * d.mz; }
+inline double coef_bytes(const Dims &d) { return 60.0 * (double)d.nx * d.ny * d.nz; }
+
 constexpr int ROWT = 128; // threads per CTA in the row kernels
 
 // ---- one row of y = A x (spmv, :813-1027), accumulated in FP64 ----
@@ -78,7 +83,7 @@ __device__ __forceinline__ double spmv_row(const OpCtx &c, const V *__restrict__
 
 __device__ __forceinline__ bool gated(const SolveState *s)
 {
-    return s != nullptr && *(volatile const int *)&s->stop;
+    return s != nullptr && *(volatile const int *)&s->stop && !s->profile;
 }
 
 __device__ __forceinline__ double warp_sum(double v)

@@ -1,0 +1,33 @@
+// mg.h -- multigrid V-cycle preconditioner (k_mg.cu).
+#pragma once
+#include "common.cuh"
+
+namespace hw {
+
+constexpr int MG_MAX_LEVELS = 16;
+
+struct MgLevel {
+    Dims d;
+    const float *coef = nullptr; // 15 * npad (level 0: the solver's probed coefficients)
+    float *cp = nullptr;         // Thomas factors of the column tridiagonal
+    float *minv = nullptr;
+    float *r = nullptr;          // level right-hand side (levels >= 1)
+    float *x1 = nullptr;         // pre-smoothed iterate
+    float *x3 = nullptr;         // post-smoothed iterate (levels >= 1)
+};
+
+struct Mg {
+    int nlev = 0;
+    int ready = 0;
+    float omega = 0.8f; // damping of the z-line Jacobi smoother
+    MgLevel lev[MG_MAX_LEVELS];
+};
+
+int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s);
+void mg_free(Mg &mg);
+template <typename V>
+void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStream_t s);
+template <typename V>
+void launch_s_update(const Dims &d, const V *r, const V *v, V *s, const SolveState *stt, cudaStream_t st);
+
+}  // namespace hw

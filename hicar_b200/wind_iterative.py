@@ -48,6 +48,9 @@ class WindOptions:
     criterion: int = _capi.CRIT_RECURRENCE
     replace_every: int = 50
     check_every: int = 8
+    precond: int = _capi.PRECOND_JACOBI
+    stall_iters: int = 0
+    mg_omega: float = 0.8
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -60,6 +63,9 @@ class WindOptions:
         o.criterion = int(self.criterion)
         o.replace_every = int(self.replace_every)
         o.check_every = int(self.check_every)
+        o.precond = int(self.precond)
+        o.stall_iters = int(self.stall_iters)
+        o.mg_omega = float(self.mg_omega)
         return o
 
 

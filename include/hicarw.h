@@ -74,6 +74,13 @@ enum {
                                     true-residual replacement (iterative refinement of lambda) */
 };
 
+/* Preconditioner. */
+enum {
+    HICARW_PRECOND_JACOBI = 0, /* the reference's Block-Jacobi / Jacobi-Richardson sweeps (:1268-1315) */
+    HICARW_PRECOND_MG = 1      /* multigrid V-cycle: z-line Jacobi smoother, 2x2 x-y aggregation,
+                                  Galerkin coarse operators down to one column (probed operator only) */
+};
+
 /* Stopping rule. */
 enum {
     HICARW_CRIT_RECURRENCE = 0, /* ||s - w t|| <= max(tol_abs, tol_rel ||b||) (wind_iterative.F90:633,758) */
@@ -96,6 +103,10 @@ typedef struct hicarw_options {
     int criterion;        /* HICARW_CRIT_* */
     int replace_every;    /* MIXED: FP64 true-residual replacement period (iterations) */
     int check_every;      /* iterations between host reads of the device-side stop flag */
+    int precond;          /* HICARW_PRECOND_* */
+    int stall_iters;      /* stop a preconditioned solve whose residual has not dropped by 1% for
+                             this many iterations and fall back to the reference solve (0 = off) */
+    float mg_omega;       /* damping of the multigrid smoother (default 0.8) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),
@@ -109,7 +120,7 @@ typedef struct hicarw_metrics {
 } hicarw_metrics;
 
 typedef struct hicarw_stats {
-    int status;        /* 0 converged, 1 iteration cap, 2 breakdown, 3 fell back */
+    int status;        /* 0 converged, 1 iteration cap, 2 breakdown, 3 fell back, 4 stalled */
     int iterations;    /* BiCGStab iterations of the accepted solve */
     int sweeps;        /* Jacobi-Richardson sweeps of the accepted solve */
     int retries;       /* adaptive sweep retries (wind_iterative.F90:479-503) */
@@ -120,6 +131,7 @@ typedef struct hicarw_stats {
     double true_res;   /* ||b - A x|| in FP64 at exit (negative when not computed) */
     int replacements;  /* FP64 residual replacements (MIXED) */
     int launches;      /* kernels launched by this call (incl. graph nodes) */
+    int precond;       /* preconditioner of the accepted solve */
     double solve_ms;   /* device time of the Krylov solve (CUDA events) */
 } hicarw_stats;
 
@@ -188,7 +200,9 @@ int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed, int mem_k
 /* y = A x over all rows (spmv, wind_iterative.F90:813-1027); x, y FP64 (nx+2, nz+2, ny+2). */
 int hicarw_apply_operator(hicarw_handle *h, const double *x, double *y, int mem_kind, void *stream);
 
-/* y = M^-1 x (apply_precond, wind_iterative.F90:1268-1315) with the current sweep count. */
+/* y = M^-1 x: sweeps >= 1 applies the reference preconditioner (apply_precond,
+ * wind_iterative.F90:1268-1315) with that many sweeps; sweeps <= 0 applies one
+ * multigrid V-cycle (probed operator only). */
 int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream);
 
 /* Solve A lambda = rhs for a caller-given right-hand side ((nx+2, nz+2, ny+2), FP64),
@@ -200,6 +214,15 @@ int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt);
 
 /* Recurrence residual norm per iteration of the last solve (FP64). Returns the count. */
 int hicarw_get_history(hicarw_handle *h, double *out, int cap);
+
+/* Profile one solve iteration of the current configuration: every kernel of the
+ * iteration is launched on its own `reps` times and timed with CUDA events on
+ * `stream`.  For each distinct kernel (first-launch order, at most cap): its
+ * name (32 bytes each in names), mean duration in ms, algorithmic bytes of one
+ * launch, and launches per iteration.  Returns the number of kernels.  The
+ * solution is reset to zero. */
+int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms, double *bytes, int *per_iter,
+                             int cap, void *stream);
 
 /* Last CUDA error string of this handle (static storage). */
 const char *hicarw_last_error(hicarw_handle *h);

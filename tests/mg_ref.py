@@ -1,0 +1,136 @@
+"""CPU restatement (numpy) of the multigrid V-cycle preconditioner of
+hicar_b200/csrc/k_mg.cu, used by the GPU tests as the checker of that kernel
+set.  The V-cycle has no counterpart in the reference; this restates the same
+algorithm with the same FP32 storage points:
+  * 2x2 x-y aggregation, Galerkin coarse operator (FP64 sums stored in FP32),
+    couplings to cells outside the interior dropped, down to one column;
+  * z-line Jacobi smoother with the column tridiagonal (C, A, B), Thomas
+    factors computed in FP64 and stored in FP32, the forward sweep stored in
+    FP32, damping omega; exact tridiagonal solve on the single-column level.
+Arrays are the interior (ny, nz, nx) blocks; coefficients are (15, ny, nz, nx)
+in the order A..O.
+"""
+import numpy as np
+
+# offsets (dk, dj, di) of A..O
+OFF = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 0, 1), (0, 0, -1), (0, 1, 0), (0, -1, 0), (1, 0, 1), (1, 0, -1),
+       (-1, 0, 1), (-1, 0, -1), (1, 1, 0), (1, -1, 0), (-1, 1, 0), (-1, -1, 0)]
+SLOT = {o: q for q, o in enumerate(OFF)}
+f32 = np.float32
+
+
+def shift(x, dk, dj, di):
+    """y[j, k, i] = x[j+dj, k+dk, i+di], zero outside."""
+    y = np.zeros_like(x)
+    ny, nz, nx = x.shape
+
+    def sl(n, d):
+        return slice(max(0, d), n + min(0, d)), slice(max(0, -d), n - max(0, d))
+
+    (sj, dj2), (sk, dk2), (si, di2) = sl(ny, dj), sl(nz, dk), sl(nx, di)
+    y[dj2, dk2, di2] = x[sj, sk, si]
+    return y
+
+
+def apply(C, x):
+    y = np.zeros(x.shape, np.float64)
+    for q, (dk, dj, di) in enumerate(OFF):
+        y += C[q].astype(np.float64) * shift(x.astype(np.float64), dk, dj, di)
+    return y
+
+
+def coarsen(C):
+    _, ny, nz, nx = C.shape
+    nyc, nxc = (ny + 1) // 2, (nx + 1) // 2
+    Cc = np.zeros((15, nyc, nz, nxc), np.float64)
+    kk = np.arange(nz)
+    for q, (dk, dj, di) in enumerate(OFF):
+        for pj in (0, 1):
+            for pi in (0, 1):
+                sub = C[q][pj::2, :, pi::2].astype(np.float64)
+                jf = np.arange(pj, ny, 2)[:, None, None]
+                if_ = np.arange(pi, nx, 2)[None, None, :]
+                k3 = kk[None, :, None]
+                ok = (jf + dj >= 0) & (jf + dj < ny) & (if_ + di >= 0) & (if_ + di < nx) & \
+                     (k3 + dk >= 0) & (k3 + dk < nz)
+                cdj = (pj + dj) // 2
+                cdi = (pi + di) // 2
+                q2 = SLOT[(dk, cdj, cdi)]
+                Cc[q2, :sub.shape[0], :, :sub.shape[2]] += np.where(ok, sub, 0.0)
+    return Cc.astype(f32)
+
+
+def factors(C):
+    A, B, Cs = C[0].astype(np.float64), C[1].astype(np.float64), C[2].astype(np.float64)
+    nz = A.shape[1]
+    cp = np.zeros(A.shape, np.float64)
+    mi = np.zeros(A.shape, np.float64)
+    cprev = np.zeros(A[:, 0].shape)
+    for k in range(nz):
+        a = Cs[:, k] if k > 0 else 0.0
+        c = B[:, k] if k < nz - 1 else 0.0
+        den = A[:, k] - a * cprev
+        m = 1.0 / den
+        mi[:, k] = m
+        cprev = c * m
+        cp[:, k] = cprev
+    return cp.astype(f32), mi.astype(f32)
+
+
+def smooth(C, cp, mi, r, x2, omega):
+    """out = x2 + omega T^-1 (r - A x2) (x2 None: out = omega T^-1 r)."""
+    res = r.astype(np.float64) - (apply(C, x2) if x2 is not None else 0.0)
+    nz = r.shape[1]
+    dp = np.zeros(r.shape, np.float32)
+    dprev = 0.0
+    for k in range(nz):
+        a = C[2][:, k].astype(np.float64) if k > 0 else 0.0
+        dv = (res[:, k] - a * dprev) * mi[:, k].astype(np.float64)
+        dp[:, k] = dv
+        dprev = dv
+    y = np.zeros(r[:, 0].shape, np.float64)
+    out = np.zeros(r.shape, np.float64)
+    for k in range(nz - 1, -1, -1):
+        y = dp[:, k].astype(np.float64) - cp[:, k].astype(np.float64) * y
+        base = x2[:, k].astype(np.float64) if x2 is not None else 0.0
+        out[:, k] = base + omega * y
+    return out
+
+
+class VCycle:
+    def __init__(self, coefs, omega=0.8):
+        self.omega = omega
+        self.lev = [np.asarray(coefs, f32)]
+        while self.lev[-1].shape[1] > 1 or self.lev[-1].shape[3] > 1:
+            self.lev.append(coarsen(self.lev[-1]))
+        self.fac = [factors(C) for C in self.lev]
+
+    def __call__(self, r0):
+        L = len(self.lev)
+        w = f32(self.omega)
+        rs = [np.asarray(r0, np.float64)]
+        x1 = []
+        for l in range(L - 1):
+            C = self.lev[l]
+            cp, mi = self.fac[l]
+            xa = smooth(C, cp, mi, rs[l], None, float(w)).astype(f32)
+            x1.append(xa)
+            res = rs[l] - apply(C, xa)
+            ny, nz, nx = res.shape
+            rc = np.zeros(((ny + 1) // 2, nz, (nx + 1) // 2))
+            for pj in (0, 1):
+                for pi in (0, 1):
+                    sub = res[pj::2, :, pi::2]
+                    rc[:sub.shape[0], :, :sub.shape[2]] += sub
+            rs.append(rc.astype(f32))
+        cp, mi = self.fac[L - 1]
+        x3 = smooth(self.lev[L - 1], cp, mi, rs[L - 1], None, 1.0).astype(f32)
+        for l in range(L - 2, -1, -1):
+            C = self.lev[l]
+            cp, mi = self.fac[l]
+            up = np.repeat(np.repeat(x3.astype(np.float64), 2, axis=0), 2, axis=2)
+            ny, nz, nx = x1[l].shape
+            x2 = x1[l].astype(np.float64) + up[:ny, :, :nx]
+            out = smooth(C, cp, mi, rs[l], x2, float(w))
+            x3 = out if l == 0 else out.astype(f32)
+        return x3
