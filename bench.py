@@ -39,11 +39,12 @@ WORKLOADS = {
     # a smaller case whose inputs still exceed L2, for ncu captures
     "mid256": dict(nx=256, ny=256, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
 }
-# BiCGStab iterations the reference method (2-sweep Jacobi-Richardson, FP64
+# BiCGStab iterations the CPU restatement (2-sweep Jacobi-Richardson, FP64
 # Krylov, probed operator, 1e-6 recurrence norm) needs on each workload's
-# seed-1 case, measured with the FP64 reference-schedule solve; the CPU sample
-# extrapolates one solve from these.
-REF_ITERS = {"plain512": 719, "cpu64": 78, "mid256": None}
+# seed-1 case, measured by running it to convergence on the host (plain512:
+# 912 iterations, 136 s on 8 cores); the CPU sample extrapolates one solve
+# from these.
+REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
