@@ -28,6 +28,7 @@ EXPORTS = [
     "hicarw_calibrate_projection_operator", "hicarw_reset_solution", "hicarw_get_lambda", "hicarw_get_coefs",
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
     "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
+    "hicarw_residual_norm_noalloc",
 ]
 
 
@@ -103,6 +104,7 @@ def load(path: str = LIB_PATH):
         "hicarw_last_error": (C.c_char_p, [vp]),
         "hicarw_kernel_launches": (C.c_longlong, []),
         "hicarw_profile_iteration": (ci, [vp, ci, vp, vp, vp, vp, ci, vp]),
+        "hicarw_residual_norm_noalloc": (ci, [vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

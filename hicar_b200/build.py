@@ -22,6 +22,7 @@ UNITS = {
     "k_krylov.cu": [],
     "k_fused.cu": [],
     "k_mg.cu": [],
+    "k_noalloc.cu": [],
     "capi.cu": [],
 }
 

@@ -1082,6 +1082,12 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     return zero_solution(h, s) ? HICARW_ERR_CUDA : n;
 }
 
+// ---- accessors for the entry points defined in other files ----
+namespace hw {
+void handle_operator(const hicarw_handle *h, OpCtx *c) { *c = opctx(h); }
+void handle_set_error(hicarw_handle *h, const char *msg) { h->err = msg; }
+}  // namespace hw
+
 // ---- pieces shared with the fused schedule ----
 FusedCtx fused_ctx(hicarw_handle *h)
 {

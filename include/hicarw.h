@@ -224,6 +224,17 @@ int hicarw_get_history(hicarw_handle *h, double *out, int cap);
 int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms, double *bytes, int *per_iter,
                              int cap, void *stream);
 
+/* ||rhs - A x||_2 in FP64 for the handle's current operator, written to the
+ * device double *norm; x and rhs are device arrays in the (nx+2, nz+2, ny+2)
+ * Fortran layout.  This entry point has no counterpart in the reference.  It
+ * allocates nothing, for callers that cannot call cudaMalloc (inside a stream
+ * capture, or in a host model whose device memory is fixed up front): its
+ * scratch is a static device array of 8192 FP64 plane partials, so ny + 2 <=
+ * 8192 (larger grids return HICARW_ERR_ARG).  The first call on a device looks
+ * up that array's address and should come before any stream capture; calls
+ * that overlap on the GPU race on the shared array. */
+int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm, void *stream);
+
 /* Last CUDA error string of this handle (static storage). */
 const char *hicarw_last_error(hicarw_handle *h);
 
