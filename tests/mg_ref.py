@@ -4,9 +4,11 @@ set.  The V-cycle has no counterpart in the reference; this restates the same
 algorithm with the same FP32 storage points:
   * 2x2 x-y aggregation, Galerkin coarse operator (FP64 sums stored in FP32),
     couplings to cells outside the interior dropped, down to one column;
-  * z-line Jacobi smoother with the column tridiagonal (C, A, B), Thomas
-    factors computed in FP64 and stored in FP32, the forward sweep stored in
-    FP32, damping omega; exact tridiagonal solve on the single-column level.
+  * z-line Jacobi smoother with the column tridiagonal (C, A, B): Thomas
+    factors computed in FP64 and stored in FP32, the recurrences in FP32, the
+    residual of the post-smoother summed in FP64 from the FP32 staged iterate
+    x2 = x1 + P xc, damping omega; exact tridiagonal solve on the
+    single-column level (reached by the fused restriction + pre-smoothing).
 Arrays are the interior (ny, nz, nx) blocks; coefficients are (15, ny, nz, nx)
 in the order A..O.
 """
@@ -77,24 +79,33 @@ def factors(C):
     return cp.astype(f32), mi.astype(f32)
 
 
-def smooth(C, cp, mi, r, x2, omega):
-    """out = x2 + omega T^-1 (r - A x2) (x2 None: out = omega T^-1 r)."""
-    res = r.astype(np.float64) - (apply(C, x2) if x2 is not None else 0.0)
-    nz = r.shape[1]
-    dp = np.zeros(r.shape, np.float32)
-    dprev = 0.0
+def thomas32(C, cp, mi, res):
+    """T^-1 res column by column, FP32 recurrences (couplings to ghost planes dropped)."""
+    nz = res.shape[1]
+    d = np.zeros(res.shape, f32)
+    dprev = np.zeros(res[:, 0].shape, f32)
     for k in range(nz):
-        a = C[2][:, k].astype(np.float64) if k > 0 else 0.0
-        dv = (res[:, k] - a * dprev) * mi[:, k].astype(np.float64)
-        dp[:, k] = dv
+        a = C[2][:, k] if k > 0 else f32(0)
+        dv = ((res[:, k] - a * dprev) * mi[:, k]).astype(f32)
+        d[:, k] = dv
         dprev = dv
-    y = np.zeros(r[:, 0].shape, np.float64)
-    out = np.zeros(r.shape, np.float64)
+    y = np.zeros(res[:, 0].shape, f32)
     for k in range(nz - 1, -1, -1):
-        y = dp[:, k].astype(np.float64) - cp[:, k].astype(np.float64) * y
-        base = x2[:, k].astype(np.float64) if x2 is not None else 0.0
-        out[:, k] = base + omega * y
-    return out
+        y = (d[:, k] - cp[:, k] * y).astype(f32)
+        d[:, k] = y
+    return d
+
+
+def pre(C, cp, mi, r, omega):
+    """out = omega T^-1 r (from zero)."""
+    return (f32(omega) * thomas32(C, cp, mi, np.asarray(r).astype(f32))).astype(f32)
+
+
+def post(C, cp, mi, r, x2, omega):
+    """out = x2 + omega T^-1 (r - A x2), x2 given in FP32."""
+    res = (np.asarray(r, np.float64) - apply(C, x2)).astype(f32)
+    y = thomas32(C, cp, mi, res)
+    return x2.astype(np.float64) + float(omega) * y.astype(np.float64)
 
 
 class VCycle:
@@ -107,15 +118,14 @@ class VCycle:
 
     def __call__(self, r0):
         L = len(self.lev)
-        w = f32(self.omega)
+        w = float(self.omega)
         rs = [np.asarray(r0, np.float64)]
         x1 = []
-        for l in range(L - 1):
-            C = self.lev[l]
-            cp, mi = self.fac[l]
-            xa = smooth(C, cp, mi, rs[l], None, float(w)).astype(f32)
-            x1.append(xa)
-            res = rs[l] - apply(C, xa)
+        cp, mi = self.fac[0]
+        x1.append(pre(self.lev[0], cp, mi, rs[0], w))
+        for l in range(1, L):
+            C = self.lev[l - 1]
+            res = rs[l - 1] - apply(C, x1[l - 1])
             ny, nz, nx = res.shape
             rc = np.zeros(((ny + 1) // 2, nz, (nx + 1) // 2))
             for pj in (0, 1):
@@ -123,14 +133,15 @@ class VCycle:
                     sub = res[pj::2, :, pi::2]
                     rc[:sub.shape[0], :, :sub.shape[2]] += sub
             rs.append(rc.astype(f32))
-        cp, mi = self.fac[L - 1]
-        x3 = smooth(self.lev[L - 1], cp, mi, rs[L - 1], None, 1.0).astype(f32)
+            cp, mi = self.fac[l]
+            x1.append(pre(self.lev[l], cp, mi, rs[l], 1.0 if l == L - 1 else w))
+        x3 = x1[L - 1]
         for l in range(L - 2, -1, -1):
             C = self.lev[l]
             cp, mi = self.fac[l]
-            up = np.repeat(np.repeat(x3.astype(np.float64), 2, axis=0), 2, axis=2)
+            up = np.repeat(np.repeat(x3, 2, axis=0), 2, axis=2)
             ny, nz, nx = x1[l].shape
-            x2 = x1[l].astype(np.float64) + up[:ny, :, :nx]
-            out = smooth(C, cp, mi, rs[l], x2, float(w))
+            x2 = (x1[l] + up[:ny, :, :nx]).astype(f32)
+            out = post(C, cp, mi, rs[l], x2, w)
             x3 = out if l == 0 else out.astype(f32)
         return x3
