@@ -38,13 +38,15 @@ WORKLOADS = {
     "cpu64": dict(nx=64, ny=64, nz=20, dx=250.0, n_hills=20, alpha="const", adv_den=True),
     # a smaller case whose inputs still exceed L2, for ncu captures
     "mid256": dict(nx=256, ny=256, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    # 67 M cells, 60 hills, alpha a smooth seeded field in [0.3, 1.0]
+    "mixed1024": dict(nx=1024, ny=1024, nz=64, dx=250.0, n_hills=60, alpha="smooth", adv_den=True),
 }
 # BiCGStab iterations the CPU restatement (2-sweep Jacobi-Richardson, FP64
 # Krylov, probed operator, 1e-6 recurrence norm) needs on each workload's
 # seed-1 case, measured by running it to convergence on the host (plain512:
 # 912 iterations, 136 s on 8 cores); the CPU sample extrapolates one solve
 # from these.
-REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None}
+REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
@@ -69,6 +71,8 @@ def solver_options(name: str):
         # the reference solve as the fallback on a 1%-per-50-iterations stall
         "mg": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64,
                    precond=_capi.PRECOND_MG, stall_iters=50),
+        # flexible GMRES(30) outer loop around the same V-cycle, FP64 Arnoldi basis
+        "fgmres": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_MG, fgmres_restart=30),
     }
     kw = presets[name]
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
@@ -390,7 +394,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain512", choices=sorted(WORKLOADS))
-    ap.add_argument("--solver", default="plain")
+    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres"])
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")

@@ -16,7 +16,7 @@ ERRORS = {-1: "HICARW_ERR_ARG", -2: "HICARW_ERR_STATE", -3: "HICARW_ERR_CUDA", -
           -5: "HICARW_ERR_NAN", -6: "HICARW_ERR_TIMEOUT"}
 MEM_DEVICE, MEM_HOST = 0, 1
 KRYLOV_F64, KRYLOV_F32 = 0, 1
-SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED = 0, 1, 2
+SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_FGMRES = 0, 1, 2, 3
 CRIT_RECURRENCE, CRIT_TRUE = 0, 1
 PRECOND_JACOBI, PRECOND_MG = 0, 1
 
@@ -40,7 +40,7 @@ class Options(C.Structure):
     _fields_ = [("max_iters", C.c_int), ("verbose", C.c_int), ("tol_rel", C.c_double), ("tol_abs", C.c_double),
                 ("krylov_precision", C.c_int), ("solver", C.c_int), ("criterion", C.c_int),
                 ("replace_every", C.c_int), ("check_every", C.c_int), ("precond", C.c_int),
-                ("stall_iters", C.c_int), ("mg_omega", C.c_float)]
+                ("stall_iters", C.c_int), ("mg_omega", C.c_float), ("fgmres_restart", C.c_int)]
 
 
 METRIC_FIELDS = ["jacobian", "jacobian_u", "jacobian_v", "jacobian_w", "dzdx", "dzdy", "dzdx_u", "dzdy_v",

@@ -23,6 +23,7 @@ UNITS = {
     "k_fused.cu": [],
     "k_mg.cu": [],
     "k_noalloc.cu": [],
+    "k_fgmres.cu": [],
     "capi.cu": [],
 }
 

@@ -21,6 +21,7 @@
 #include "kernels.h"
 #include "fused.h"
 #include "mg.h"
+#include "fgmres.h"
 
 using namespace hw;
 
@@ -121,6 +122,13 @@ struct hicarw_handle {
     std::map<GraphKey, GraphRec> graphs;
     FusedBufs fb;
     Mg mg;
+    GmresState *gst = nullptr;      // FGMRES device state
+    struct {
+        hicarw_handle *h;
+        int sweeps;
+    } fg_pc;                        // preconditioner context of the FGMRES launches
+    double *fgV = nullptr, *fgZ = nullptr, *fgW = nullptr;
+    int fg_m = 0;
     int mg_dirty = 1;     // coefficients changed since the multigrid hierarchy was built
     int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
@@ -153,6 +161,7 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->precond = HICARW_PRECOND_JACOBI;
     o->stall_iters = 0;
     o->mg_omega = 0.8f;
+    o->fgmres_restart = 30;
 }
 
 static Metrics metrics_of(const hicarw_handle *h)
@@ -208,6 +217,15 @@ static int ensure_vectors(hicarw_handle *h, int prec)
 
 template <typename T>
 static T *V(hicarw_handle *h, int q) { return (T *)h->vec[q]; }
+
+// Krylov vector precision of the configured solve: the reference schedule takes
+// the option, FGMRES is FP64, the FP32 schedules are FP32.
+static int solve_precision(const hicarw_handle *h)
+{
+    if (h->opt.solver == HICARW_SOLVER_REFERENCE) return h->opt.krylov_precision;
+    if (h->opt.solver == HICARW_SOLVER_FGMRES) return HICARW_KRYLOV_F64;
+    return HICARW_KRYLOV_F32;
+}
 
 // Stage a caller array to the device when it lives in host memory.
 static int stage_in(hicarw_handle *h, const float *src, float **buf, size_t n, int mem_kind, cudaStream_t s,
@@ -299,6 +317,10 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     h->graphs.clear();
     fused_free(h->fb);
     mg_free(h->mg);
+    if (h->gst) cudaFree(h->gst);
+    if (h->fgV) cudaFree(h->fgV);
+    if (h->fgZ) cudaFree(h->fgZ);
+    if (h->fgW) cudaFree(h->fgW);
     void *ptrs[] = {h->mjac, h->mju, h->mjv, h->mjw, h->mdzdx, h->mdzdy, h->mdzdx_u, h->mdzdy_v, h->madz, h->mnterr,
                     h->mf[0], h->mf[1], h->mf[2], h->mf[3], h->mf[4], h->dz_if, h->dzdx_surf, h->dzdy_surf, h->adz_col,
                     h->alpha, h->div, h->coef, h->bc, h->st, h->hist, h->partials, h->scan, h->su, h->sv, h->sw,
@@ -330,7 +352,7 @@ extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
         h->hist_cap = h->opt.max_iters + 2;
         CK(dalloc((void **)&h->hist, (size_t)h->hist_cap * sizeof(double)));
     }
-    int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    int prec = solve_precision(h);
     int rc = ensure_vectors(h, prec);
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
@@ -446,18 +468,21 @@ static int fetch_state(hicarw_handle *h, cudaStream_t s)
 }
 
 // bicgstab_solve (:555-791) on the current x / rhs.  Fills st (pinned mirror).
+static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s);
+
 static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allow_mg = 1)
 {
     int rc;
     h->use_mg = allow_mg && h->opt.precond == HICARW_PRECOND_MG && h->operator_probed &&
-                h->opt.solver == HICARW_SOLVER_REFERENCE;
+                (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES);
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
         if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
         h->mg_dirty = 0;
     }
+    if (h->opt.solver == HICARW_SOLVER_FGMRES) return fgmres_solve(h, sweeps, s);
     const int solver = h->opt.solver;
-    const int prec = solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    const int prec = solve_precision(h);
     rc = ensure_vectors(h, prec);
     if (rc) return rc;
     OpCtx c = opctx(h);
@@ -509,6 +534,122 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     return fetch_state(h, s);
 }
 
+// ---- flexible GMRES ------------------------------------------------------------
+
+static void fgmres_precond_cb(void *ctx, const double *in, double *out, cudaStream_t s)
+{
+    auto *pc = (decltype(hicarw_handle::fg_pc) *)ctx;
+    hicarw_handle *h = pc->h;
+    if (h->use_mg) mg_apply<double>(h->mg, in, out, h->st, s);
+    else enqueue_precond<double>(h, in, out, pc->sweeps, h->st, 0, s);
+}
+
+// Buffers (sized for the restart length) and the launch context of FGMRES(m).
+static int fgmres_prepare(hicarw_handle *h, int sweeps, FgmresCtx *f)
+{
+    int rc = ensure_vectors(h, HICARW_KRYLOV_F64);
+    if (rc) return rc;
+    const Dims &d = h->d;
+    int m = h->opt.fgmres_restart;
+    if (m < 1) m = 1;
+    if (m > FG_MAXM) m = FG_MAXM;
+    if (!h->gst) CK(dalloc((void **)&h->gst, sizeof(GmresState)));
+    if (h->fg_m != m) {
+        if (h->fgV) cudaFree(h->fgV);
+        if (h->fgZ) cudaFree(h->fgZ);
+        if (h->fgW) cudaFree(h->fgW);
+        h->fgV = h->fgZ = h->fgW = nullptr;
+        CK(dalloc((void **)&h->fgV, (size_t)(m + 1) * d.npad * sizeof(double)));
+        CK(dalloc((void **)&h->fgZ, (size_t)m * d.npad * sizeof(double)));
+        CK(dalloc((void **)&h->fgW, (size_t)d.npad * sizeof(double)));
+        h->fg_m = m;
+        for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+        h->graphs.clear();
+    }
+    h->fg_pc.h = h;
+    h->fg_pc.sweeps = sweeps;
+    f->op = opctx(h);
+    f->m = m;
+    f->x = V<double>(h, V_X);
+    f->b = V<double>(h, V_RHS);
+    f->V = h->fgV;
+    f->Z = h->fgZ;
+    f->W = h->fgW;
+    f->partials = h->partials;
+    f->red_blocks = h->red_blocks;
+    f->dot_blocks = 296;
+    f->g = h->gst;
+    f->g_h1 = h->gst->h1;
+    f->g_h2 = h->gst->h2;
+    f->g_hnext = &h->gst->hnext;
+    f->precond = fgmres_precond_cb;
+    f->pctx = &h->fg_pc;
+    return 0;
+}
+
+static void fgmres_enqueue_cycle(const FgmresCtx &f, cudaStream_t s)
+{
+    fgmres_enqueue_restart(f, s);
+    for (int j = 0; j < f.m; j++) fgmres_enqueue_step(f, j, s);
+    fgmres_enqueue_finish(f, s);
+}
+
+static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
+{
+    FgmresCtx f;
+    int rc = fgmres_prepare(h, sweeps, &f);
+    if (rc) return rc;
+    const int m = f.m;
+    fgmres_reset(h->gst, m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
+    CK(cudaEventRecord(h->t0, s));
+    // one restart cycle = one graph
+    GraphKey key{HICARW_KRYLOV_F64, sweeps, m, HICARW_SOLVER_FGMRES, 0, h->use_mg};
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+        cudaGraph_t graph;
+        g_capturing = 1;
+        g_capture_nodes = 0;
+        CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+        fgmres_enqueue_cycle(f, h->cap);
+        cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+        g_capturing = 0;
+        if (e != cudaSuccess) { set_err(h, "capture fgmres", e); return HICARW_ERR_CUDA; }
+        GraphRec rec;
+        rec.nodes = g_capture_nodes;
+        e = cudaGraphInstantiate(&rec.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { set_err(h, "instantiate fgmres", e); return HICARW_ERR_CUDA; }
+        it = h->graphs.emplace(key, rec).first;
+    }
+    const int max_cycles = h->opt.max_iters / m + 2;
+    int hstate[3];
+    for (int c = 0; c < max_cycles; c++) {
+        CK(cudaGraphLaunch(it->second.exec, s));
+        g_launches += it->second.nodes;
+        CK(cudaMemcpyAsync(hstate, &h->gst->it_total, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        // hstate = it_total, max_iters, status (GmresState field order)
+        if (hstate[2] == 0 || hstate[0] >= hstate[1]) break;
+        // not converged within the cycle: the next launch restarts from the current x
+    }
+    CK(cudaEventRecord(h->t1, s));
+    // map onto the BiCGStab state mirror for stats
+    GmresState gh;
+    CK(cudaMemcpyAsync(&gh, h->gst, sizeof(GmresState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+    if ((rc = fetch_state(h, s)) != 0) return rc;
+    h->hst->status = gh.status;
+    h->hst->it = gh.it_total;
+    h->hst->res0 = gh.res0;
+    h->hst->rnorm = gh.res;
+    h->hst->bnorm2 = gh.bnorm * gh.bnorm;
+    h->hst->target = gh.target;
+    return 0;
+}
+
 static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retries)
 {
     if (!o) return;
@@ -534,7 +675,7 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
 static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float *u, float *v, float *w, cudaStream_t s)
 {
     Metrics m = metrics_of(h);
-    if (h->opt.solver == HICARW_SOLVER_REFERENCE) {
+    if (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES) {
         if (h->vprec == HICARW_KRYLOV_F64) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
         else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
     } else {
@@ -581,7 +722,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
     const Dims &d = h->d;
     h->launches_at_call = g_launches.load();
     int rc;
-    const int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    const int prec = solve_precision(h);
     if ((rc = ensure_vectors(h, prec)) != 0) return rc;
     // module copies of alpha and div (:308-317)
     cudaMemcpyKind kind = mem_kind == HICARW_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
@@ -976,7 +1117,7 @@ extern "C" int hicarw_solve_rhs(hicarw_handle *h, const double *rhs, int mem_kin
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
     h->launches_at_call = g_launches.load();
-    const int prec = h->opt.solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    const int prec = solve_precision(h);
     int rc = ensure_vectors(h, prec);
     if (rc) return rc;
     double *b;
@@ -1030,14 +1171,21 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     if (!h || reps < 1 || cap < 1) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int solver = h->opt.solver;
-    const int prec = solver == HICARW_SOLVER_REFERENCE ? h->opt.krylov_precision : HICARW_KRYLOV_F32;
+    const int prec = solve_precision(h);
     int rc = ensure_vectors(h, prec);
     if (rc) return rc;
-    if (solver != HICARW_SOLVER_REFERENCE && (rc = fused_prepare(h->fb, h->d, s)) != 0) return HICARW_ERR_CUDA;
-    h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed && solver == HICARW_SOLVER_REFERENCE;
+    const int fused = solver == HICARW_SOLVER_FUSED || solver == HICARW_SOLVER_MIXED;
+    if (fused && (rc = fused_prepare(h->fb, h->d, s)) != 0) return HICARW_ERR_CUDA;
+    h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed && !fused;
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         if (mg_build(h->mg, h->d, h->coef, s) != 0) return HICARW_ERR_CUDA;
         h->mg_dirty = 0;
+    }
+    FgmresCtx fg;
+    if (solver == HICARW_SOLVER_FGMRES) {
+        if ((rc = fgmres_prepare(h, h->precond_n_sweeps, &fg)) != 0) return rc;
+        fgmres_reset(h->gst, fg.m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
+        fgmres_set_profile(h->gst, 1, s);
     }
     prof_state_kernel<<<1, 1, 0, s>>>(h->st, 1);
     CK(cudaStreamSynchronize(s));
@@ -1045,7 +1193,9 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     g_prof.clear();
     g_prof_on = 1;
     for (int q = 0; q < reps; q++) {
-        if (solver == HICARW_SOLVER_REFERENCE) {
+        if (solver == HICARW_SOLVER_FGMRES) {
+            fgmres_enqueue_cycle(fg, s);
+        } else if (solver == HICARW_SOLVER_REFERENCE) {
             if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, s);
             else enqueue_iteration<float, float>(h, V<float>(h, V_X), h->precond_n_sweeps, s);
         } else {
@@ -1055,6 +1205,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     }
     g_prof_on = 0;
     prof_state_kernel<<<1, 1, 0, s>>>(h->st, 0);
+    if (solver == HICARW_SOLVER_FGMRES) fgmres_set_profile(h->gst, 0, s);
     CK(cudaStreamSynchronize(s));
     // aggregate by kernel name, in first-launch order
     std::vector<std::string> nm;
@@ -1065,8 +1216,9 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         cudaEventElapsedTime(&t, r.a, r.b);
         size_t q = 0;
         while (q < nm.size() && nm[q] != r.name) q++;
-        if (q == nm.size()) { nm.push_back(r.name); tot.push_back(0.0); by.push_back(r.bytes); cnt.push_back(0); }
+        if (q == nm.size()) { nm.push_back(r.name); tot.push_back(0.0); by.push_back(0.0); cnt.push_back(0); }
         tot[q] += t;
+        by[q] += r.bytes;
         cnt[q] += 1;
     }
     for (auto &r : g_prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
@@ -1075,7 +1227,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     for (int q = 0; q < n; q++) {
         if (names) { strncpy(names + 32 * q, nm[q].c_str(), 31); names[32 * q + 31] = 0; }
         if (ms) ms[q] = tot[q] / cnt[q];
-        if (bytes) bytes[q] = by[q];
+        if (bytes) bytes[q] = by[q] / cnt[q];
         if (per_iter) per_iter[q] = cnt[q] / reps;
     }
     // the profiling pass overwrote the Krylov state: restart the next solve cold

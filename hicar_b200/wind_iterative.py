@@ -51,6 +51,7 @@ class WindOptions:
     precond: int = _capi.PRECOND_JACOBI
     stall_iters: int = 0
     mg_omega: float = 0.8
+    fgmres_restart: int = 30
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -66,6 +67,7 @@ class WindOptions:
         o.precond = int(self.precond)
         o.stall_iters = int(self.stall_iters)
         o.mg_omega = float(self.mg_omega)
+        o.fgmres_restart = int(self.fgmres_restart)
         return o
 
 

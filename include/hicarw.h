@@ -70,8 +70,10 @@ enum {
     HICARW_SOLVER_REFERENCE = 0, /* right-preconditioned BiCGStab, reference kernel schedule */
     HICARW_SOLVER_FUSED = 1,     /* same method, fused FP32 kernels (temporal blocking of the
                                     Jacobi-Richardson sweeps with the outer matvec) */
-    HICARW_SOLVER_MIXED = 2      /* FUSED + FP64 solution accumulation and periodic FP64
+    HICARW_SOLVER_MIXED = 2,     /* FUSED + FP64 solution accumulation and periodic FP64
                                     true-residual replacement (iterative refinement of lambda) */
+    HICARW_SOLVER_FGMRES = 3     /* flexible GMRES(m), FP64 Krylov, right-preconditioned with any
+                                    (also variable) preconditioner; the outer loop of the learned one */
 };
 
 /* Preconditioner. */
@@ -107,6 +109,7 @@ typedef struct hicarw_options {
     int stall_iters;      /* stop a preconditioned solve whose residual has not dropped by 1% for
                              this many iterations and fall back to the reference solve (0 = off) */
     float mg_omega;       /* damping of the multigrid smoother (default 0.8) */
+    int fgmres_restart;   /* FGMRES restart length m (1..32, default 30) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),
@@ -218,9 +221,10 @@ int hicarw_get_history(hicarw_handle *h, double *out, int cap);
 /* Profile one solve iteration of the current configuration: every kernel of the
  * iteration is launched on its own `reps` times and timed with CUDA events on
  * `stream`.  For each distinct kernel (first-launch order, at most cap): its
- * name (32 bytes each in names), mean duration in ms, algorithmic bytes of one
- * launch, and launches per iteration.  Returns the number of kernels.  The
- * solution is reset to zero. */
+ * name (32 bytes each in names), mean duration in ms, mean algorithmic bytes
+ * of one launch, and launches per iteration.  With HICARW_SOLVER_FGMRES one
+ * iteration is one restart cycle (fgmres_restart Arnoldi steps).  Returns the
+ * number of kernels.  The solution is reset to zero. */
 int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms, double *bytes, int *per_iter,
                              int cap, void *stream);
 
