@@ -28,7 +28,7 @@ EXPORTS = [
     "hicarw_calibrate_projection_operator", "hicarw_reset_solution", "hicarw_get_lambda", "hicarw_get_coefs",
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
     "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
-    "hicarw_residual_norm_noalloc",
+    "hicarw_residual_norm_noalloc", "hicarw_nn_act_pitch", "hicarw_nn_conv3", "hicarw_nn_conv3_wgrad",
 ]
 
 
@@ -105,6 +105,9 @@ def load(path: str = LIB_PATH):
         "hicarw_kernel_launches": (C.c_longlong, []),
         "hicarw_profile_iteration": (ci, [vp, ci, vp, vp, vp, vp, ci, vp]),
         "hicarw_residual_norm_noalloc": (ci, [vp, vp, vp, vp, vp]),
+        "hicarw_nn_act_pitch": (ci, [ci]),
+        "hicarw_nn_conv3": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp]),
+        "hicarw_nn_conv3_wgrad": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -24,6 +24,8 @@ UNITS = {
     "k_mg.cu": [],
     "k_noalloc.cu": [],
     "k_fgmres.cu": [],
+    "k_conv.cu": [],
+    "k_unet.cu": [],
     "capi.cu": [],
 }
 

@@ -36,7 +36,7 @@ void count_launch(int n)
 }
 
 struct ProfRec {
-    const char *name;
+    std::string name; // copied: callers may pass a temporary buffer
     double bytes;
     cudaEvent_t a, b;
 };

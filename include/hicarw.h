@@ -245,6 +245,25 @@ const char *hicarw_last_error(hicarw_handle *h);
 /* Number of kernels this library has launched since load (graph nodes included). */
 long long hicarw_kernel_launches(void);
 
+/* ---- learned preconditioner: tensor-core convolutions (no reference counterpart) ----
+ * Activation tensors use the "act layout": BF16, channels in groups of 8,
+ * element (c, i, k, j) of an (nx, nz, ny) grid at 16-byte unit
+ * (((j+1)*(nz+2) + (k+1))*(C/8) + c/8)*PX + (i+1), lane c%8, with
+ * PX = hicarw_nn_act_pitch(nx); halo cells are zero.  Weights are FP32
+ * [27][cin][cout] with tap t = (dj+1)*9 + (dk+1)*3 + (di+1).  Supported
+ * (cin, cout): (16,16), (16,32), (32,32), (32,16).  All pointers are device
+ * pointers; the calls are synchronous on `stream`. */
+int hicarw_nn_act_pitch(int nx);
+/* out = epilogue(bias + conv3x3x3(in)); epilogue: + skip, ReLU (relu != 0),
+ * zero where mask <= 0.  transpose != 0 runs the data-gradient convolution
+ * (cout -> cin channels, flipped taps).  out0 (optional) receives channel 0 in
+ * FP32 at the interior index (j*nz + k)*nx + i. */
+int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const void *in, const float *w, const float *bias,
+                    const void *skip, const void *mask, int relu, int transpose, void *out, float *out0, void *stream);
+/* dw[t][ci][co] += sum_v dy[v][co] x[v + off(t)][ci];  db[co] += sum_v dy[v][co]. */
+int hicarw_nn_conv3_wgrad(int cin, int cout, int nx, int ny, int nz, const void *x, const void *dy, float *dw,
+                          float *db, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
