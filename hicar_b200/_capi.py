@@ -18,7 +18,7 @@ MEM_DEVICE, MEM_HOST = 0, 1
 KRYLOV_F64, KRYLOV_F32 = 0, 1
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_FGMRES = 0, 1, 2, 3
 CRIT_RECURRENCE, CRIT_TRUE = 0, 1
-PRECOND_JACOBI, PRECOND_MG = 0, 1
+PRECOND_JACOBI, PRECOND_MG, PRECOND_LEARNED = 0, 1, 2
 
 # Every exported symbol of include/hicarw.h (checked by the CPU test suite).
 EXPORTS = [
@@ -29,6 +29,10 @@ EXPORTS = [
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
     "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
     "hicarw_residual_norm_noalloc", "hicarw_nn_act_pitch", "hicarw_nn_conv3", "hicarw_nn_conv3_wgrad",
+    "hicarw_unet_create", "hicarw_unet_destroy", "hicarw_unet_grid", "hicarw_unet_num_params",
+    "hicarw_unet_get_params", "hicarw_unet_set_params", "hicarw_unet_get_grads", "hicarw_unet_zero_grads",
+    "hicarw_unet_features", "hicarw_unet_forward", "hicarw_unet_backward", "hicarw_unet_backward_residual",
+    "hicarw_unet_adam_step", "hicarw_unet_apply", "hicarw_set_learned_precond",
 ]
 
 
@@ -108,6 +112,21 @@ def load(path: str = LIB_PATH):
         "hicarw_nn_act_pitch": (ci, [ci]),
         "hicarw_nn_conv3": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp]),
         "hicarw_nn_conv3_wgrad": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp]),
+        "hicarw_unet_create": (ci, [ci, ci, ci, C.c_ulonglong, P(vp)]),
+        "hicarw_unet_destroy": (ci, [vp]),
+        "hicarw_unet_grid": (ci, [vp, P(ci), P(ci), P(ci)]),
+        "hicarw_unet_num_params": (C.c_longlong, [vp]),
+        "hicarw_unet_get_params": (ci, [vp, vp, ci, vp]),
+        "hicarw_unet_set_params": (ci, [vp, vp, ci, vp]),
+        "hicarw_unet_get_grads": (ci, [vp, vp, ci, vp]),
+        "hicarw_unet_zero_grads": (ci, [vp, vp]),
+        "hicarw_unet_features": (ci, [vp, vp, vp, vp, P(C.c_float), vp]),
+        "hicarw_unet_forward": (ci, [vp, vp, vp, vp]),
+        "hicarw_unet_backward": (ci, [vp, vp, C.c_float, P(C.c_float), vp]),
+        "hicarw_unet_backward_residual": (ci, [vp, vp, vp, C.c_float, P(C.c_float), vp]),
+        "hicarw_unet_adam_step": (ci, [vp, C.c_float, vp]),
+        "hicarw_unet_apply": (ci, [vp, vp, vp, vp, vp]),
+        "hicarw_set_learned_precond": (ci, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

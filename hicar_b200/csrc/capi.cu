@@ -13,6 +13,7 @@
 
 #include <atomic>
 #include <map>
+#include <cstddef>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,7 @@
 #include "fused.h"
 #include "mg.h"
 #include "fgmres.h"
+#include "unet.h"
 
 using namespace hw;
 
@@ -123,6 +125,7 @@ struct hicarw_handle {
     FusedBufs fb;
     Mg mg;
     GmresState *gst = nullptr;      // FGMRES device state
+    GmresState *fg_host = nullptr;  // pinned copy of its scalar head
     struct {
         hicarw_handle *h;
         int sweeps;
@@ -130,6 +133,9 @@ struct hicarw_handle {
     double *fgV = nullptr, *fgZ = nullptr, *fgW = nullptr;
     int fg_m = 0;
     int mg_dirty = 1;     // coefficients changed since the multigrid hierarchy was built
+    hicarw_unet *unet = nullptr; // learned preconditioner (not owned)
+    int unet_dirty = 1;   // coefficients changed since the network's operator features were computed
+    int use_learned = 0;  // the current solve applies the learned preconditioner
     int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
     long long launches_at_call = 0;
@@ -318,6 +324,7 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     fused_free(h->fb);
     mg_free(h->mg);
     if (h->gst) cudaFree(h->gst);
+    if (h->fg_host) cudaFreeHost(h->fg_host);
     if (h->fgV) cudaFree(h->fgV);
     if (h->fgZ) cudaFree(h->fgZ);
     if (h->fgW) cudaFree(h->fgW);
@@ -475,6 +482,8 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     int rc;
     h->use_mg = allow_mg && h->opt.precond == HICARW_PRECOND_MG && h->operator_probed &&
                 (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES);
+    h->use_learned = allow_mg && h->opt.precond == HICARW_PRECOND_LEARNED && h->operator_probed &&
+                     h->opt.solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
         if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
@@ -535,12 +544,18 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
 }
 
 // ---- flexible GMRES ------------------------------------------------------------
+namespace hw { // k_unet.cu
+int unet_prepare_operator(hicarw_unet *n, const OpCtx &c, cudaStream_t s);
+int unet_precond(hicarw_unet *n, const OpCtx &c, const double *in, double *out, const SolveState *gate, cudaStream_t s);
+bool unet_matches(const hicarw_unet *n, const Dims &d);
+}  // namespace hw
 
 static void fgmres_precond_cb(void *ctx, const double *in, double *out, cudaStream_t s)
 {
     auto *pc = (decltype(hicarw_handle::fg_pc) *)ctx;
     hicarw_handle *h = pc->h;
-    if (h->use_mg) mg_apply<double>(h->mg, in, out, h->st, s);
+    if (h->use_learned) unet_precond(h->unet, opctx(h), in, out, h->st, s);
+    else if (h->use_mg) mg_apply<double>(h->mg, in, out, h->st, s);
     else enqueue_precond<double>(h, in, out, pc->sweeps, h->st, 0, s);
 }
 
@@ -554,6 +569,7 @@ static int fgmres_prepare(hicarw_handle *h, int sweeps, FgmresCtx *f)
     if (m < 1) m = 1;
     if (m > FG_MAXM) m = FG_MAXM;
     if (!h->gst) CK(dalloc((void **)&h->gst, sizeof(GmresState)));
+    if (!h->fg_host) CK(cudaMallocHost((void **)&h->fg_host, sizeof(GmresState)));
     if (h->fg_m != m) {
         if (h->fgV) cudaFree(h->fgV);
         if (h->fgZ) cudaFree(h->fgZ);
@@ -603,7 +619,15 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
     fgmres_reset(h->gst, m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
     CK(cudaEventRecord(h->t0, s));
     // one restart cycle = one graph
-    GraphKey key{HICARW_KRYLOV_F64, sweeps, m, HICARW_SOLVER_FGMRES, 0, h->use_mg};
+    if (h->use_learned && h->unet_dirty) {
+        if (unet_prepare_operator(h->unet, opctx(h), s) != 0) {
+            h->err = "learned preconditioner grid mismatch";
+            return HICARW_ERR_ARG;
+        }
+        h->unet_dirty = 0;
+    }
+    const int pkind = h->use_learned ? HICARW_PRECOND_LEARNED : (h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI);
+    GraphKey key{HICARW_KRYLOV_F64, sweeps, m, HICARW_SOLVER_FGMRES, 0, pkind};
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
         cudaGraph_t graph;
@@ -622,14 +646,23 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
         it = h->graphs.emplace(key, rec).first;
     }
     const int max_cycles = h->opt.max_iters / m + 2;
-    int hstate[3];
+    GmresState *hg = h->fg_host;
+    double best = 0.0;
+    int best_it = 0, stalled = 0;
     for (int c = 0; c < max_cycles; c++) {
         CK(cudaGraphLaunch(it->second.exec, s));
         g_launches += it->second.nodes;
-        CK(cudaMemcpyAsync(hstate, &h->gst->it_total, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hg, h->gst, offsetof(GmresState, hist), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        // hstate = it_total, max_iters, status (GmresState field order)
-        if (hstate[2] == 0 || hstate[0] >= hstate[1]) break;
+        if (hg->status == 0 || hg->it_total >= hg->max_iters) break;
+        // stall detector (as for BiCGStab): no 1% decrease of the residual within stall_iters steps
+        if (c == 0 || hg->res < 0.99 * best) {
+            best = hg->res;
+            best_it = hg->it_total;
+        } else if (h->opt.stall_iters > 0 && hg->it_total - best_it >= h->opt.stall_iters) {
+            stalled = 1;
+            break;
+        }
         // not converged within the cycle: the next launch restarts from the current x
     }
     CK(cudaEventRecord(h->t1, s));
@@ -641,7 +674,7 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
     RedBuf rb{h->partials, h->red_blocks};
     launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
     if ((rc = fetch_state(h, s)) != 0) return rc;
-    h->hst->status = gh.status;
+    h->hst->status = stalled ? 4 : gh.status;
     h->hst->it = gh.it_total;
     h->hst->res0 = gh.res0;
     h->hst->rnorm = gh.res;
@@ -664,7 +697,7 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
     o->target = st->target;
     o->true_res = st->true_res;
     o->replacements = st->replacements;
-    o->precond = h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI;
+    o->precond = h->use_learned ? HICARW_PRECOND_LEARNED : (h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, h->t0, h->t1);
     o->solve_ms = ms;
@@ -743,7 +776,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
         if ((rc = zero_solution(h, s)) != 0) return rc;
         h->structure_uploaded = 1;
-        h->mg_dirty = 1;
+        h->mg_dirty = h->unet_dirty = 1;
         CK(cudaStreamSynchronize(s));
     } else {
         CK(cudaStreamSynchronize(s));
@@ -751,7 +784,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         if (bmx > bmn && !h->operator_probed) { // varying alpha -> update_coefs_gpu (:423-426)
             launch_coefs(d, metrics_of(h), h->alpha, h->coef, 1, s);
             launch_bccol(d, metrics_of(h), h->alpha, h->bc, s);
-            h->mg_dirty = 1;
+            h->mg_dirty = h->unet_dirty = 1;
         }
     }
     if (h->hscan[0] > 0 && h->opt.verbose)
@@ -760,7 +793,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
     int sweeps = h->precond_n_sweeps;
     if ((rc = bicgstab_solve(h, sweeps, s)) != 0) return rc;
     int fell_back = 0;
-    if (h->use_mg && h->hst->status != 0) { // preconditioned solve stalled or failed: the reference solve decides
+    if ((h->use_mg || h->use_learned) && h->hst->status != 0) { // preconditioned solve stalled or failed: the reference solve decides
         if (h->opt.verbose)
             fprintf(stderr, " HICAR multigrid BiCGStab status=%d after %d iterations: falling back to Jacobi\n",
                     h->hst->status, h->hst->it);
@@ -910,7 +943,7 @@ extern "C" int hicarw_probe_finalize(hicarw_handle *h, float max_leak, void *str
     if (!h) return HICARW_ERR_ARG;
     h->operator_probed = 1;
     h->structure_uploaded = 1;
-    h->mg_dirty = 1;
+    h->mg_dirty = h->unet_dirty = 1;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     if (h->opt.verbose)
@@ -1030,7 +1063,7 @@ extern "C" int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed
                                  sizeof(float) * d.nx, d.nz, kind, s));
     h->operator_probed = probed ? 1 : 0;
     h->structure_uploaded = 1;
-    h->mg_dirty = 1;
+    h->mg_dirty = h->unet_dirty = 1;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     CK(cudaStreamSynchronize(s));
@@ -1177,6 +1210,12 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     const int fused = solver == HICARW_SOLVER_FUSED || solver == HICARW_SOLVER_MIXED;
     if (fused && (rc = fused_prepare(h->fb, h->d, s)) != 0) return HICARW_ERR_CUDA;
     h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed && !fused;
+    h->use_learned = h->opt.precond == HICARW_PRECOND_LEARNED && h->operator_probed &&
+                     solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
+    if (h->use_learned && h->unet_dirty) {
+        if (unet_prepare_operator(h->unet, opctx(h), s) != 0) return HICARW_ERR_ARG;
+        h->unet_dirty = 0;
+    }
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         if (mg_build(h->mg, h->d, h->coef, s) != 0) return HICARW_ERR_CUDA;
         h->mg_dirty = 0;
@@ -1232,6 +1271,23 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     }
     // the profiling pass overwrote the Krylov state: restart the next solve cold
     return zero_solution(h, s) ? HICARW_ERR_CUDA : n;
+}
+
+extern "C" int hicarw_set_learned_precond(hicarw_handle *h, hicarw_unet *n)
+{
+    if (!h) return HICARW_ERR_ARG;
+    if (n && !unet_matches(n, h->d)) {
+        h->err = "learned preconditioner: network grid differs from the handle's";
+        return HICARW_ERR_ARG;
+    }
+    if (h->unet != n) {
+        cudaDeviceSynchronize();
+        for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+        h->graphs.clear();
+    }
+    h->unet = n;
+    h->unet_dirty = 1;
+    return HICARW_OK;
 }
 
 // ---- accessors for the entry points defined in other files ----

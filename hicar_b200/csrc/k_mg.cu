@@ -250,7 +250,6 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
     const int nz = d.nz, n = TC * nz;
     float *s_res = sm, *s_c = sm + n, *s_m = sm + 2 * n, *s_cp = sm + 3 * n, *s_x = sm + 4 * n;
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
-    const long long cofs = (long long)CC * d.npad;
     stage_window<SX, SY>(d, x1, dc, xc, i0 - 1, j0 - 1, s_x);
     __syncthreads();
     for (int base = threadIdx.x; base < n; base += MG_THREADS * 2) {

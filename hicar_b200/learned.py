@@ -79,3 +79,197 @@ def conv3_wgrad(x_act, dy_act, nx, ny, nz, cin, cout, stream=None):
     if rc != 0:
         raise RuntimeError(f"hicarw_nn_conv3_wgrad failed ({rc})")
     return dw, db
+
+
+class UNet:
+    """The learned preconditioner's network for one grid size (owns its device
+    activations); parameters are an FP32 vector (conv weights [27][cin][cout]
+    then bias, convs a..g)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, seed: int = 0):
+        self.lib = _capi.load()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        h = C.c_void_p()
+        rc = self.lib.hicarw_unet_create(nx, ny, nz, seed, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"hicarw_unet_create failed ({rc})")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.hicarw_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _s(stream=None):
+        torch = _torch()
+        return C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+
+    @staticmethod
+    def _check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc})")
+
+    @property
+    def nparams(self) -> int:
+        return int(self.lib.hicarw_unet_num_params(self.h))
+
+    def params(self):
+        torch = _torch()
+        p = torch.empty(self.nparams, dtype=torch.float32, device="cuda")
+        self._check(self.lib.hicarw_unet_get_params(self.h, _ptr(p), _capi.MEM_DEVICE, self._s()), "get_params")
+        return p
+
+    def set_params(self, p):
+        torch = _torch()
+        p = p.to(device="cuda", dtype=torch.float32).contiguous()
+        self._check(self.lib.hicarw_unet_set_params(self.h, _ptr(p), _capi.MEM_DEVICE, self._s()), "set_params")
+
+    def grads(self):
+        torch = _torch()
+        g = torch.empty(self.nparams, dtype=torch.float32, device="cuda")
+        self._check(self.lib.hicarw_unet_get_grads(self.h, _ptr(g), _capi.MEM_DEVICE, self._s()), "get_grads")
+        return g
+
+    def zero_grads(self):
+        self._check(self.lib.hicarw_unet_zero_grads(self.h, self._s()), "zero_grads")
+
+    def features(self, handle, r):
+        """(x0 act tensor, rms) of residual r (cuda FP64 (ny+2, nz+2, nx+2))."""
+        x0 = act_empty(self.nx, self.ny, self.nz, 16, "cuda")
+        rms = C.c_float()
+        self._check(self.lib.hicarw_unet_features(self.h, handle, _ptr(r), _ptr(x0), C.byref(rms), self._s()),
+                    "features")
+        return x0, rms.value
+
+    def forward(self, x0):
+        torch = _torch()
+        o = torch.empty((self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
+        self._check(self.lib.hicarw_unet_forward(self.h, _ptr(x0), _ptr(o), self._s()), "forward")
+        return o
+
+    def backward(self, target, weight: float = 1.0) -> float:
+        """loss = weight * mean((O_0 - target)^2); its gradients are accumulated."""
+        loss = C.c_float()
+        self._check(self.lib.hicarw_unet_backward(self.h, _ptr(target), C.c_float(weight), C.byref(loss), self._s()),
+                    "backward")
+        return loss.value
+
+    def backward_residual(self, coefs, rhat, weight: float = 1.0) -> float:
+        """loss = weight * mean((A z - rhat)^2), z = O_0 / coef_A; gradients accumulated."""
+        loss = C.c_float()
+        self._check(self.lib.hicarw_unet_backward_residual(self.h, _ptr(coefs), _ptr(rhat), C.c_float(weight),
+                                                           C.byref(loss), self._s()), "backward_residual")
+        return loss.value
+
+    def adam_step(self, lr: float):
+        self._check(self.lib.hicarw_unet_adam_step(self.h, C.c_float(lr), self._s()), "adam_step")
+
+    def apply(self, handle, r):
+        torch = _torch()
+        z = torch.zeros_like(r)
+        self._check(self.lib.hicarw_unet_apply(self.h, handle, _ptr(r), _ptr(z), self._s()), "apply")
+        return z
+
+    def attach(self, handle):
+        """Use this network for HICARW_PRECOND_LEARNED solves of `handle` (same grid)."""
+        self._check(self.lib.hicarw_set_learned_precond(handle, self.h), "set_learned_precond")
+
+
+def random_residual(nx, ny, nz, gen, device="cuda"):
+    """A residual-like field (FP64, (ny+2, nz+2, nx+2), zero ghost cells): white
+    noise smoothed by a random number of 3x3 x-y box passes (0..16) and z passes
+    (0..2), so that the training set spans rough and smooth components."""
+    torch = _torch()
+    F = torch.nn.functional
+    x = torch.randn((1, 1, ny, nz, nx), generator=gen, dtype=torch.float64).to(device)
+    nxy = int(torch.randint(0, 17, (1,), generator=gen))
+    nzp = int(torch.randint(0, 3, (1,), generator=gen))
+    for _ in range(nxy):
+        x = F.avg_pool3d(F.pad(x, (1, 1, 0, 0, 1, 1), mode="replicate"), (3, 1, 3), stride=1)
+    for _ in range(nzp):
+        x = F.avg_pool3d(F.pad(x, (0, 0, 1, 1, 0, 0), mode="replicate"), (1, 3, 1), stride=1)
+    x = x / x.std()
+    r = torch.zeros((ny + 2, nz + 2, nx + 2), dtype=torch.float64, device=device)
+    r[1:-1, 1:-1, 1:-1] = x[0, 0]
+    return r
+
+
+def calibrated_handle(case):
+    """(DeviceDomain, handle) with the case's probed operator, calibrated as in update_winds."""
+    torch = _torch()
+    from . import wind, wind_iterative as wi
+    from .domain import DeviceDomain
+    dom = DeviceDomain.from_case(case, "cuda")
+    opt = wi.WindOptions(tol_rel=1e-6)
+    wi.init_iter_winds(dom, opt)
+    div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    wind.update_winds_iterative(dom, opt, div)
+    return dom, wi.handle(dom.nest_indx)
+
+
+def training_pairs(case, net: UNet, n_samples: int, seed: int = 0, solve: bool = False, tol: float = 1e-8):
+    """Training samples of one terrain case: for random residuals r (random_residual)
+    the network input features x0, the unit-rms residual rhat = r / rms(r) (FP32,
+    (ny, nz, nx)) and the operator's FP32 coefficients (15, ny, nz, nx), which the
+    residual loss ||A z - rhat||^2 needs.  With solve=True also the exact step
+    e = A^-1 r (FGMRES + multigrid to `tol`) as the target e * coef_A / rms(r) of
+    the supervised loss.  Each sample is (x0, rhat, coefs, target or None).
+    The handles made here are released again."""
+    torch = _torch()
+    from . import wind, wind_iterative as wi
+    dom, h = calibrated_handle(case)
+    lib = _capi.load()
+    wi.set_options(wi.WindOptions(tol_rel=tol, wind_solver_iterations=2000, solver=_capi.SOLVER_FGMRES,
+                                  precond=_capi.PRECOND_MG))
+    coefs = torch.empty((15, dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    _capi.check(lib.hicarw_get_coefs(h, _ptr(coefs), _capi.MEM_DEVICE, None), h)
+    diag = coefs[0].double()
+    gen = torch.Generator().manual_seed(seed)
+    out = []
+    st = _capi.Stats()
+    for _ in range(n_samples):
+        r = random_residual(dom.nx, dom.ny, dom.nz, gen)
+        x0, rms = net.features(h, r)
+        rhat = (r[1:-1, 1:-1, 1:-1] / rms).float().contiguous()
+        target = None
+        if solve:
+            lib.hicarw_reset_solution(h, None)
+            _capi.check(lib.hicarw_solve_rhs(h, _ptr(r), _capi.MEM_DEVICE, None, C.byref(st)), h)
+            e = torch.empty_like(r)
+            _capi.check(lib.hicarw_get_lambda(h, _ptr(e), _capi.MEM_DEVICE, None), h)
+            target = (e[1:-1, 1:-1, 1:-1] * diag / rms).float().contiguous()
+        out.append((x0, rhat, coefs, target))
+    wi.finalize_iter_winds()
+    wind.reset()
+    return out
+
+
+def train(net: UNet, pairs, steps: int, lr: float = 1e-3, batch: int = 4, seed: int = 0, loss: str = "residual"):
+    """Adam on the mean of the per-sample losses; returns the loss history.
+    loss="residual": mean((A z - rhat)^2) with z = O_0 / coef_A, the preconditioned
+    residual of a unit-rms residual, which weighs every error component by how
+    much the operator amplifies it.  loss="error": ||O_0 - T||^2 / ||T||^2 against
+    the exact step (pairs made with solve=True)."""
+    torch = _torch()
+    gen = torch.Generator().manual_seed(seed)
+    hist = []
+    for _ in range(steps):
+        net.zero_grads()
+        tot = 0.0
+        for _ in range(batch):
+            x0, rhat, coefs, target = pairs[int(torch.randint(0, len(pairs), (1,), generator=gen))]
+            net.forward(x0)
+            if loss == "residual":
+                tot += net.backward_residual(coefs, rhat)
+            else:
+                tot += net.backward(target, 1.0 / float((target.double() ** 2).mean()))
+        net.adam_step(lr)
+        hist.append(tot / batch)
+    return hist

@@ -79,8 +79,10 @@ enum {
 /* Preconditioner. */
 enum {
     HICARW_PRECOND_JACOBI = 0, /* the reference's Block-Jacobi / Jacobi-Richardson sweeps (:1268-1315) */
-    HICARW_PRECOND_MG = 1      /* multigrid V-cycle: z-line Jacobi smoother, 2x2 x-y aggregation,
+    HICARW_PRECOND_MG = 1,     /* multigrid V-cycle: z-line Jacobi smoother, 2x2 x-y aggregation,
                                   Galerkin coarse operators down to one column (probed operator only) */
+    HICARW_PRECOND_LEARNED = 2 /* the U-Net attached by hicarw_set_learned_precond (FGMRES only,
+                                  probed operator only) */
 };
 
 /* Stopping rule. */
@@ -139,6 +141,7 @@ typedef struct hicarw_stats {
 } hicarw_stats;
 
 typedef struct hicarw_handle hicarw_handle;
+typedef struct hicarw_unet hicarw_unet;
 
 /* Default options: the reference's constants (max_iters 1500, tol 1e-5/1e-10,
  * FP64 Krylov vectors, reference schedule, recurrence-norm stop). */
@@ -263,6 +266,44 @@ int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const void *in, c
 /* dw[t][ci][co] += sum_v dy[v][co] x[v + off(t)][ci];  db[co] += sum_v dy[v][co]. */
 int hicarw_nn_conv3_wgrad(int cin, int cout, int nx, int ny, int nz, const void *x, const void *dy, float *dw,
                           float *db, void *stream);
+
+/* ---- learned preconditioner: the U-Net (no reference counterpart) ----
+ * A 3-level U-Net of the convolutions above (levels: full grid, x-y halved,
+ * x-y quartered; 16/32/32 channels; ReLU; 2x2 average pooling; nearest
+ * upsampling; additive skips) maps the features of a residual r (r / rms(r)
+ * and the 14 stencil ratios coef_q / coef_A) to z = O_0 rms(r) / coef_A, a
+ * correction of the Jacobi step it starts from.  Parameters are FP32 (the
+ * 7 convolutions' [27][cin][cout] weights, each followed by its bias, in order
+ * a..g); activations BF16.  A network object owns the activations of one grid
+ * size; copy parameters between objects with get/set_params. */
+int hicarw_unet_create(int nx, int ny, int nz, unsigned long long seed, hicarw_unet **out);
+int hicarw_unet_destroy(hicarw_unet *n);
+int hicarw_unet_grid(const hicarw_unet *n, int *nx, int *ny, int *nz);
+long long hicarw_unet_num_params(const hicarw_unet *n);
+int hicarw_unet_get_params(hicarw_unet *n, float *out, int mem_kind, void *stream);
+int hicarw_unet_set_params(hicarw_unet *n, const float *in, int mem_kind, void *stream);
+int hicarw_unet_get_grads(hicarw_unet *n, float *out, int mem_kind, void *stream);
+int hicarw_unet_zero_grads(hicarw_unet *n, void *stream);
+/* Input features of r (device FP64, (nx+2, nz+2, ny+2)) for the handle's probed
+ * operator into x0 (device, act layout, 16 channels); rms(r) to *rms (host). */
+int hicarw_unet_features(hicarw_unet *n, hicarw_handle *h, const double *r, void *x0, float *rms, void *stream);
+/* Forward pass from features x0; out0 (device, optional) receives O_0 at (j*nz + k)*nx + i. */
+int hicarw_unet_forward(hicarw_unet *n, const void *x0, float *out0, void *stream);
+/* After a forward pass: loss = weight * mean((O_0 - target)^2) (to *loss, host),
+ * and the parameter gradients of that loss added to the accumulated gradients. */
+int hicarw_unet_backward(hicarw_unet *n, const float *target, float weight, float *loss, void *stream);
+/* After a forward pass on the features of a unit-rms residual rhat (device FP32
+ * (ny, nz, nx)): loss = weight * mean((A z - rhat)^2) with z = O_0 / coef_A and A
+ * the operator of the (15, ny, nz, nx) FP32 coefficients coef (hicarw_get_coefs
+ * layout, zero values outside the interior); gradients accumulated as above. */
+int hicarw_unet_backward_residual(hicarw_unet *n, const float *coef, const float *rhat, float weight, float *loss,
+                                  void *stream);
+/* Adam step (beta 0.9 / 0.999) with the mean of the accumulated gradients; clears them. */
+int hicarw_unet_adam_step(hicarw_unet *n, float lr, void *stream);
+/* z = M(r) on device FP64 (nx+2, nz+2, ny+2) vectors (ghost cells of z untouched). */
+int hicarw_unet_apply(hicarw_unet *n, hicarw_handle *h, const double *r, double *z, void *stream);
+/* Attach the network used by HICARW_PRECOND_LEARNED (same grid; NULL detaches). */
+int hicarw_set_learned_precond(hicarw_handle *h, hicarw_unet *n);
 
 #ifdef __cplusplus
 }
