@@ -73,6 +73,10 @@ def solver_options(name: str):
                    precond=_capi.PRECOND_MG, stall_iters=50),
         # flexible GMRES(30) outer loop around the same V-cycle, FP64 Arnoldi basis
         "fgmres": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_MG, fgmres_restart=30),
+        # flexible GMRES(30) with the trained U-Net preconditioner (BF16 tensor-core
+        # convolutions), the reference solve as the fallback on a stall
+        "learned": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_LEARNED, fgmres_restart=30,
+                        stall_iters=100),
     }
     kw = presets[name]
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
@@ -255,6 +259,13 @@ def run_ours(args, wl):
     ref_iters = ref_stats["iterations"]
     opt = solver_options(args.solver)
     wi.set_options(opt)
+    net = None
+    if args.solver == "learned":  # trained parameters, shipped with the package
+        from hicar_b200 import learned as L
+        from hicar_b200.train_unet import load_params
+        net = L.UNet(dom.nx, dom.ny, dom.nz)
+        net.set_params(torch.from_numpy(load_params()))
+        net.attach(h)
 
     def step():
         dom.set_winds(u0, v0, w0)
@@ -394,7 +405,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain512", choices=sorted(WORKLOADS))
-    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres"])
+    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres", "learned"])
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")

@@ -1,0 +1,80 @@
+"""Train the learned preconditioner's U-Net on synthetic terrains and save its
+parameters (FP32 .npy), e.g.
+
+    python -m hicar_b200.train_unet --nx 128 --ny 128 --nz 32 --terrains 16 \\
+        --samples 8 --steps 2000 --out hicar_b200/weights/unet_128x128x32.npy
+
+Terrains are the seeded generator's cases (hicar_b200.cases, seeds
+--seed0 .. --seed0 + terrains - 1); every sample is a random residual of one
+terrain's calibrated operator, and the loss is the residual loss
+mean((A z - rhat)^2) of hicar_b200.learned.train.  The network is
+convolutional, so parameters trained on one grid size serve any other
+(load_params / UNet.set_params)."""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_128x128x32.npy")
+
+
+def load_params(path: str = DEFAULT_WEIGHTS):
+    """FP32 parameter vector saved by this module."""
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"no trained U-Net parameters at {path} (run python -m hicar_b200.train_unet)")
+    return np.load(path).astype(np.float32)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=128)
+    ap.add_argument("--ny", type=int, default=128)
+    ap.add_argument("--nz", type=int, default=32)
+    ap.add_argument("--terrains", type=int, default=16)
+    ap.add_argument("--samples", type=int, default=8, help="random residuals per terrain")
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed0", type=int, default=1000)
+    ap.add_argument("--hills", type=int, default=20)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    args = ap.parse_args(argv)
+
+    import torch
+
+    from . import cases, learned as L
+    net = L.UNet(args.nx, args.ny, args.nz, seed=args.seed0)
+    t0 = time.time()
+    pairs = []
+    for t in range(args.terrains):
+        case = cases.build_case(args.nx, args.ny, args.nz, seed=args.seed0 + t, adv_den=True, n_hills=args.hills)
+        pairs += L.training_pairs(case, net, args.samples, seed=args.seed0 + t)
+    torch.cuda.synchronize()
+    t_data = time.time() - t0
+    t0 = time.time()
+    hist = []
+    lr = args.lr
+    for phase in range(4):  # step-decayed learning rate
+        hist += L.train(net, pairs, steps=args.steps // 4, lr=lr, batch=args.batch, seed=args.seed0 + phase)
+        lr *= 0.5
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    p = net.params().cpu().numpy()
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    np.save(args.out, p)
+    info = {"grid": [args.nx, args.ny, args.nz], "terrains": args.terrains, "samples": args.samples,
+            "steps": args.steps, "batch": args.batch, "lr": args.lr, "seed0": args.seed0,
+            "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
+            "data_s": t_data, "train_s": t_train, "params": int(p.size)}
+    with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+        json.dump(info, f, indent=1)
+    print(json.dumps(info))
+
+
+if __name__ == "__main__":
+    main()
