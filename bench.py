@@ -40,13 +40,17 @@ WORKLOADS = {
     "mid256": dict(nx=256, ny=256, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
     # 67 M cells, 60 hills, alpha a smooth seeded field in [0.3, 1.0]
     "mixed1024": dict(nx=1024, ny=1024, nz=64, dx=250.0, n_hills=60, alpha="smooth", adv_den=True),
+    # the learned preconditioner's training grid (its parameters come from seeds 1000..1015;
+    # the bench case, seed 1, is unseen) and its larger evaluation domain
+    "learn128": dict(nx=128, ny=128, nz=32, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    "eval768": dict(nx=768, ny=1536, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
 }
 # BiCGStab iterations the CPU restatement (2-sweep Jacobi-Richardson, FP64
 # Krylov, probed operator, 1e-6 recurrence norm) needs on each workload's
 # seed-1 case, measured by running it to convergence on the host (plain512:
 # 912 iterations, 136 s on 8 cores); the CPU sample extrapolates one solve
 # from these.
-REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None}
+REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None, "learn128": None, "eval768": None}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
@@ -73,6 +77,8 @@ def solver_options(name: str):
                    precond=_capi.PRECOND_MG, stall_iters=50),
         # flexible GMRES(30) outer loop around the same V-cycle, FP64 Arnoldi basis
         "fgmres": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_MG, fgmres_restart=30),
+        # flexible GMRES(30) with the reference Jacobi-Richardson preconditioner (A/B baseline)
+        "fgmres_jacobi": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_JACOBI, fgmres_restart=30),
         # flexible GMRES(30) with the trained U-Net preconditioner (BF16 tensor-core
         # convolutions), the reference solve as the fallback on a stall
         "learned": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_LEARNED, fgmres_restart=30,
@@ -405,7 +411,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain512", choices=sorted(WORKLOADS))
-    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres", "learned"])
+    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres", "fgmres_jacobi", "learned"])
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")
