@@ -33,7 +33,14 @@ EXPORTS = [
     "hicarw_unet_get_params", "hicarw_unet_set_params", "hicarw_unet_get_grads", "hicarw_unet_zero_grads",
     "hicarw_unet_features", "hicarw_unet_forward", "hicarw_unet_backward", "hicarw_unet_backward_residual",
     "hicarw_unet_adam_step", "hicarw_unet_apply", "hicarw_set_learned_precond",
+    "hicarw_batch_create", "hicarw_batch_destroy", "hicarw_batch_config", "hicarw_batch_get_config",
+    "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune",
 ]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("alpha", C.c_void_p), ("div", C.c_void_p), ("density", C.c_void_p),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p)]
 
 
 class Grid(C.Structure):
@@ -127,6 +134,12 @@ def load(path: str = LIB_PATH):
         "hicarw_unet_adam_step": (ci, [vp, C.c_float, vp]),
         "hicarw_unet_apply": (ci, [vp, vp, vp, vp, vp]),
         "hicarw_set_learned_precond": (ci, [vp, vp]),
+        "hicarw_batch_create": (ci, [ci, vp, P(vp)]),
+        "hicarw_batch_destroy": (ci, [vp]),
+        "hicarw_batch_config": (ci, [vp, ci, ci]),
+        "hicarw_batch_get_config": (ci, [vp, P(ci), P(ci)]),
+        "hicarw_batch_calc_iter_winds": (ci, [vp, P(BatchItem), ci, ci, vp, P(Stats)]),
+        "hicarw_batch_autotune": (ci, [vp, P(BatchItem), ci, vp, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -13,6 +13,7 @@
 
 #include <atomic>
 #include <map>
+#include <algorithm>
 #include <cstddef>
 #include <string>
 #include <vector>
@@ -1287,6 +1288,331 @@ extern "C" int hicarw_set_learned_precond(hicarw_handle *h, hicarw_unet *n)
     }
     h->unet = n;
     h->unet_dirty = 1;
+    return HICARW_OK;
+}
+
+// ---- batched solves of independent subdomains ---------------------------------
+// One CUDA graph solves every subdomain of the batch: per subdomain a chain
+// [inputs + RHS + BiCGStab set-up] -> WHILE node whose body is `chunk`
+// iterations plus a one-thread kernel that keeps the loop running while the
+// device-side solve state has not stopped.  So a whole batch of uneven solves
+// is one graph launch and one host synchronisation; the subdomains are spread
+// over `lanes` independent chains (longest-processing-time order by size) that
+// the GPU runs concurrently.  Every WHILE loop is also bounded by a body count
+// (max_iters / chunk + 2), so it ends even if a solve never sets its flag.
+#define BCK(x)                                                                                                   \
+    do {                                                                                                         \
+        cudaError_t e_ = (x);                                                                                    \
+        if (e_ != cudaSuccess) {                                                                                 \
+            fprintf(stderr, "hicarw batch: %s: %s\n", #x, cudaGetErrorString(e_));                               \
+            return HICARW_ERR_CUDA;                                                                              \
+        }                                                                                                        \
+    } while (0)
+
+struct hicarw_batch {
+    std::vector<hicarw_handle *> hs;
+    int lanes = 0, chunk = 4; // lanes <= 0: one chain per subdomain
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;
+    std::vector<hicarw_batch_item> built;
+    int built_lanes = -1, built_chunk = -1, built_cold = -1;
+    int *counters = nullptr; // device: WHILE-body executions per subdomain
+    cudaStream_t cap = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    float last_ms = 0.0f;
+};
+
+__global__ void batch_count_reset_kernel(int *count) { *count = 0; }
+
+__global__ void batch_cond_kernel(cudaGraphConditionalHandle hc, const SolveState *st, int *count, int limit)
+{
+    const int c = *count + 1;
+    *count = c;
+    const int more = !*(volatile const int *)&st->stop && c < limit;
+    cudaGraphSetConditional(hc, more ? 1u : 0u);
+}
+
+static bool same_items(const hicarw_batch *b, const hicarw_batch_item *items)
+{
+    if (b->built.size() != b->hs.size()) return false;
+    for (size_t i = 0; i < b->hs.size(); i++) {
+        const hicarw_batch_item &x = b->built[i], &y = items[i];
+        if (x.alpha != y.alpha || x.div != y.div || x.density != y.density || x.u != y.u || x.v != y.v || x.w != y.w)
+            return false;
+    }
+    return true;
+}
+
+static void batch_drop_graph(hicarw_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->built.clear();
+}
+
+// enqueue (capture) the per-subdomain set-up: inputs, diagonal, RHS, solve state, r = b - A x
+static void batch_enqueue_setup(hicarw_batch *b, int i, const hicarw_batch_item &it, int cold, cudaStream_t s)
+{
+    hicarw_handle *h = b->hs[i];
+    const Dims &d = h->d;
+    cudaMemcpyAsync(h->alpha, it.alpha, n_cell(d) * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(h->div, it.div, n_cell(d) * 4, cudaMemcpyDeviceToDevice, s);
+    if (cold) cudaMemsetAsync(h->vec[V_X], 0, (size_t)d.npad * 8, s);
+    prepare_system(h, s);
+    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->use_mg ? h->opt.stall_iters : 0, s);
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R), V<double>(h, V_RHAT),
+                                 V<double>(h, V_P), h->st, h->hist, rb, s);
+    batch_count_reset_kernel<<<1, 1, 0, s>>>(b->counters + i);
+    count_launch(1);
+}
+
+static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold)
+{
+    batch_drop_graph(b);
+    const int n = (int)b->hs.size();
+    const int lanes = b->lanes <= 0 || b->lanes > n ? n : b->lanes;
+    // longest processing time first: biggest subdomain to the least loaded lane
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int c) { return b->hs[a]->d.npad > b->hs[c]->d.npad; });
+    std::vector<long long> load(lanes, 0);
+    std::vector<cudaGraphNode_t> tail(lanes, nullptr);
+    cudaGraph_t g;
+    BCK(cudaGraphCreate(&g, 0));
+    long long nodes = 0;
+    cudaError_t e = cudaSuccess;
+    for (int oi = 0; oi < n && e == cudaSuccess; oi++) {
+        const int i = order[oi];
+        hicarw_handle *h = b->hs[i];
+        int L = 0;
+        for (int q = 1; q < lanes; q++)
+            if (load[q] < load[L]) L = q;
+        load[L] += h->d.npad;
+        // set-up as a child graph
+        cudaGraph_t sg;
+        g_capturing = 1;
+        g_capture_nodes = 0;
+        e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) break;
+        batch_enqueue_setup(b, i, items[i], cold, b->cap);
+        e = cudaStreamEndCapture(b->cap, &sg);
+        g_capturing = 0;
+        if (e != cudaSuccess) break;
+        nodes += g_capture_nodes;
+        cudaGraphNode_t sn, wn;
+        e = cudaGraphAddChildGraphNode(&sn, g, tail[L] ? &tail[L] : nullptr, tail[L] ? 1 : 0, sg);
+        cudaGraphDestroy(sg);
+        if (e != cudaSuccess) break;
+        // the device-driven loop
+        cudaGraphConditionalHandle hc;
+        e = cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) break;
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = hc;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        e = cudaGraphAddNode(&wn, g, &sn, 1, &p);
+        if (e != cudaSuccess) break;
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        g_capturing = 1;
+        g_capture_nodes = 0;
+        e = cudaStreamBeginCaptureToGraph(b->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { g_capturing = 0; break; }
+        for (int q = 0; q < b->chunk; q++)
+            enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, b->cap);
+        const int limit = h->opt.max_iters / b->chunk + 2;
+        batch_cond_kernel<<<1, 1, 0, b->cap>>>(hc, h->st, b->counters + i, limit);
+        count_launch(1);
+        e = cudaStreamEndCapture(b->cap, &body);
+        g_capturing = 0;
+        nodes += g_capture_nodes;
+        tail[L] = wn;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->exec = nullptr;
+        fprintf(stderr, "hicarw batch graph: %s\n", cudaGetErrorString(e));
+        return HICARW_ERR_CUDA;
+    }
+    b->nodes = nodes;
+    b->built.assign(items, items + n);
+    b->built_lanes = b->lanes;
+    b->built_chunk = b->chunk;
+    b->built_cold = cold;
+    return 0;
+}
+
+// One batched solve; apply != 0 also corrects the winds.  stats: n entries or null.
+static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold, int apply, cudaStream_t s,
+                     hicarw_stats *stats)
+{
+    const int n = (int)b->hs.size();
+    int rc;
+    bool rebuild = !b->exec || !same_items(b, items) || b->built_lanes != b->lanes || b->built_chunk != b->chunk ||
+                   b->built_cold != cold;
+    for (int i = 0; i < n; i++) {
+        hicarw_handle *h = b->hs[i];
+        h->launches_at_call = g_launches.load();
+        h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed;
+        h->use_learned = 0;
+        if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
+            h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+            if (mg_build(h->mg, h->d, h->coef, s) != 0) {
+                fprintf(stderr, "hicarw batch: multigrid build of subdomain %d failed\n", i);
+                return HICARW_ERR_CUDA;
+            }
+            h->mg_dirty = 0;
+            rebuild = true;
+        }
+    }
+    if (rebuild) {
+        BCK(cudaStreamSynchronize(s));
+        if ((rc = batch_build(b, items, cold)) != 0) return rc;
+    }
+    BCK(cudaEventRecord(b->t0, s));
+    for (int i = 0; i < n; i++) BCK(cudaEventRecord(b->hs[i]->t0, s)); // per-handle solve time = the batch's
+    BCK(cudaGraphLaunch(b->exec, s));
+    g_launches += b->nodes;
+    BCK(cudaEventRecord(b->t1, s));
+    for (int i = 0; i < n; i++) BCK(cudaEventRecord(b->hs[i]->t1, s));
+    for (int i = 0; i < n; i++)
+        BCK(cudaMemcpyAsync(b->hs[i]->hst, b->hs[i]->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
+    std::vector<int> fell(n, 0);
+    for (int i = 0; i < n; i++) { // a stalled or failed preconditioned solve: the reference solve decides
+        hicarw_handle *h = b->hs[i];
+        if (h->hst->status != 0 && h->use_mg) {
+            if ((rc = zero_solution(h, s)) != 0 || (rc = bicgstab_solve(h, h->precond_n_sweeps, s, 0)) != 0) {
+                fprintf(stderr, "hicarw batch: fallback solve of subdomain %d: %s\n", i, h->err.c_str());
+                return rc;
+            }
+            fell[i] = 1;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        hicarw_handle *h = b->hs[i];
+        OpCtx c = opctx(h);
+        RedBuf rb{h->partials, h->red_blocks};
+        launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+        if (apply) enqueue_winds(h, adv_den ? items[i].density : nullptr, adv_den, items[i].u, items[i].v, items[i].w, s);
+        BCK(cudaMemcpyAsync(h->hst, h->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    }
+    BCK(cudaStreamSynchronize(s));
+    if (stats)
+        for (int i = 0; i < n; i++) {
+            fill_stats(b->hs[i], &stats[i], b->hs[i]->precond_n_sweeps, 0);
+            stats[i].solve_ms = b->last_ms;
+            if (fell[i]) {
+                stats[i].status = HICARW_FELL_BACK;
+                stats[i].precond = HICARW_PRECOND_JACOBI;
+            }
+        }
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_batch **out)
+{
+    if (n < 1 || !handles || !out) return HICARW_ERR_ARG;
+    for (int i = 0; i < n; i++) {
+        hicarw_handle *h = handles[i];
+        if (!h || !h->operator_probed || h->opt.solver != HICARW_SOLVER_REFERENCE ||
+            h->opt.krylov_precision != HICARW_KRYLOV_F64)
+            return HICARW_ERR_ARG; // calibrated handles with the reference schedule and FP64 Krylov vectors
+        for (int q = 0; q < i; q++)
+            if (handles[q] == h) return HICARW_ERR_ARG;
+        if (ensure_vectors(h, HICARW_KRYLOV_F64) != 0) return HICARW_ERR_CUDA;
+    }
+    hicarw_batch *b = new hicarw_batch();
+    b->hs.assign(handles, handles + n);
+    if (cudaMalloc((void **)&b->counters, n * sizeof(int)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) {
+        delete b;
+        return HICARW_ERR_CUDA;
+    }
+    cudaMemset(b->counters, 0, n * sizeof(int));
+    *out = b;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_batch_destroy(hicarw_batch *b)
+{
+    if (!b) return HICARW_ERR_ARG;
+    cudaDeviceSynchronize();
+    batch_drop_graph(b);
+    if (b->counters) cudaFree(b->counters);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->t0) cudaEventDestroy(b->t0);
+    if (b->t1) cudaEventDestroy(b->t1);
+    delete b;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_batch_config(hicarw_batch *b, int lanes, int chunk)
+{
+    if (!b || chunk < 1 || chunk > 64) return HICARW_ERR_ARG;
+    b->lanes = lanes;
+    b->chunk = chunk;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *chunk)
+{
+    if (!b) return HICARW_ERR_ARG;
+    if (lanes) *lanes = b->lanes <= 0 ? (int)b->hs.size() : b->lanes;
+    if (chunk) *chunk = b->chunk;
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold,
+                                            void *stream, hicarw_stats *stats)
+{
+    if (!b || !items) return HICARW_ERR_ARG;
+    for (size_t i = 0; i < b->hs.size(); i++)
+        if (!items[i].alpha || !items[i].div || !items[i].u || !items[i].v || !items[i].w ||
+            (adv_den && !items[i].density))
+            return HICARW_ERR_ARG;
+    return batch_run(b, items, adv_den, cold, 1, (cudaStream_t)stream, stats);
+}
+
+// Autotuner: time cold batched solves (no wind correction) for every (lanes,
+// chunk) candidate and keep the fastest; the solutions are cleared afterwards.
+extern "C" int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, void *stream,
+                                     double *best_ms)
+{
+    if (!b || !items) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = (int)b->hs.size();
+    const int lane_c[] = {1, 2, 4, 8, 16, 32, 64};
+    const int chunk_c[] = {2, 4, 8};
+    double best = 1e300;
+    int bl = b->lanes, bc = b->chunk;
+    for (int lc : lane_c) {
+        if (lc > n) continue;
+        for (int cc : chunk_c) {
+            b->lanes = lc;
+            b->chunk = cc;
+            int rc = batch_run(b, items, adv_den, 1, 0, s, nullptr); // build + warm
+            if (rc) return rc;
+            if ((rc = batch_run(b, items, adv_den, 1, 0, s, nullptr)) != 0) return rc;
+            if (b->last_ms < best) {
+                best = b->last_ms;
+                bl = lc;
+                bc = cc;
+            }
+        }
+    }
+    b->lanes = bl;
+    b->chunk = bc;
+    batch_drop_graph(b);
+    for (int i = 0; i < n; i++) zero_solution(b->hs[i], s);
+    BCK(cudaStreamSynchronize(s));
+    if (best_ms) *best_ms = best;
     return HICARW_OK;
 }
 

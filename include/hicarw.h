@@ -142,6 +142,7 @@ typedef struct hicarw_stats {
 
 typedef struct hicarw_handle hicarw_handle;
 typedef struct hicarw_unet hicarw_unet;
+typedef struct hicarw_batch hicarw_batch;
 
 /* Default options: the reference's constants (max_iters 1500, tol 1e-5/1e-10,
  * FP64 Krylov vectors, reference schedule, recurrence-norm stop). */
@@ -244,6 +245,31 @@ int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double
 
 /* Last CUDA error string of this handle (static storage). */
 const char *hicarw_last_error(hicarw_handle *h);
+
+/* ---- batched solves of independent, unevenly sized subdomains (no reference counterpart) ----
+ * A batch borrows n calibrated handles (probed operator, HICARW_SOLVER_REFERENCE,
+ * FP64 Krylov; Jacobi or multigrid preconditioner) and solves all of them in one
+ * CUDA graph launch: per subdomain the set-up and a device-driven WHILE loop of
+ * BiCGStab iterations, the subdomains spread over `lanes` concurrent chains.
+ * Stalled multigrid solves fall back to the reference solve (status 3) as in
+ * hicarw_calc_iter_winds.  All item pointers are device pointers in the layouts
+ * of hicarw_calc_iter_winds; a handle may belong to one batch at a time. */
+typedef struct hicarw_batch_item {
+    const float *alpha, *div, *density; /* density may be NULL when adv_den == 0 */
+    float *u, *v, *w;
+} hicarw_batch_item;
+int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_batch **out);
+int hicarw_batch_destroy(hicarw_batch *b);
+/* lanes <= 0: one chain per subdomain; chunk: BiCGStab iterations per loop body (1..64). */
+int hicarw_batch_config(hicarw_batch *b, int lanes, int chunk);
+int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *chunk);
+/* Solve every subdomain (cold != 0 starts from lambda = 0, else from the last
+ * solution, as calc_iter_winds) and correct its winds; stats: n entries (or NULL). */
+int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold, void *stream,
+                                 hicarw_stats *stats);
+/* Time cold solves (winds untouched) for lanes in {1,2,4,...,64} and chunk in
+ * {2,4,8}, keep the fastest configuration; *best_ms its batch time. */
+int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, void *stream, double *best_ms);
 
 /* Number of kernels this library has launched since load (graph nodes included). */
 long long hicarw_kernel_launches(void);
