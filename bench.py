@@ -44,13 +44,17 @@ WORKLOADS = {
     # the bench case, seed 1, is unseen) and its larger evaluation domain
     "learn128": dict(nx=128, ny=128, nz=32, dx=250.0, n_hills=20, alpha="const", adv_den=True),
     "eval768": dict(nx=768, ny=1536, nz=48, dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    # 96 independent subdomains, nx, ny in 96..512 step 32, nz in 20..48 step 4 (seeded), solved
+    # together by the batched graph solver (one step = all 96 solves)
+    "batch12": dict(batch=12, nxy=(96, 256, 32), nz=(20, 32, 4), dx=250.0, n_hills=20, alpha="const", adv_den=True),
+    "batch96": dict(batch=96, nxy=(96, 512, 32), nz=(20, 48, 4), dx=250.0, n_hills=20, alpha="const", adv_den=True),
 }
 # BiCGStab iterations the CPU restatement (2-sweep Jacobi-Richardson, FP64
 # Krylov, probed operator, 1e-6 recurrence norm) needs on each workload's
 # seed-1 case, measured by running it to convergence on the host (plain512:
 # 912 iterations, 136 s on 8 cores); the CPU sample extrapolates one solve
 # from these.
-REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None, "learn128": None, "eval768": None}
+REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
@@ -228,6 +232,40 @@ def run_reference(args, wl):
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
+def profile_roofline(lib, h, stream, ncu_range: bool, traffic_key: str):
+    """Per-launch CUDA-event profile of one solve iteration of handle h (every
+    kernel of the iteration launched on its own, timed on `stream`) -> the
+    roofline object of the dominant kernel."""
+    import ctypes as C
+
+    import torch
+    cap = 32
+    names = C.create_string_buffer(32 * cap)
+    ms = (C.c_double * cap)()
+    by = (C.c_double * cap)()
+    cnt = (C.c_int * cap)()
+    if ncu_range:
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+    n = lib.hicarw_profile_iteration(h, 5, names, ms, by, cnt, cap, stream.cuda_stream)
+    if ncu_range:
+        torch.cuda.cudart().cudaProfilerStop()
+    prof = []
+    for q in range(max(n, 0)):
+        nm = names.raw[32 * q:32 * q + 32].split(b"\0")[0].decode()
+        prof.append({"kernel": nm, "ms": ms[q], "bytes": by[q], "per_iter": cnt[q], "share_ms": ms[q] * cnt[q]})
+    if not prof:
+        return None
+    tot = sum(p["share_ms"] for p in prof) or 1.0
+    dom_k = max(prof, key=lambda p: p["share_ms"])
+    peak, peak_kind = peaks()
+    ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "peak_kind": peak_kind, "traffic": TRAFFIC.get(f"{traffic_key}:{dom_k['kernel']}"),
+            "share": dom_k["share_ms"] / tot,
+            "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
+
+
 def run_ours(args, wl):
     import ctypes as C
 
@@ -347,32 +385,7 @@ def run_ours(args, wl):
     e2e_value = world * e2e_steps / (te / 1000.0)
 
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
-    cap = 32
-    names = C.create_string_buffer(32 * cap)
-    ms = (C.c_double * cap)()
-    by = (C.c_double * cap)()
-    cnt = (C.c_int * cap)()
-    if args.ncu_range == "profile":
-        torch.cuda.synchronize()
-        torch.cuda.cudart().cudaProfilerStart()
-    n = lib.hicarw_profile_iteration(h, 5, names, ms, by, cnt, cap, stream.cuda_stream)
-    if args.ncu_range == "profile":
-        torch.cuda.cudart().cudaProfilerStop()
-    prof = []
-    for q in range(max(n, 0)):
-        nm = names.raw[32 * q:32 * q + 32].split(b"\0")[0].decode()
-        prof.append({"kernel": nm, "ms": ms[q], "bytes": by[q], "per_iter": cnt[q], "share_ms": ms[q] * cnt[q]})
-    tot = sum(p["share_ms"] for p in prof) or 1.0
-    dom_k = max(prof, key=lambda p: p["share_ms"]) if prof else None
-    peak, peak_kind = peaks()
-    traffic = TRAFFIC.get(f"{args.workload}:{args.solver}:{dom_k['kernel']}") if dom_k else None
-    roofline = None
-    if dom_k:
-        ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
-                    "share": dom_k["share_ms"] / tot,
-                    "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
+    roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", f"{args.workload}:{args.solver}")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -404,6 +417,137 @@ def run_ours(args, wl):
         dist.destroy_process_group()
 
 
+def run_batch(args, wl):
+    """The batch workload: every step solves all subdomains (divergence, batched
+    MG-preconditioned BiCGStab in one graph launch, wind correction)."""
+    import ctypes as C
+
+    import torch
+    from hicar_b200 import _capi
+    from hicar_b200.batch import BatchSolver, subdomain_cases
+    from hicar_b200.domain import ptr
+    from hicar_b200.wind_iterative import WindOptions
+
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = _capi.load()
+    stream = torch.cuda.current_stream()
+    opts = WindOptions(tol_rel=TOL, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50,
+                       advect_density=wl["adv_den"])
+    bs = BatchSolver(subdomain_cases(wl["batch"], seed=1 + rank, nxy=wl["nxy"], nz=wl["nz"], n_hills=wl["n_hills"],
+                                     dx=wl["dx"]), options=opts, stream=stream.cuda_stream)
+    tuned_ms = bs.autotune()
+    lanes, chunk = bs.config()
+    # the same subdomains one after another through hicarw_calc_iter_winds (untimed by the contract; reported)
+    bs.restore_winds()
+    bs.divergence()
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    st = _capi.Stats()
+    for i, (h, dom) in enumerate(zip(bs.handles, bs.domains)):
+        lib.hicarw_reset_solution(h, C.c_void_p(bs.stream))
+        _capi.check(lib.hicarw_calc_iter_winds(h, ptr(dom.wind_alpha), ptr(bs.divs[i]), ptr(dom.density), 1,
+                                               ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt), _capi.MEM_DEVICE,
+                                               C.c_void_p(bs.stream), C.byref(st)), h)
+    q1.record()
+    torch.cuda.synchronize()
+    seq_ms = q0.elapsed_time(q1)
+    for _ in range(args.warmup):
+        bs.step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = lib.hicarw_kernel_launches()
+    torch.cuda.synchronize()
+    e0.record()
+    stats = []
+    for _ in range(args.steps):
+        stats = bs.step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = lib.hicarw_kernel_launches() - l0
+    clocks = sampler.stop()
+    t_ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([t_ms], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * args.steps * bs.n / (t_ms / 1000.0)
+    # e2e: every subdomain's winds from pinned host memory in, corrected winds out
+    host = [[torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in sv] for sv in bs.saved]
+    for hs, sv in zip(host, bs.saved):
+        for dst, src in zip(hs, sv):
+            dst.copy_(src.cpu())
+    outs = [[torch.empty_like(a) for a in hs] for hs in host]
+    h2d = sum(a.numel() * 4 for hs in host for a in hs)
+
+    def e2e_step():
+        for dom, hs in zip(bs.domains, host):
+            dom.u_dqdt.copy_(hs[0], non_blocking=True)
+            dom.v_dqdt.copy_(hs[1], non_blocking=True)
+            dom.w_dqdt.copy_(hs[2], non_blocking=True)
+        bs.divergence()
+        bs.solve(cold=True)
+        for dom, os_ in zip(bs.domains, outs):
+            os_[0].copy_(dom.u_dqdt, non_blocking=True)
+            os_[1].copy_(dom.v_dqdt, non_blocking=True)
+            os_[2].copy_(dom.w_dqdt, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    te = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([te], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = world * e2e_steps * bs.n / (te / 1000.0)
+    big = max(range(bs.n), key=lambda i: bs.domains[i].nx * bs.domains[i].ny * bs.domains[i].nz)
+    roofline = profile_roofline(lib, bs.handles[big], stream, False, f"{args.workload}:batch")
+    if roofline:
+        d = bs.domains[big]
+        roofline["profiled_subdomain"] = [d.nx, d.ny, d.nz]
+    iters = [s["iterations"] for s in stats]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {bs.n} subdomains, nx,ny in {wl['nxy'][0]}..{wl['nxy'][1]} "
+                                   f"step {wl['nxy'][2]}, nz in {wl['nz'][0]}..{wl['nz'][1]} step {wl['nz'][2]}, "
+                                   f"{bs.cells} cells, {wl['n_hills']} hills each, adv_den={wl['adv_den']}",
+                       "solver": "batched mg (one graph launch per step)", "tol_rel": TOL, "fields": "f32",
+                       "krylov": "f64", "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms,
+                       "sequential_solves_per_s": bs.n / (seq_ms / 1000.0), "iterations_min": min(iters),
+                       "iterations_max": max(iters), "statuses": sorted(set(s["status"] for s in stats)),
+                       "l2": "inputs larger than L2 (coefficients of all subdomains)",
+                       "parallelism": f"{world} ranks x {bs.n} subdomains" if world > 1 else "1 GPU"},
+            "roofline": roofline, "cpu_baseline": None,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+            "clocks": clocks, "gpu_launches": int(launches)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bs.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,6 +565,14 @@ def main():
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if "batch" in wl:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batch workload has no CPU reference arm; "
+                                                                  "its subdomains are timed one by one on the GPU "
+                                                                  "(config.sequential_solves_per_s)"}))
+            return
+        run_batch(args, wl)
+        return
     if args.impl == "reference":
         if args.ref_iters is None:
             args.ref_iters = REF_ITERS[args.workload]

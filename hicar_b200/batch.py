@@ -19,18 +19,16 @@ def _torch():
 def subdomain_cases(n: int, seed: int = 0, nxy=(96, 512, 32), nz=(20, 48, 4), n_hills: int = 20, dx: float = 250.0):
     """n seeded subdomains with nx, ny drawn from range(*nxy) and nz from
     range(*nz), inclusive of the upper bound (the 96-subdomain batch workload:
-    nx, ny in 96..512 step 32, nz in 20..48 step 4)."""
+    nx, ny in 96..512 step 32, nz in 20..48 step 4).  Yields the cases."""
     import numpy as np
 
     from . import cases
     rng = np.random.default_rng(seed)
     xy = np.arange(nxy[0], nxy[1] + 1, nxy[2])
     zz = np.arange(nz[0], nz[1] + 1, nz[2])
-    out = []
-    for i in range(n):
-        out.append(cases.build_case(int(rng.choice(xy)), int(rng.choice(xy)), int(rng.choice(zz)), dx, n_hills,
-                                    seed=seed * 100003 + i, adv_den=True))
-    return out
+    shapes = [(int(rng.choice(xy)), int(rng.choice(xy)), int(rng.choice(zz))) for _ in range(n)]
+    for i, (nx, ny, nzz) in enumerate(shapes):  # a generator: one case on the host at a time
+        yield cases.build_case(nx, ny, nzz, dx, n_hills, seed=seed * 100003 + i, adv_den=True)
 
 
 class BatchSolver:

@@ -1588,8 +1588,8 @@ extern "C" int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *i
     if (!b || !items) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int n = (int)b->hs.size();
-    const int lane_c[] = {1, 2, 4, 8, 16, 32, 64};
-    const int chunk_c[] = {2, 4, 8};
+    const int lane_c[] = {1, 4, 16, 64};
+    const int chunk_c[] = {4, 8};
     double best = 1e300;
     int bl = b->lanes, bc = b->chunk;
     for (int lc : lane_c) {

@@ -267,8 +267,8 @@ int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *chunk);
  * solution, as calc_iter_winds) and correct its winds; stats: n entries (or NULL). */
 int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold, void *stream,
                                  hicarw_stats *stats);
-/* Time cold solves (winds untouched) for lanes in {1,2,4,...,64} and chunk in
- * {2,4,8}, keep the fastest configuration; *best_ms its batch time. */
+/* Time cold solves (winds untouched) for lanes in {1, 4, 16, 64} (at most n) and
+ * chunk in {4, 8}, keep the fastest configuration; *best_ms its batch time. */
 int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, void *stream, double *best_ms);
 
 /* Number of kernels this library has launched since load (graph nodes included). */

@@ -74,7 +74,7 @@ def test_batch_autotune(solver):
     best = bs.autotune()
     lanes, chunk = bs.config()
     assert best > 0.0
-    assert lanes in (1, 2, 4) and chunk in (2, 4, 8)
+    assert lanes in (1, 4) and chunk in (4, 8)
     stats = bs.step()
     assert all(s["status"] == 0 for s in stats)
     st, lam, _ = _single(bs, 3)
