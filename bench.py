@@ -54,7 +54,8 @@ WORKLOADS = {
 # seed-1 case, measured by running it to convergence on the host (plain512:
 # 912 iterations, 136 s on 8 cores); the CPU sample extrapolates one solve
 # from these.
-REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": None, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
+# mixed1024: 1245, the count of the same method (plain BiCGStab, FP64 Krylov) on the GPU.
+REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
@@ -266,6 +267,40 @@ def profile_roofline(lib, h, stream, ncu_range: bool, traffic_key: str):
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
 
 
+def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, solver):
+    """Relative L2 differences of lambda and u/v/w between one solve of `solver`
+    (tolerance TOL) and a tight FP64 solve of the same system (FGMRES + V-cycle to
+    1e-11), and the final divergence of both corrected wind fields relative to the
+    input divergence."""
+    import torch
+    from hicar_b200 import _capi
+
+    def solve_with(opt):
+        wi.set_options(opt)
+        dom.set_winds(u0, v0, w0)
+        lib.hicarw_reset_solution(h, stream.cuda_stream)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        d0 = float(div.double().norm())
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
+        lam = torch.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2), dtype=torch.float64, device=div.device)
+        lib.hicarw_get_lambda(h, lam.data_ptr(), _capi.MEM_DEVICE, stream.cuda_stream)
+        winds = [a.clone() for a in (dom.u_dqdt, dom.v_dqdt, dom.w_dqdt)]
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        return st, lam, winds, float(div.double().norm()) / d0
+
+    st_a, lam_a, w_a, div_a = solve_with(solver_options(solver))
+    tight = solver_options("fgmres")
+    tight.tol_rel, tight.wind_solver_iterations, tight.stall_iters = 1e-11, 6000, 0
+    st_t, lam_t, w_t, div_t = solve_with(tight)
+
+    def rel(a, b):
+        return float((a.double() - b.double()).norm() / b.double().norm())
+
+    return {"reference_solve": "FGMRES(30) + V-cycle, FP64, 1e-11 relative", "reference_iterations": st_t["iterations"],
+            "lambda_rel_l2": rel(lam_a, lam_t), "u_rel_l2": rel(w_a[0], w_t[0]), "v_rel_l2": rel(w_a[1], w_t[1]),
+            "w_rel_l2": rel(w_a[2], w_t[2]), "final_div_rel": div_a, "final_div_rel_reference": div_t}
+
+
 def run_ours(args, wl):
     import ctypes as C
 
@@ -299,7 +334,13 @@ def run_ours(args, wl):
     dom.set_winds(u0, v0, w0)
     lib.hicarw_reset_solution(h, stream.cuda_stream)
     wind.calc_divergence(div, dom, use_dqdt=True)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    p0.record()
     ref_stats = wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
+    p1.record()
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)  # one plain GPU BiCGStab solve (reference method), for the speed-up
     ref_iters = ref_stats["iterations"]
     opt = solver_options(args.solver)
     wi.set_options(opt)
@@ -387,6 +428,12 @@ def run_ours(args, wl):
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
     roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", f"{args.workload}:{args.solver}")
 
+    # ---- accuracy: this solver's lambda / winds / final divergence against a tight FP64 solve ----
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, args.solver)
+        wi.set_options(opt)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         coefs = np.empty((15, dom.ny, dom.nz, dom.nx), np.float32)
@@ -404,6 +451,8 @@ def run_ours(args, wl):
                                    f"{wl['n_hills']} hills, alpha={wl['alpha']}, adv_den={wl['adv_den']}",
                        "solver": args.solver, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
                        "iterations": it[0], "ref_method_iterations": ref_iters, "true_res_rel": max(tr),
+                       "plain_gpu_solves_per_s": 1000.0 / plain_ms,
+                       "speedup_vs_plain_gpu": value / world / (1000.0 / plain_ms), "accuracy": accuracy,
                        "l2": "inputs larger than L2 (15 FP32 coefficient arrays, 0.8 GB)",
                        "parallelism": f"{world} independent subdomains" if world > 1 else "1 GPU"},
             "roofline": roofline, "cpu_baseline": cpu,
@@ -549,13 +598,16 @@ def run_batch(args, wl):
 
 
 def main():
+    global TOL
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain512", choices=sorted(WORKLOADS))
-    ap.add_argument("--solver", default="plain", choices=["plain", "mg", "fgmres", "fgmres_jacobi", "learned"])
+    ap.add_argument("--workload", default="mixed1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--solver", default="mg", choices=["plain", "mg", "fgmres", "fgmres_jacobi", "learned"])
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the tight-solve accuracy report")
+    ap.add_argument("--tol", type=float, default=TOL, help="relative residual tolerance of the timed solves")
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")
@@ -564,6 +616,7 @@ def main():
                     help="bracket the first timed step or the per-kernel profiling pass with "
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
+    TOL = args.tol
     wl = WORKLOADS[args.workload]
     if "batch" in wl:
         if args.impl == "reference":
