@@ -471,6 +471,7 @@ def run_batch(args, wl):
     MG-preconditioned BiCGStab in one graph launch, wind correction)."""
     import ctypes as C
 
+    import numpy as np
     import torch
     from hicar_b200 import _capi
     from hicar_b200.batch import BatchSolver, subdomain_cases
@@ -500,11 +501,13 @@ def run_batch(args, wl):
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record()
     st = _capi.Stats()
+    seq_each = []
     for i, (h, dom) in enumerate(zip(bs.handles, bs.domains)):
         lib.hicarw_reset_solution(h, C.c_void_p(bs.stream))
         _capi.check(lib.hicarw_calc_iter_winds(h, ptr(dom.wind_alpha), ptr(bs.divs[i]), ptr(dom.density), 1,
                                                ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt), _capi.MEM_DEVICE,
                                                C.c_void_p(bs.stream), C.byref(st)), h)
+        seq_each.append(st.solve_ms)
     q1.record()
     torch.cuda.synchronize()
     seq_ms = q0.elapsed_time(q1)
@@ -574,6 +577,14 @@ def run_batch(args, wl):
         d = bs.domains[big]
         roofline["profiled_subdomain"] = [d.nx, d.ny, d.nz]
     iters = [s["iterations"] for s in stats]
+    bs.step()
+    lat = bs.latencies()
+    seq_lat = np.asarray(seq_each)
+    latency = {"batched_p50_ms": float(np.percentile(lat, 50)), "batched_p99_ms": float(np.percentile(lat, 99)),
+               "batched_max_ms": float(lat.max()), "sequential_p50_ms": float(np.percentile(seq_lat, 50)),
+               "sequential_p99_ms": float(np.percentile(seq_lat, 99)),
+               "note": "batched: completion time of each solve from the start of the batch graph; sequential: "
+                       "each subdomain's own calc_iter_winds"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -584,6 +595,7 @@ def run_batch(args, wl):
                        "krylov": "f64", "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms,
                        "sequential_solves_per_s": bs.n / (seq_ms / 1000.0), "iterations_min": min(iters),
                        "iterations_max": max(iters), "statuses": sorted(set(s["status"] for s in stats)),
+                       "latency": latency,
                        "l2": "inputs larger than L2 (coefficients of all subdomains)",
                        "parallelism": f"{world} ranks x {bs.n} subdomains" if world > 1 else "1 GPU"},
             "roofline": roofline, "cpu_baseline": None,

@@ -34,7 +34,7 @@ EXPORTS = [
     "hicarw_unet_features", "hicarw_unet_forward", "hicarw_unet_backward", "hicarw_unet_backward_residual",
     "hicarw_unet_adam_step", "hicarw_unet_apply", "hicarw_set_learned_precond",
     "hicarw_batch_create", "hicarw_batch_destroy", "hicarw_batch_config", "hicarw_batch_get_config",
-    "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune",
+    "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune", "hicarw_batch_latencies",
 ]
 
 
@@ -140,6 +140,7 @@ def load(path: str = LIB_PATH):
         "hicarw_batch_get_config": (ci, [vp, P(ci), P(ci)]),
         "hicarw_batch_calc_iter_winds": (ci, [vp, P(BatchItem), ci, ci, vp, P(Stats)]),
         "hicarw_batch_autotune": (ci, [vp, P(BatchItem), ci, vp, P(C.c_double)]),
+        "hicarw_batch_latencies": (ci, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -123,6 +123,13 @@ class BatchSolver:
                                                    C.byref(best)))
         return best.value
 
+    def latencies(self):
+        """Per-subdomain solve latency (ms from the batch start) of the last solve."""
+        import numpy as np
+        out = np.zeros(self.n)
+        _capi.check(self.lib.hicarw_batch_latencies(self.batch, out.ctypes.data))
+        return out
+
     def lambda_of(self, i: int):
         torch = _torch()
         d = self.domains[i]

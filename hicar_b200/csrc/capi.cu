@@ -1317,12 +1317,36 @@ struct hicarw_batch {
     std::vector<hicarw_batch_item> built;
     int built_lanes = -1, built_chunk = -1, built_cold = -1;
     int *counters = nullptr; // device: WHILE-body executions per subdomain
+    unsigned long long *stamps = nullptr; // device: %globaltimer at each solve's end, [n] = batch start
     cudaStream_t cap = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     float last_ms = 0.0f;
 };
 
 __global__ void batch_count_reset_kernel(int *count) { *count = 0; }
+
+__global__ void batch_stamp_kernel(unsigned long long *slot)
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *slot = t;
+}
+
+// a child-graph node holding one timestamp kernel
+static cudaError_t batch_stamp_node(hicarw_batch *b, cudaGraph_t g, const cudaGraphNode_t *dep, int ndep,
+                                    unsigned long long *slot, cudaGraphNode_t *out)
+{
+    cudaGraph_t sg;
+    cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    batch_stamp_kernel<<<1, 1, 0, b->cap>>>(slot);
+    count_launch(1);
+    e = cudaStreamEndCapture(b->cap, &sg);
+    if (e != cudaSuccess) return e;
+    e = cudaGraphAddChildGraphNode(out, g, dep, ndep, sg);
+    cudaGraphDestroy(sg);
+    return e;
+}
 
 __global__ void batch_cond_kernel(cudaGraphConditionalHandle hc, const SolveState *st, int *count, int limit)
 {
@@ -1382,7 +1406,9 @@ static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold
     cudaGraph_t g;
     BCK(cudaGraphCreate(&g, 0));
     long long nodes = 0;
-    cudaError_t e = cudaSuccess;
+    cudaGraphNode_t root;
+    cudaError_t e = batch_stamp_node(b, g, nullptr, 0, b->stamps + n, &root);
+    for (int L = 0; L < lanes; L++) tail[L] = root;
     for (int oi = 0; oi < n && e == cudaSuccess; oi++) {
         const int i = order[oi];
         hicarw_handle *h = b->hs[i];
@@ -1402,7 +1428,7 @@ static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold
         if (e != cudaSuccess) break;
         nodes += g_capture_nodes;
         cudaGraphNode_t sn, wn;
-        e = cudaGraphAddChildGraphNode(&sn, g, tail[L] ? &tail[L] : nullptr, tail[L] ? 1 : 0, sg);
+        e = cudaGraphAddChildGraphNode(&sn, g, &tail[L], 1, sg);
         cudaGraphDestroy(sg);
         if (e != cudaSuccess) break;
         // the device-driven loop
@@ -1429,7 +1455,10 @@ static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold
         e = cudaStreamEndCapture(b->cap, &body);
         g_capturing = 0;
         nodes += g_capture_nodes;
-        tail[L] = wn;
+        if (e != cudaSuccess) break;
+        cudaGraphNode_t tn;
+        e = batch_stamp_node(b, g, &wn, 1, b->stamps + i, &tn);
+        tail[L] = tn;
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
     cudaGraphDestroy(g);
@@ -1530,6 +1559,7 @@ extern "C" int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_
     hicarw_batch *b = new hicarw_batch();
     b->hs.assign(handles, handles + n);
     if (cudaMalloc((void **)&b->counters, n * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&b->stamps, (n + 1) * sizeof(unsigned long long)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) {
         delete b;
@@ -1546,6 +1576,7 @@ extern "C" int hicarw_batch_destroy(hicarw_batch *b)
     cudaDeviceSynchronize();
     batch_drop_graph(b);
     if (b->counters) cudaFree(b->counters);
+    if (b->stamps) cudaFree(b->stamps);
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->t0) cudaEventDestroy(b->t0);
     if (b->t1) cudaEventDestroy(b->t1);
@@ -1578,6 +1609,18 @@ extern "C" int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_
             (adv_den && !items[i].density))
             return HICARW_ERR_ARG;
     return batch_run(b, items, adv_den, cold, 1, (cudaStream_t)stream, stats);
+}
+
+// Per-subdomain solve latency of the last batched call: milliseconds from the
+// start of the batch graph to the end of that subdomain's solve loop.
+extern "C" int hicarw_batch_latencies(hicarw_batch *b, double *ms)
+{
+    if (!b || !ms || !b->exec) return HICARW_ERR_ARG;
+    const int n = (int)b->hs.size();
+    std::vector<unsigned long long> t(n + 1);
+    BCK(cudaMemcpy(t.data(), b->stamps, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) ms[i] = t[i] >= t[n] ? (double)(t[i] - t[n]) * 1e-6 : 0.0;
+    return HICARW_OK;
 }
 
 // Autotuner: time cold batched solves (no wind correction) for every (lanes,

@@ -267,6 +267,9 @@ int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *chunk);
  * solution, as calc_iter_winds) and correct its winds; stats: n entries (or NULL). */
 int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold, void *stream,
                                  hicarw_stats *stats);
+/* Per-subdomain latency of the last batched call (n entries): ms from the start of
+ * the batch graph to the end of that subdomain's solve loop (%globaltimer). */
+int hicarw_batch_latencies(hicarw_batch *b, double *ms);
 /* Time cold solves (winds untouched) for lanes in {1, 4, 16, 64} (at most n) and
  * chunk in {4, 8}, keep the fastest configuration; *best_ms its batch time. */
 int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, void *stream, double *best_ms);

@@ -57,6 +57,8 @@ def test_batch_matches_single_solves(solver, lanes, chunk):
     bs.configure(lanes, chunk)
     stats = bs.step()
     lam_b = [bs.lambda_of(i).cpu() for i in range(bs.n)]
+    lat = bs.latencies()
+    assert (lat > 0).all() and np.isfinite(lat).all()
     winds_b = [[a.clone().cpu() for a in (d.u_dqdt, d.v_dqdt, d.w_dqdt)] for d in bs.domains]
     for i in range(bs.n):
         st, lam, winds = _single(bs, i)
