@@ -273,3 +273,57 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, batch: int = 4, seed: 
         net.adam_step(lr)
         hist.append(tot / batch)
     return hist
+
+
+def conv_benchmark(cin: int, cout: int, nx: int, ny: int, nz: int, reps: int = 5, seed: int = 0):
+    """Time the tensor-core convolution (forward) on random act-layout data:
+    returns ms per call, achieved TFLOP/s (54 cin cout flop per cell) and GB/s
+    (2 (cin + cout) bytes per cell)."""
+    torch = _torch()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = act_empty(nx, ny, nz, cin)
+    x[1:ny + 1, 1:nz + 1, :, 1:nx + 1, :] = torch.randn((ny, nz, cin // 8, nx, 8), generator=g, device="cuda").to(
+        torch.bfloat16)
+    w = torch.randn((27, cin, cout), generator=g, device="cuda") * (2.0 / (27 * cin)) ** 0.5
+    b = torch.zeros(cout, device="cuda")
+    out = act_empty(nx, ny, nz, cout)
+    lib = _capi.load()
+    s = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        rc = lib.hicarw_nn_conv3(cin, cout, nx, ny, nz, _ptr(x), _ptr(w), _ptr(b), None, None, 1, 0, _ptr(out), None,
+                                 C.c_void_p(s))
+        if rc != 0:
+            raise RuntimeError(f"hicarw_nn_conv3 failed ({rc})")
+
+    call()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    cells = nx * ny * nz
+    return {"cin": cin, "cout": cout, "grid": [nx, ny, nz], "ms": ms,
+            "tflops": 54.0 * cin * cout * cells / (ms * 1e-3) / 1e12,
+            "gbs": 2.0 * (cin + cout) * cells / (ms * 1e-3) / 1e9}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="time the tensor-core convolution")
+    ap.add_argument("--cin", type=int, default=16)
+    ap.add_argument("--cout", type=int, default=16)
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=48)
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args(argv)
+    print(json.dumps(conv_benchmark(a.cin, a.cout, a.nx, a.ny, a.nz, a.reps)))
+
+
+if __name__ == "__main__":
+    main()
