@@ -35,6 +35,8 @@ EXPORTS = [
     "hicarw_unet_adam_step", "hicarw_unet_apply", "hicarw_set_learned_precond",
     "hicarw_batch_create", "hicarw_batch_destroy", "hicarw_batch_config", "hicarw_batch_get_config",
     "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune", "hicarw_batch_latencies",
+    "hicarw_calc_w_real", "hicarw_calc_idealized_wgrid", "hicarw_balance_uvw", "hicarw_calc_alpha",
+    "hicarw_smooth_alpha",
 ]
 
 
@@ -141,6 +143,11 @@ def load(path: str = LIB_PATH):
         "hicarw_batch_calc_iter_winds": (ci, [vp, P(BatchItem), ci, ci, vp, P(Stats)]),
         "hicarw_batch_autotune": (ci, [vp, P(BatchItem), ci, vp, P(C.c_double)]),
         "hicarw_batch_latencies": (ci, [vp, vp]),
+        "hicarw_calc_w_real": (ci, [vp, vp, vp, vp, vp, ci, vp]),
+        "hicarw_calc_idealized_wgrid": (ci, [vp, vp, vp, vp, vp, ci, vp]),
+        "hicarw_balance_uvw": (ci, [vp, vp, vp, vp, vp, ci, ci, ci, vp]),
+        "hicarw_calc_alpha": (ci, [vp, vp, vp, ci, ci, vp]),
+        "hicarw_smooth_alpha": (ci, [vp, vp, ci, ci, ci, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -121,6 +121,7 @@ struct hicarw_handle {
     // staging for host pointers
     float *su = nullptr, *sv = nullptr, *sw = nullptr, *sT = nullptr, *srho = nullptr, *sdiv = nullptr;
     float *sprobe_u = nullptr, *sprobe_v = nullptr, *sprobe_w = nullptr;
+    float *swork = nullptr; // cell-sized scratch of balance_uvw (divergence) and smooth_alpha (ping-pong)
     int structure_uploaded = 0, operator_probed = 0, precond_n_sweeps = 2;
     std::map<GraphKey, GraphRec> graphs;
     FusedBufs fb;
@@ -332,7 +333,7 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     void *ptrs[] = {h->mjac, h->mju, h->mjv, h->mjw, h->mdzdx, h->mdzdy, h->mdzdx_u, h->mdzdy_v, h->madz, h->mnterr,
                     h->mf[0], h->mf[1], h->mf[2], h->mf[3], h->mf[4], h->dz_if, h->dzdx_surf, h->dzdy_surf, h->adz_col,
                     h->alpha, h->div, h->coef, h->bc, h->st, h->hist, h->partials, h->scan, h->su, h->sv, h->sw,
-                    h->sT, h->srho, h->sdiv, h->sprobe_u, h->sprobe_v, h->sprobe_w};
+                    h->sT, h->srho, h->sdiv, h->sprobe_u, h->sprobe_v, h->sprobe_w, h->swork};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int q = 0; q < NVEC; q++)
@@ -1288,6 +1289,73 @@ extern "C" int hicarw_set_learned_precond(hicarw_handle *h, hicarw_unet *n)
     }
     h->unet = n;
     h->unet_dirty = 1;
+    return HICARW_OK;
+}
+
+// ---- the steps either side of the solve in update_winds (wind.F90) --------------
+// Device pointers, caller (Fortran) layouts; stream-ordered, no host sync.
+static int device_only(int mem_kind) { return mem_kind == HICARW_MEM_DEVICE ? 0 : HICARW_ERR_ARG; }
+
+static int ensure_work(hicarw_handle *h)
+{
+    if (!h->swork) CK(cudaMalloc((void **)&h->swork, n_cell(h->d) * 4));
+    return 0;
+}
+
+extern "C" int hicarw_calc_w_real(hicarw_handle *h, const float *u, const float *v, const float *w_grid, float *w_real,
+                                  int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !w_real || device_only(mem_kind)) return HICARW_ERR_ARG;
+    launch_w_real(h->d, metrics_of(h), u, v, w_grid, w_real, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_calc_idealized_wgrid(hicarw_handle *h, const float *u, const float *v, const float *w_real,
+                                           float *w, int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !w_real || !w || device_only(mem_kind)) return HICARW_ERR_ARG;
+    launch_idealized_wgrid(h->d, metrics_of(h), u, v, w_real, w, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_balance_uvw(hicarw_handle *h, const float *u, const float *v, const float *density, float *w,
+                                  int adv_den, int use_dqdt, int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !w || (adv_den && !density) || device_only(mem_kind)) return HICARW_ERR_ARG;
+    int rc;
+    if ((rc = ensure_work(h)) != 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Metrics m = metrics_of(h);
+    launch_divergence(h->d, m, u, v, w, adv_den ? density : nullptr, h->swork, adv_den, 1, use_dqdt, s);
+    launch_calc_w(h->d, m, h->swork, adv_den ? density : nullptr, w, adv_den, s);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *alpha, int halo, int mem_kind,
+                                 void *stream)
+{
+    if (!h || !froude || !alpha || halo < 0 || 2 * halo >= h->d.nx || 2 * halo >= h->d.ny || device_only(mem_kind))
+        return HICARW_ERR_ARG;
+    launch_calc_alpha(h->d, froude, alpha, halo, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_smooth_alpha(hicarw_handle *h, float *alpha, int window, int nsmooths, int mem_kind,
+                                   void *stream)
+{
+    if (!h || !alpha || window < 0 || nsmooths < 0 || device_only(mem_kind)) return HICARW_ERR_ARG;
+    int rc;
+    if ((rc = ensure_work(h)) != 0) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int p = 0; p < nsmooths; p++) {
+        CK(cudaMemcpyAsync(h->swork, alpha, n_cell(h->d) * 4, cudaMemcpyDeviceToDevice, s));
+        launch_smooth_xy(h->d, h->swork, alpha, window, s);
+    }
+    CK(cudaGetLastError());
     return HICARW_OK;
 }
 

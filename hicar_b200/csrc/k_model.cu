@@ -507,3 +507,187 @@ void launch_scan_inputs(long long n, const float *div, const float *alpha, unsig
 }
 
 }  // namespace hw
+
+namespace hw {
+
+// ---------------------------------------------------------------------------
+// The steps either side of the solve in update_winds (wind.F90), caller layouts,
+// 1-based indices, Fortran's left-to-right FP32 order (this unit: -fmad=false).
+// ---------------------------------------------------------------------------
+// calc_w_real (wind.F90:1175-1227) at cell (i, k, j); w_grid may be null (zero)
+__device__ __forceinline__ float w_real_at(const Dims &d, const Metrics &m, const float *u, const float *v,
+                                           const float *w_grid, int i, int k, int j)
+{
+    const long long c = cidx(d, i, k, j);
+    float lo = 0.0f, hi = 0.0f;
+    if (w_grid) {
+        hi = w_grid[c] * m.jw[c];
+        if (k > 1) lo = w_grid[cidx(d, i, k - 1, j)] * m.jw[cidx(d, i, k - 1, j)];
+    }
+    const long long u0 = uidx(d, i, k, j), u1 = uidx(d, i + 1, k, j);
+    const long long v0 = cidx(d, i, k, j), v1 = cidx(d, i, k, j + 1);
+    return (u[u0] * m.dzdx_u[u0] + u[u1] * m.dzdx_u[u1]) * 0.5f + (v[v0] * m.dzdy_v[v0] + v[v1] * m.dzdy_v[v1]) * 0.5f +
+           (lo + hi) * 0.5f;
+}
+
+__global__ void w_real_kernel(Dims d, Metrics m, const float *__restrict__ u, const float *__restrict__ v,
+                              const float *__restrict__ w_grid, float *__restrict__ w_real)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int k = blockIdx.y + 1;
+    int j = blockIdx.z + 1;
+    if (i > d.nx) return;
+    w_real[cidx(d, i, k, j)] = w_real_at(d, m, u, v, w_grid, i, k, j);
+}
+
+// calc_idealized_wgrid (wind.F90:940-998): one thread per column
+__global__ void idealized_wgrid_kernel(Dims d, Metrics m, const float *__restrict__ u, const float *__restrict__ v,
+                                       const float *__restrict__ w_real_field, float *__restrict__ w)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int j = blockIdx.y + 1;
+    if (i > d.nx) return;
+    float cur = w_real_field[cidx(d, i, 1, j)] - w_real_at(d, m, u, v, nullptr, i, 1, j);
+    for (int k = 1; k <= d.nz - 1; k++) {
+        const long long c = cidx(d, i, k, j), cp = cidx(d, i, k + 1, j);
+        const float nxt = w_real_field[cp] - w_real_at(d, m, u, v, nullptr, i, k + 1, j);
+        float wk = (cur * m.adz[cp] + nxt * m.adz[c]) / (m.adz[c] + m.adz[cp]);
+        w[c] = wk / m.jw[c];
+        cur = nxt;
+    }
+    w[cidx(d, i, d.nz, j)] = 0.0f;
+}
+
+// calc_w (wind.F90:201-248): upward integration of the horizontal divergence per column
+__global__ void calc_w_kernel(Dims d, Metrics m, const float *__restrict__ div, const float *__restrict__ rho,
+                              float *__restrict__ w, int adv_den)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int j = blockIdx.y + 1;
+    if (i > d.nx) return;
+    const int nz = d.nz;
+    float w_prev = 0.0f, rho_prev = 0.0f, jw_prev = 0.0f;
+    for (int k = 1; k <= nz; k++) {
+        const long long c = cidx(d, i, k, j);
+        const float dz = m.adz[c], jw = m.jw[c], dv = div[c];
+        float wk;
+        if (adv_den) {
+            float rho_i;
+            if (k < nz) {
+                const long long cp = cidx(d, i, k + 1, j);
+                rho_i = (rho[c] * m.adz[cp] + rho[cp] * dz) / (dz + m.adz[cp]);
+            } else rho_i = rho[c];
+            if (k == 1) wk = 0.0f - dv * dz / (jw * rho_i);
+            else wk = ((w_prev * rho_prev * jw_prev) - dv * dz) / (jw * rho_i);
+            rho_prev = rho_i;
+        } else {
+            if (k == 1) wk = (0.0f - dv * dz) / (jw);
+            else wk = (w_prev * jw_prev - dv * dz) / (jw);
+        }
+        w[c] = wk;
+        w_prev = wk;
+        jw_prev = jw;
+    }
+}
+
+// calc_alpha (wind.F90:1102-1173), elementwise part; (1/Fr)**4 as (t*t)*(t*t)
+__global__ void calc_alpha_kernel(Dims d, const float *__restrict__ froude, float *__restrict__ alpha)
+{
+    const long long n = (long long)d.nx * d.nz * d.ny;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const float t = 1.0f / froude[q];
+        const float t2 = t * t;
+        const float p = t2 * t2;
+        const float mx = p > 0.00001f ? p : 0.00001f;
+        float a = 1.0f - 0.5f * mx * (sqrtf(1.0f + 4.0f / mx) - 1.0f);
+        a = sqrtf(a > 0.00001f ? a : 0.00001f);
+        a = a > 0.2f ? a : 0.2f;
+        a = a < 2.0f ? a : 2.0f;
+        const int k = (int)((q / d.nx) % d.nz) + 1;
+        alpha[q] = k == d.nz ? 0.2f : a;
+    }
+}
+
+// one of the four boundary copies of calc_alpha: side 0 south (j <= h), 1 west
+// (i <= h), 2 north (j > ny - h), 3 east (i > nx - h); whole columns
+__global__ void alpha_edge_kernel(Dims d, float *__restrict__ alpha, int h, int side)
+{
+    const int ni = (side == 1 || side == 3) ? h : d.nx, nj = (side == 0 || side == 2) ? h : d.ny;
+    const long long n = (long long)ni * nj * d.nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int a = (int)(q % ni) + 1;
+        long long r = q / ni;
+        int k = (int)(r % d.nz) + 1, b = (int)(r / d.nz) + 1;
+        int i = a, j = b, is = a, js = b;
+        if (side == 0) js = h + 1;
+        else if (side == 1) is = h + 1;
+        else if (side == 2) { j = d.ny - h + b; js = d.ny - h; }
+        else { i = d.nx - h + a; is = d.nx - h; }
+        alpha[cidx(d, i, k, j)] = alpha[cidx(d, is, k, js)];
+    }
+}
+
+// one pass of smooth_array_3d, ydim = 3 (array_utilities.F90:322-397): x-y box
+// mean with clamped indices, double sum (y offset outer, x inner)
+__global__ void smooth_xy_kernel(Dims d, const float *__restrict__ in, float *__restrict__ out, int w)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int k = blockIdx.y + 1;
+    int j = blockIdx.z + 1;
+    if (i > d.nx) return;
+    double cur = 0.0;
+    for (int dj = -w; dj <= w; dj++) {
+        const int jj = j + dj < 1 ? 1 : (j + dj > d.ny ? d.ny : j + dj);
+        for (int di = -w; di <= w; di++) {
+            const int ii = i + di < 1 ? 1 : (i + di > d.nx ? d.nx : i + di);
+            cur = cur + (double)in[cidx(d, ii, k, jj)];
+        }
+    }
+    const int nc = 2 * w + 1;
+    out[cidx(d, i, k, j)] = (float)(cur / (double)(nc * nc));
+}
+
+void launch_w_real(const Dims &d, const Metrics &m, const float *u, const float *v, const float *w_grid, float *w_real,
+                   cudaStream_t st)
+{
+    dim3 b(128), g((d.nx + 127) / 128, d.nz, d.ny);
+    w_real_kernel<<<g, b, 0, st>>>(d, m, u, v, w_grid, w_real);
+    count_launch(1);
+}
+
+void launch_idealized_wgrid(const Dims &d, const Metrics &m, const float *u, const float *v, const float *w_real_field,
+                            float *w, cudaStream_t st)
+{
+    dim3 b(64), g((d.nx + 63) / 64, d.ny);
+    idealized_wgrid_kernel<<<g, b, 0, st>>>(d, m, u, v, w_real_field, w);
+    count_launch(1);
+}
+
+void launch_calc_w(const Dims &d, const Metrics &m, const float *div, const float *rho, float *w, int adv_den,
+                   cudaStream_t st)
+{
+    dim3 b(64), g((d.nx + 63) / 64, d.ny);
+    calc_w_kernel<<<g, b, 0, st>>>(d, m, div, rho, w, adv_den);
+    count_launch(1);
+}
+
+void launch_calc_alpha(const Dims &d, const float *froude, float *alpha, int halo, cudaStream_t st)
+{
+    const long long n = (long long)d.nx * d.nz * d.ny;
+    calc_alpha_kernel<<<(int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16), 256, 0, st>>>(d, froude, alpha);
+    count_launch(1);
+    if (halo > 0)
+        for (int side = 0; side < 4; side++) {
+            alpha_edge_kernel<<<148, 256, 0, st>>>(d, alpha, halo, side);
+            count_launch(1);
+        }
+}
+
+void launch_smooth_xy(const Dims &d, const float *in, float *out, int w, cudaStream_t st)
+{
+    dim3 b(128), g((d.nx + 127) / 128, d.nz, d.ny);
+    smooth_xy_kernel<<<g, b, 0, st>>>(d, in, out, w);
+    count_launch(1);
+}
+
+}  // namespace hw

@@ -26,6 +26,14 @@ template <typename V>
 void launch_probe_pattern(const Dims &d, V *x, int ca, int cb, int cc, cudaStream_t st);
 void launch_probe_record(const Dims &d, const float *T, float *coef, int ca, int cb, int cc, unsigned int *leak,
                          cudaStream_t st);
+void launch_w_real(const Dims &d, const Metrics &m, const float *u, const float *v, const float *w_grid, float *w_real,
+                   cudaStream_t st);
+void launch_idealized_wgrid(const Dims &d, const Metrics &m, const float *u, const float *v, const float *w_real_field,
+                            float *w, cudaStream_t st);
+void launch_calc_w(const Dims &d, const Metrics &m, const float *div, const float *rho, float *w, int adv_den,
+                   cudaStream_t st);
+void launch_calc_alpha(const Dims &d, const float *froude, float *alpha, int halo, cudaStream_t st);
+void launch_smooth_xy(const Dims &d, const float *in, float *out, int w, cudaStream_t st);
 void launch_module_vars(const Dims &d, const float *adz, const float *dzdx, const float *dzdy, const float *nterr,
                         float *dz_if, float *dzdx_surf, float *dzdy_surf, float *adz_col, cudaStream_t st);
 void launch_coefs(const Dims &d, const Metrics &m, const float *alpha, float *coef, int mode, cudaStream_t st);

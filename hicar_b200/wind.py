@@ -78,3 +78,41 @@ def update_winds_iterative(domain: DeviceDomain, options: wi.WindOptions, div) -
 
 def reset() -> None:
     _operator_calibrated.clear()
+
+
+# ---- the steps either side of the solve (device arrays) ----------------------
+def _s():
+    return wi._stream[0]
+
+
+def calc_w_real(domain: DeviceDomain, u, v, w_grid, w_real) -> None:
+    """calc_w_real (wind.F90:1175-1227) with jaco = jacobian_w; w_grid None = zero."""
+    h = wi.handle(domain.nest_indx)
+    _capi.check(_capi.load().hicarw_calc_w_real(h, ptr(u), ptr(v), ptr(w_grid) if w_grid is not None else None,
+                                                ptr(w_real), _capi.MEM_DEVICE, _s()), h)
+
+
+def calc_idealized_wgrid(domain: DeviceDomain, w_real) -> None:
+    """calc_idealized_wgrid (wind.F90:940-998): domain.w_dqdt from the dqdt winds and w_real."""
+    h = wi.handle(domain.nest_indx)
+    _capi.check(_capi.load().hicarw_calc_idealized_wgrid(h, ptr(domain.u_dqdt), ptr(domain.v_dqdt), ptr(w_real),
+                                                         ptr(domain.w_dqdt), _capi.MEM_DEVICE, _s()), h)
+
+
+def balance_uvw(domain: DeviceDomain, adv_den: bool, update: bool = False) -> None:
+    """balance_uvw (wind.F90:123-199): w (dqdt winds if update, else data winds)
+    from the horizontal divergence of u and v."""
+    h = wi.handle(domain.nest_indx)
+    u, v, w = (domain.u_dqdt, domain.v_dqdt, domain.w_dqdt) if update else (domain.u, domain.v, domain.w)
+    _capi.check(_capi.load().hicarw_balance_uvw(h, ptr(u), ptr(v), ptr(domain.density), ptr(w), int(bool(adv_den)),
+                                                int(bool(update)), _capi.MEM_DEVICE, _s()), h)
+
+
+def calc_alpha(domain: DeviceDomain, froude, halo: int = 1, window: int = 2, nsmooths: int = 3) -> None:
+    """calc_alpha (wind.F90:1102-1173) into domain.wind_alpha, then the smoothing of
+    update_winds (:784: windowsize 2, clamped to the halo width, 3 passes)."""
+    h = wi.handle(domain.nest_indx)
+    lib = _capi.load()
+    _capi.check(lib.hicarw_calc_alpha(h, ptr(froude), ptr(domain.wind_alpha), int(halo), _capi.MEM_DEVICE, _s()), h)
+    _capi.check(lib.hicarw_smooth_alpha(h, ptr(domain.wind_alpha), min(int(window), int(halo)), int(nsmooths),
+                                        _capi.MEM_DEVICE, _s()), h)

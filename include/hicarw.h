@@ -277,6 +277,29 @@ int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int a
 /* Number of kernels this library has launched since load (graph nodes included). */
 long long hicarw_kernel_launches(void);
 
+/* ---- the steps either side of the solve in update_winds (wind.F90) ----
+ * Device pointers only (mem_kind must be HICARW_MEM_DEVICE); caller layouts as
+ * hicarw_calc_iter_winds: cells (nx, nz, ny), u (nx+1, nz, ny), v (nx, nz, ny+1).
+ * Stream-ordered, FP32 in Fortran's order of operations. */
+/* calc_w_real (wind.F90:1175-1227): w_real = u dz/dx + v dz/dy (face means) + the
+ * mean of w_grid * jacobian_w over the cell's two w levels; w_grid may be NULL (zero). */
+int hicarw_calc_w_real(hicarw_handle *h, const float *u, const float *v, const float *w_grid, float *w_real,
+                       int mem_kind, void *stream);
+/* calc_idealized_wgrid (wind.F90:940-998): the w_grid predictor w = stagger(w_real -
+ * calc_w_real(u, v, 0)) / jacobian_w, zero on the top level (u, v: the dqdt winds). */
+int hicarw_calc_idealized_wgrid(hicarw_handle *h, const float *u, const float *v, const float *w_real, float *w,
+                                int mem_kind, void *stream);
+/* balance_uvw + calc_w (wind.F90:123-248): w from the horizontal divergence of u, v
+ * (use_dqdt selects the divergence form of the dqdt winds, as calc_divergence). */
+int hicarw_balance_uvw(hicarw_handle *h, const float *u, const float *v, const float *density, float *w, int adv_den,
+                       int use_dqdt, int mem_kind, void *stream);
+/* calc_alpha (wind.F90:1102-1173): alpha(Froude) in [0.2, 2], 0.2 on the top level,
+ * the `halo` outermost rows / columns copied from the first tile row / column. */
+int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *alpha, int halo, int mem_kind, void *stream);
+/* smooth_array of alpha (update_winds :784, array_utilities.F90:322-397, ydim 3):
+ * nsmooths passes of the (2 window + 1)^2 x-y box mean with clamped edges. */
+int hicarw_smooth_alpha(hicarw_handle *h, float *alpha, int window, int nsmooths, int mem_kind, void *stream);
+
 /* ---- learned preconditioner: tensor-core convolutions (no reference counterpart) ----
  * Activation tensors use the "act layout": BF16, channels in groups of 8,
  * element (c, i, k, j) of an (nx, nz, ny) grid at 16-byte unit

@@ -57,6 +57,12 @@ def _lib(precision: str):
     lib.orc_calc_iter_winds.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp]
     lib.orc_calc_divergence.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_int]
     lib.orc_calc_updated_winds.argtypes = [vp, C.c_int, vp, vp, vp]
+    lib.orc_calc_w_real.argtypes = [vp, vp, vp, vp, vp]
+    lib.orc_calc_idealized_wgrid.argtypes = [vp, vp, vp, vp, vp]
+    lib.orc_calc_w.argtypes = [vp, vp, vp, C.c_int]
+    lib.orc_balance_uvw.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
+    lib.orc_calc_alpha.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, C.c_int]
+    lib.orc_smooth_array.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int]
     lib.orc_spmv.argtypes = [vp, vp, vp]
     lib.orc_apply_precond.argtypes = [vp, vp, vp]
     lib.orc_bicgstab.argtypes = [vp, C.c_int, vp]
@@ -160,6 +166,39 @@ class OracleSolver:
         self.lib.orc_calc_divergence(C.byref(self._dom), _ptr(self._a(u)), _ptr(self._a(v)), _ptr(self._a(w)),
                                      _ptr(div), int(bool(adv_den)), int(bool(horz_only)), int(bool(use_dqdt)))
         return div
+
+    def w_real(self, u, v, w_grid=None):
+        """calc_w_real (wind.F90:1175-1227) with jaco = jacobian_w."""
+        out = np.empty((self.ny, self.nz, self.nx), self.dt)
+        self.lib.orc_calc_w_real(C.byref(self._dom), _ptr(self._a(u)), _ptr(self._a(v)),
+                                 _ptr(self._a(w_grid)) if w_grid is not None else None, _ptr(out))
+        return out
+
+    def idealized_wgrid(self, u, v, w_real_field):
+        """calc_idealized_wgrid (wind.F90:940-998): the w_grid predictor."""
+        out = np.empty((self.ny, self.nz, self.nx), self.dt)
+        self.lib.orc_calc_idealized_wgrid(C.byref(self._dom), _ptr(self._a(u)), _ptr(self._a(v)),
+                                          _ptr(self._a(w_real_field)), _ptr(out))
+        return out
+
+    def balance_uvw(self, u, v, w, adv_den=True, use_dqdt=True):
+        """balance_uvw (wind.F90:123-199): w from the horizontal divergence (w updated in place)."""
+        w = self._a(w).copy()
+        self.lib.orc_balance_uvw(C.byref(self._dom), _ptr(self._a(u)), _ptr(self._a(v)), _ptr(w),
+                                 int(bool(adv_den)), int(bool(use_dqdt)))
+        return w
+
+    def calc_alpha(self, froude, halo=1):
+        """calc_alpha (wind.F90:1102-1173)."""
+        out = np.empty((self.ny, self.nz, self.nx), self.dt)
+        self.lib.orc_calc_alpha(self.nx, self.ny, self.nz, _ptr(self._a(froude)), _ptr(out), int(halo))
+        return out
+
+    def smooth_array(self, a, window, nsmooths):
+        """smooth_array_3d, ydim = 3 (array_utilities.F90:322-397), nsmooths passes."""
+        a = self._a(a).copy()
+        self.lib.orc_smooth_array(self.nx, self.ny, self.nz, _ptr(a), int(window), int(nsmooths))
+        return a
 
     def updated_winds(self, adv_den, u, v, w):
         self.lib.orc_calc_updated_winds(self.h, int(bool(adv_den)), _ptr(u), _ptr(v), _ptr(w))

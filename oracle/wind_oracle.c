@@ -43,8 +43,10 @@
 
 #ifdef ORC_FLD_DOUBLE
 typedef double fld;
+#define FLD_SQRT sqrt
 #else
 typedef float fld;
+#define FLD_SQRT sqrtf /* single-precision square root, as Fortran's sqrt of a real */
 #endif
 
 #define NCOEF 15
@@ -963,4 +965,173 @@ double orc_true_residual(orc_solver *s)
         acc += e * e;
     }
     return sqrt(acc);
+}
+
+/* ------------------------------------------------------------------------ */
+/* the steps either side of the solve in update_winds (wind.F90)            */
+/* ------------------------------------------------------------------------ */
+
+/* calc_w_real (wind.F90:1175-1227): w_real = mean of u dz/dx over the two
+ * u faces + mean of v dz/dy over the two v faces + mean of w_grid * jaco over
+ * the two w levels (zero below the first), jaco = jacobian_w.  w_grid may be
+ * NULL (all zero, as calc_idealized_wgrid passes it). */
+void orc_calc_w_real(const orc_domain *d, const fld *u, const fld *v, const fld *w_grid, fld *w_real)
+{
+    orc_solver tmp;
+    tmp.nx = d->nx; tmp.ny = d->ny; tmp.nz = d->nz;
+    orc_solver *s = &tmp;
+    const fld *jw = d->jacobian_w;
+#pragma omp parallel for
+    for (int j = 1; j <= d->ny; j++)
+        for (int k = 1; k <= d->nz; k++)
+            for (int i = 1; i <= d->nx; i++) {
+                size_t c = IC(s, i, k, j);
+                fld lo = 0, hi = 0;
+                if (w_grid) {
+                    hi = w_grid[c] * jw[c];
+                    if (k > 1) lo = w_grid[IC(s, i, k - 1, j)] * jw[IC(s, i, k - 1, j)];
+                }
+                w_real[c] = (u[IU(s, i, k, j)] * d->dzdx_u[IU(s, i, k, j)] + u[IU(s, i + 1, k, j)] * d->dzdx_u[IU(s, i + 1, k, j)]) * (fld)0.5
+                          + (v[IV(s, i, k, j)] * d->dzdy_v[IV(s, i, k, j)] + v[IV(s, i, k, j + 1)] * d->dzdy_v[IV(s, i, k, j + 1)]) * (fld)0.5
+                          + (lo + hi) * (fld)0.5;
+            }
+}
+
+/* calc_idealized_wgrid (wind.F90:940-998): w = w_real_field - calc_w_real(u, v, 0),
+ * staggered to the w levels with advection_dz weights, divided by jacobian_w,
+ * zero at the top level. */
+void orc_calc_idealized_wgrid(const orc_domain *d, const fld *u, const fld *v, const fld *w_real_field, fld *w)
+{
+    orc_solver tmp;
+    tmp.nx = d->nx; tmp.ny = d->ny; tmp.nz = d->nz;
+    orc_solver *s = &tmp;
+    const fld *dz = d->advection_dz, *jw = d->jacobian_w;
+    orc_calc_w_real(d, u, v, NULL, w);
+    size_t n = (size_t)d->nx * d->nz * d->ny;
+    for (size_t q = 0; q < n; q++) w[q] = w_real_field[q] - w[q];
+#pragma omp parallel for
+    for (int j = 1; j <= d->ny; j++)
+        for (int i = 1; i <= d->nx; i++) {
+            for (int k = 1; k <= d->nz - 1; k++) { /* w(k+1) still holds its unstaggered value */
+                size_t c = IC(s, i, k, j), cp = IC(s, i, k + 1, j);
+                w[c] = (w[c] * dz[cp] + w[cp] * dz[c]) / (dz[c] + dz[cp]);
+                w[c] = w[c] / jw[c];
+            }
+            w[IC(s, i, d->nz, j)] = 0;
+        }
+}
+
+/* calc_w (wind.F90:201-248): w integrated upward from a (horizontal) divergence. */
+void orc_calc_w(const orc_domain *d, fld *w, const fld *div, int adv_den)
+{
+    orc_solver tmp;
+    tmp.nx = d->nx; tmp.ny = d->ny; tmp.nz = d->nz;
+    orc_solver *s = &tmp;
+    const fld *dz = d->advection_dz, *jw = d->jacobian_w, *rho = d->density;
+    int nz = d->nz;
+#pragma omp parallel for
+    for (int j = 1; j <= d->ny; j++)
+        for (int i = 1; i <= d->nx; i++) {
+            fld rho_prev = 0;
+            for (int k = 1; k <= nz; k++) {
+                size_t c = IC(s, i, k, j);
+                fld rho_i = 0;
+                if (adv_den) {
+                    if (k < nz) {
+                        size_t cp = IC(s, i, k + 1, j);
+                        rho_i = (rho[c] * dz[cp] + rho[cp] * dz[c]) / (dz[c] + dz[cp]);
+                    } else rho_i = rho[c];
+                    if (k == 1) w[c] = 0 - div[c] * dz[c] / (jw[c] * rho_i);
+                    else {
+                        size_t cm = IC(s, i, k - 1, j);
+                        w[c] = ((w[cm] * rho_prev * jw[cm]) - div[c] * dz[c]) / (jw[c] * rho_i);
+                    }
+                } else {
+                    if (k == 1) w[c] = (0 - div[c] * dz[c]) / (jw[c]);
+                    else {
+                        size_t cm = IC(s, i, k - 1, j);
+                        w[c] = (w[cm] * jw[cm] - div[c] * dz[c]) / (jw[c]);
+                    }
+                }
+                rho_prev = rho_i;
+            }
+        }
+}
+
+/* balance_uvw (wind.F90:123-199): w from the horizontal divergence of u, v. */
+void orc_balance_uvw(const orc_domain *d, const fld *u, const fld *v, fld *w, int adv_den, int use_dqdt)
+{
+    size_t n = (size_t)d->nx * d->nz * d->ny;
+    fld *div = (fld *)malloc(n * sizeof(fld));
+    orc_calc_divergence(d, u, v, w, div, adv_den, 1, use_dqdt);
+    orc_calc_w(d, w, div, adv_den);
+    free(div);
+}
+
+/* calc_alpha (wind.F90:1102-1173): alpha from the Froude number (Moussiopoulos
+ * et al. 1988), bounded to [0.2, 2], 0.2 on the top level, and the `halo`
+ * outermost rows/columns copied from the first tile row/column (south, west,
+ * north, east, in that order).  (1/Fr)**4 is evaluated as (t*t)*(t*t). */
+void orc_calc_alpha(int nx, int ny, int nz, const fld *froude, fld *alpha, int halo)
+{
+    const fld amin = (fld)0.2, amax = (fld)2.0;
+    size_t n = (size_t)nx * nz * ny;
+    for (size_t q = 0; q < n; q++) {
+        fld t = (fld)1.0 / froude[q];
+        fld t2 = t * t;
+        fld p = t2 * t2;
+        fld mx = p > (fld)0.00001 ? p : (fld)0.00001;
+        fld a = (fld)1.0 - (fld)0.5 * mx * (FLD_SQRT((fld)1.0 + (fld)4.0 / mx) - (fld)1.0);
+        a = FLD_SQRT(a > (fld)0.00001 ? a : (fld)0.00001);
+        a = a > amin ? a : amin;
+        a = a < amax ? a : amax;
+        alpha[q] = a;
+    }
+#define IA(i, k, j) ((size_t)((i) - 1) + (size_t)nx * ((size_t)((k) - 1) + (size_t)nz * (size_t)((j) - 1)))
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) alpha[IA(i, nz, j)] = amin;
+    if (halo > 0) {
+        for (int j = 1; j <= halo; j++)
+            for (int k = 1; k <= nz; k++)
+                for (int i = 1; i <= nx; i++) alpha[IA(i, k, j)] = alpha[IA(i, k, halo + 1)];
+        for (int j = 1; j <= ny; j++)
+            for (int k = 1; k <= nz; k++)
+                for (int i = 1; i <= halo; i++) alpha[IA(i, k, j)] = alpha[IA(halo + 1, k, j)];
+        for (int j = ny - halo + 1; j <= ny; j++)
+            for (int k = 1; k <= nz; k++)
+                for (int i = 1; i <= nx; i++) alpha[IA(i, k, j)] = alpha[IA(i, k, ny - halo)];
+        for (int j = 1; j <= ny; j++)
+            for (int k = 1; k <= nz; k++)
+                for (int i = nx - halo + 1; i <= nx; i++) alpha[IA(i, k, j)] = alpha[IA(nx - halo, k, j)];
+    }
+#undef IA
+}
+
+/* smooth_array_3d with ydim = 3 (array_utilities.F90:322-397), `nsmooths`
+ * passes: each level's x-y field replaced by its (2w+1)^2 box mean with
+ * edge-replicated (clamped) indices, summed in double (y offset outer, x inner)
+ * from the values before the pass. */
+void orc_smooth_array(int nx, int ny, int nz, fld *a, int window, int nsmooths)
+{
+    size_t n = (size_t)nx * nz * ny;
+    fld *in = (fld *)malloc(n * sizeof(fld));
+    const int nc = window * 2 + 1;
+    for (int pass = 0; pass < nsmooths; pass++) {
+        memcpy(in, a, n * sizeof(fld));
+#pragma omp parallel for
+        for (int j = 1; j <= ny; j++)
+            for (int k = 1; k <= nz; k++)
+                for (int i = 1; i <= nx; i++) {
+                    double cur = 0.0;
+                    for (int dj = -window; dj <= window; dj++) {
+                        int jj = j + dj < 1 ? 1 : (j + dj > ny ? ny : j + dj);
+                        for (int di = -window; di <= window; di++) {
+                            int ii = i + di < 1 ? 1 : (i + di > nx ? nx : i + di);
+                            cur = cur + (double)in[(size_t)(ii - 1) + (size_t)nx * ((size_t)(k - 1) + (size_t)nz * (jj - 1))];
+                        }
+                    }
+                    a[(size_t)(i - 1) + (size_t)nx * ((size_t)(k - 1) + (size_t)nz * (j - 1))] = (fld)(cur / (double)(nc * nc));
+                }
+    }
+    free(in);
 }

@@ -142,3 +142,68 @@ def test_odd_sizes(oracle_mod, shape):
     s, u, v, w, st1, st2, leak = oracle_mod.update_winds_first(c)
     assert st2["status"] == 0 and leak == 0.0
     assert np.isfinite(u).all() and np.isfinite(v).all() and np.isfinite(w).all()
+
+
+# ---- the steps either side of the solve in update_winds ----------------------
+def test_balance_uvw_closes_the_divergence(oracle_mod, c1):
+    """balance_uvw's w makes the full 3-D divergence vanish: the vertical flux
+    difference of calc_w cancels the horizontal divergence level by level."""
+    s = oracle_mod.OracleSolver(c1.domain, "f64")
+    for adv in (True, False):
+        dh = s.divergence(c1.u, c1.v, c1.w, adv_den=adv, horz_only=True, use_dqdt=True)
+        w = s.balance_uvw(c1.u, c1.v, c1.w, adv_den=adv, use_dqdt=True)
+        full = s.divergence(c1.u, c1.v, w, adv_den=adv, horz_only=False, use_dqdt=True)
+        assert np.abs(full).max() <= 1e-9 * np.abs(dh).max()
+
+
+def test_w_real_and_idealized_wgrid(oracle_mod, c1):
+    s = oracle_mod.OracleSolver(c1.domain, "f64")
+    d = c1.domain
+    rng = np.random.default_rng(5)
+    wg = rng.standard_normal(c1.w.shape)
+    # w_grid part alone (u = v = 0): mean of w_grid * J over the two levels, zero below
+    zu, zv = np.zeros_like(c1.u), np.zeros_like(c1.v)
+    wr = s.w_real(zu, zv, wg)
+    wj = wg * d.jacobian_w.astype(np.float64)
+    ref = 0.5 * wj
+    ref[:, 1:, :] += 0.5 * wj[:, :-1, :]
+    np.testing.assert_allclose(wr, ref, rtol=1e-12, atol=1e-12)
+    # the u/v part: face means of u dz/dx and v dz/dy
+    wr2 = s.w_real(c1.u, c1.v)
+    uu = c1.u.astype(np.float64) * d.dzdx_u
+    vv = c1.v.astype(np.float64) * d.dzdy_v
+    ref2 = 0.5 * (uu[:, :, :-1] + uu[:, :, 1:]) + 0.5 * (vv[:-1] + vv[1:])
+    np.testing.assert_allclose(wr2, ref2, rtol=1e-12, atol=1e-12)
+    # idealized w_grid: staggered (w_real_field - w_real(u, v, 0)) / J_w, zero on top
+    field = rng.standard_normal(c1.w.shape)
+    w = s.idealized_wgrid(c1.u, c1.v, field)
+    t = field - wr2
+    dz = d.advection_dz.astype(np.float64)
+    stag = (t[:, :-1] * dz[:, 1:] + t[:, 1:] * dz[:, :-1]) / (dz[:, :-1] + dz[:, 1:]) / d.jacobian_w[:, :-1]
+    np.testing.assert_allclose(w[:, :-1], stag, rtol=1e-12, atol=1e-12)
+    assert not w[:, -1].any()
+
+
+def test_calc_alpha_and_smoothing(oracle_mod, c1):
+    s = oracle_mod.OracleSolver(c1.domain, "f64")
+    rng = np.random.default_rng(6)
+    fr = np.exp(rng.uniform(np.log(0.05), np.log(20.0), c1.w.shape))
+    a = s.calc_alpha(fr, halo=2)
+    p = np.maximum((1.0 / fr) ** 4, 1e-5)
+    ref = np.clip(np.sqrt(np.maximum(1.0 - 0.5 * p * (np.sqrt(1.0 + 4.0 / p) - 1.0), 1e-5)), 0.2, 2.0)
+    ref[:, -1, :] = 0.2
+    ny, nx = a.shape[0], a.shape[2]
+    np.testing.assert_allclose(a[2:ny - 2, :, 2:nx - 2], ref[2:ny - 2, :, 2:nx - 2], rtol=1e-12)
+    # halo rows / columns repeat the first tile row / column (south, west, north, east)
+    np.testing.assert_array_equal(a[0], a[2])
+    np.testing.assert_array_equal(a[:, :, 1], a[:, :, 2])
+    np.testing.assert_array_equal(a[-1], a[-3])
+    np.testing.assert_array_equal(a[:, :, -2], a[:, :, -3])
+    # smoothing: constants are fixed points; an interior spike spreads over the box
+    c = np.full(c1.w.shape, 0.7)
+    np.testing.assert_allclose(s.smooth_array(c, 2, 3), c, rtol=1e-14)
+    spike = np.zeros(c1.w.shape)
+    spike[10, 3, 12] = 25.0
+    sm = s.smooth_array(spike, 2, 1)
+    assert sm[8:13, 3, 10:15] == pytest.approx(np.ones((5, 5)))
+    assert sm.sum() == pytest.approx(25.0)
