@@ -60,6 +60,7 @@ REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "l
 # (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
 TRAFFIC = {}
 TOL = 1.0e-6
+MG_COARSE_SCALE = None  # --mg-coarse-scale
 
 
 def peaks():
@@ -80,6 +81,9 @@ def solver_options(name: str):
         # the reference solve as the fallback on a 1%-per-50-iterations stall
         "mg": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64,
                    precond=_capi.PRECOND_MG, stall_iters=50),
+        # the same with FP32 Krylov vectors (FP64 reductions)
+        "mg32": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F32,
+                     precond=_capi.PRECOND_MG, stall_iters=50),
         # flexible GMRES(30) outer loop around the same V-cycle, FP64 Arnoldi basis
         "fgmres": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_MG, fgmres_restart=30),
         # flexible GMRES(30) with the reference Jacobi-Richardson preconditioner (A/B baseline)
@@ -89,7 +93,9 @@ def solver_options(name: str):
         "learned": dict(solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_LEARNED, fgmres_restart=30,
                         stall_iters=100),
     }
-    kw = presets[name]
+    kw = dict(presets[name])
+    if MG_COARSE_SCALE is not None and "precond" in kw:
+        kw["mg_coarse_scale"] = MG_COARSE_SCALE
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
 
 
@@ -610,16 +616,18 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL
+    global TOL, MG_COARSE_SCALE
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed1024", choices=sorted(WORKLOADS))
-    ap.add_argument("--solver", default="mg", choices=["plain", "mg", "fgmres", "fgmres_jacobi", "learned"])
+    ap.add_argument("--solver", default="mg", choices=["plain", "mg", "mg32", "fgmres", "fgmres_jacobi", "learned"])
     ap.add_argument("--no-accuracy", action="store_true", help="skip the tight-solve accuracy report")
     ap.add_argument("--tol", type=float, default=TOL, help="relative residual tolerance of the timed solves")
+    ap.add_argument("--mg-coarse-scale", type=float, default=None,
+                    help="override the V-cycle's coarse-correction scale of the solver preset")
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")
@@ -629,6 +637,7 @@ def main():
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     args = ap.parse_args()
     TOL = args.tol
+    MG_COARSE_SCALE = args.mg_coarse_scale
     wl = WORKLOADS[args.workload]
     if "batch" in wl:
         if args.impl == "reference":

@@ -170,6 +170,7 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->stall_iters = 0;
     o->mg_omega = 0.8f;
     o->fgmres_restart = 30;
+    o->mg_coarse_scale = 1.35f; // over-correction of the aggregation coarse grid: 35 -> 25 iterations at 512x512x48
 }
 
 static Metrics metrics_of(const hicarw_handle *h)
@@ -365,6 +366,9 @@ extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
     int rc = ensure_vectors(h, prec);
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
+    // V-cycle parameters are read when its launches are enqueued (the graphs were just dropped)
+    h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+    h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
     return rc;
 }
 
@@ -488,6 +492,7 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
                      h->opt.solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
         if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
         h->mg_dirty = 0;
     }
@@ -1124,6 +1129,7 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
     if (!rc && sweeps <= 0) {
         if (h->mg_dirty || !h->mg.ready) {
             h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
             if (mg_build(h->mg, d, h->coef, s) != 0) rc = HICARW_ERR_CUDA;
             else h->mg_dirty = 0;
         }
@@ -1558,6 +1564,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         h->use_learned = 0;
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
             h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
             if (mg_build(h->mg, h->d, h->coef, s) != 0) {
                 fprintf(stderr, "hicarw batch: multigrid build of subdomain %d failed\n", i);
                 return HICARW_ERR_CUDA;

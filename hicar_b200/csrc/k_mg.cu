@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(MG_THREADS) pre_kernel(Dims d, const float *__
 // corner is (ia, ja), all k including the ghost planes, zero outside the interior.
 template <int SX, int SY>
 __device__ __forceinline__ void stage_window(const Dims &d, const float *__restrict__ x1, const Dims &dc,
-                                             const float *__restrict__ xc, int ia, int ja, float *s_x)
+                                             const float *__restrict__ xc, int ia, int ja, float *s_x,
+                                             float cs = 1.0f)
 {
     constexpr int SP = SX * SY;
     const int nst = SP * (d.nz + 2);
@@ -222,7 +223,7 @@ __device__ __forceinline__ void stage_window(const Dims &d, const float *__restr
             float a = 0.0f;
             if (t < nst && inside(d, i, k, j)) {
                 a = __ldg(x1 + kidx(d, i, k, j));
-                if (xc) a += __ldg(xc + kidx(dc, (i + 1) >> 1, k, (j + 1) >> 1));
+                if (xc) a += cs * __ldg(xc + kidx(dc, (i + 1) >> 1, k, (j + 1) >> 1));
             }
             v[u] = a;
         }
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
                                                           const float *__restrict__ minv, const TR *__restrict__ r,
                                                           const float *__restrict__ x1, Dims dc,
                                                           const float *__restrict__ xc, TO *__restrict__ out,
-                                                          float omega, const SolveState *gate)
+                                                          float omega, float cscale, const SolveState *gate)
 {
     if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
     constexpr int TC = TX * TY, SX = TX + 2, SY = TY + 2, SP = SX * SY;
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
     const int nz = d.nz, n = TC * nz;
     float *s_res = sm, *s_c = sm + n, *s_m = sm + 2 * n, *s_cp = sm + 3 * n, *s_x = sm + 4 * n;
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
-    stage_window<SX, SY>(d, x1, dc, xc, i0 - 1, j0 - 1, s_x);
+    stage_window<SX, SY>(d, x1, dc, xc, i0 - 1, j0 - 1, s_x, cscale);
     __syncthreads();
     for (int base = threadIdx.x; base < n; base += MG_THREADS * 2) {
         float res2[2], vc[2], vm[2], vp[2];
@@ -481,24 +482,24 @@ static void launch_pre(const MgLevel &L, int level, const TR *r, float *out, flo
 }
 
 template <typename TR, typename TO, int TX, int TY>
-static void post_t(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, float omega, const SolveState *gate,
-                   cudaStream_t s)
+static void post_t(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, float omega, float cscale,
+                   const SolveState *gate, cudaStream_t s)
 {
     dim3 g((L.d.nx + TX - 1) / TX, (L.d.ny + TY - 1) / TY);
     size_t smem = ((size_t)4 * TX * TY * L.d.nz + (size_t)(TX + 2) * (TY + 2) * (L.d.nz + 2)) * sizeof(float);
     set_smem(post_kernel<TR, TO, TX, TY>, smem);
     post_kernel<TR, TO, TX, TY><<<g, MG_THREADS, smem, s>>>(L.d, L.coef, L.cp, L.minv, r, L.x1, C.d, C.x3, out,
-                                                            omega, gate);
+                                                            omega, cscale, gate);
 }
 
 template <typename TR, typename TO>
 static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel &C, TO *out, float omega,
-                        const SolveState *gate, cudaStream_t s)
+                        float cscale, const SolveState *gate, cudaStream_t s)
 {
     const double N = (double)L.d.nx * L.d.ny * L.d.nz;
     ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + 60.0 + 4.0 + 1.0 + 8.0) * N, s);
-    if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, r, C, out, omega, gate, s);
-    else post_t<TR, TO, 32, 1>(L, r, C, out, omega, gate, s);
+    if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, r, C, out, omega, cscale, gate, s);
+    else post_t<TR, TO, 32, 1>(L, r, C, out, omega, cscale, gate, s);
     count_launch(1);
 }
 
@@ -545,8 +546,8 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     for (int l = L - 2; l >= 0; l--) {
         const MgLevel &F = mg.lev[l];
         const MgLevel &C = mg.lev[l + 1];
-        if (l == 0) launch_post<V, V>(F, 0, in, C, out, w, gate, s);
-        else launch_post<float, float>(F, l, F.r, C, F.x3, w, gate, s);
+        if (l == 0) launch_post<V, V>(F, 0, in, C, out, w, mg.cscale, gate, s);
+        else launch_post<float, float>(F, l, F.r, C, F.x3, w, mg.cscale, gate, s);
     }
 }
 

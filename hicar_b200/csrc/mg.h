@@ -19,7 +19,8 @@ struct MgLevel {
 struct Mg {
     int nlev = 0;
     int ready = 0;
-    float omega = 0.8f; // damping of the z-line Jacobi smoother
+    float omega = 0.8f;  // damping of the z-line Jacobi smoother
+    float cscale = 1.0f; // scale of the prolongated coarse-grid correction (over-correction > 1)
     MgLevel lev[MG_MAX_LEVELS];
 };
 

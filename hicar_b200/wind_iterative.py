@@ -52,6 +52,7 @@ class WindOptions:
     stall_iters: int = 0
     mg_omega: float = 0.8
     fgmres_restart: int = 30
+    mg_coarse_scale: float = 1.35          # V-cycle over-correction of the aggregation coarse grid
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -68,6 +69,7 @@ class WindOptions:
         o.stall_iters = int(self.stall_iters)
         o.mg_omega = float(self.mg_omega)
         o.fgmres_restart = int(self.fgmres_restart)
+        o.mg_coarse_scale = float(self.mg_coarse_scale)
         return o
 
 

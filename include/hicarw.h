@@ -112,6 +112,8 @@ typedef struct hicarw_options {
                              this many iterations and fall back to the reference solve (0 = off) */
     float mg_omega;       /* damping of the multigrid smoother (default 0.8) */
     int fgmres_restart;   /* FGMRES restart length m (1..32, default 30) */
+    float mg_coarse_scale; /* V-cycle: scale of the prolongated coarse-grid correction; over-correction
+                              of the piecewise-constant aggregation (default 1.35) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),

@@ -7,7 +7,8 @@ algorithm with the same FP32 storage points:
   * z-line Jacobi smoother with the column tridiagonal (C, A, B): Thomas
     factors computed in FP64 and stored in FP32, the recurrences in FP32, the
     residual of the post-smoother summed in FP64 from the FP32 staged iterate
-    x2 = x1 + P xc, damping omega; exact tridiagonal solve on the
+    x2 = x1 + cscale P xc (FP32, cscale the over-correction), damping omega;
+    exact tridiagonal solve on the
     single-column level (reached by the fused restriction + pre-smoothing).
 Arrays are the interior (ny, nz, nx) blocks; coefficients are (15, ny, nz, nx)
 in the order A..O.
@@ -109,8 +110,9 @@ def post(C, cp, mi, r, x2, omega):
 
 
 class VCycle:
-    def __init__(self, coefs, omega=0.8):
+    def __init__(self, coefs, omega=0.8, cscale=1.35):
         self.omega = omega
+        self.cscale = cscale
         self.lev = [np.asarray(coefs, f32)]
         while self.lev[-1].shape[1] > 1 or self.lev[-1].shape[3] > 1:
             self.lev.append(coarsen(self.lev[-1]))
@@ -141,7 +143,7 @@ class VCycle:
             cp, mi = self.fac[l]
             up = np.repeat(np.repeat(x3, 2, axis=0), 2, axis=2)
             ny, nz, nx = x1[l].shape
-            x2 = (x1[l] + up[:ny, :, :nx]).astype(f32)
+            x2 = (x1[l] + f32(self.cscale) * up[:ny, :, :nx].astype(f32)).astype(f32)
             out = post(C, cp, mi, rs[l], x2, w)
             x3 = out if l == 0 else out.astype(f32)
         return x3
