@@ -61,6 +61,7 @@ REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "l
 TRAFFIC = {}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
+MG_OMEGA = None  # --mg-omega
 
 
 def peaks():
@@ -96,6 +97,8 @@ def solver_options(name: str):
     kw = dict(presets[name])
     if MG_COARSE_SCALE is not None and "precond" in kw:
         kw["mg_coarse_scale"] = MG_COARSE_SCALE
+    if MG_OMEGA is not None and "precond" in kw:
+        kw["mg_omega"] = MG_OMEGA
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
 
 
@@ -616,7 +619,7 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL, MG_COARSE_SCALE
+    global TOL, MG_COARSE_SCALE, MG_OMEGA
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -628,6 +631,8 @@ def main():
     ap.add_argument("--tol", type=float, default=TOL, help="relative residual tolerance of the timed solves")
     ap.add_argument("--mg-coarse-scale", type=float, default=None,
                     help="override the V-cycle's coarse-correction scale of the solver preset")
+    ap.add_argument("--mg-omega", type=float, default=None,
+                    help="override the V-cycle's smoother damping of the solver preset")
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")
@@ -638,6 +643,7 @@ def main():
     args = ap.parse_args()
     TOL = args.tol
     MG_COARSE_SCALE = args.mg_coarse_scale
+    MG_OMEGA = args.mg_omega
     wl = WORKLOADS[args.workload]
     if "batch" in wl:
         if args.impl == "reference":
