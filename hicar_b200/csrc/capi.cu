@@ -1234,6 +1234,20 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         fgmres_reset(h->gst, fg.m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
         fgmres_set_profile(h->gst, 1, s);
     }
+    if (solver == HICARW_SOLVER_REFERENCE) {
+        // start from the set-up of a cold solve (x = 0, r = r^ = p = b), so that every
+        // kernel of the profiled iterations does the work of a live iteration
+        OpCtx c = opctx(h);
+        RedBuf rb{h->partials, h->red_blocks};
+        if ((rc = zero_solution(h, s)) != 0) return rc;
+        launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, 0, s);
+        if (prec == HICARW_KRYLOV_F64)
+            launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
+                                         V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+        else
+            launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R),
+                                       V<float>(h, V_RHAT), V<float>(h, V_P), h->st, h->hist, rb, s);
+    }
     prof_state_kernel<<<1, 1, 0, s>>>(h->st, 1);
     CK(cudaStreamSynchronize(s));
     for (auto &r : g_prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }

@@ -80,16 +80,14 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
     extern __shared__ __align__(128) uint8_t sm[];
     uint8_t *wsm = sm;
     uint8_t *stg0 = sm + C::WB, *stg1 = sm + C::WB + C::STAGE;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + C::WB + 2 * C::STAGE); // copy[0], copy[1], mma
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 3);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + C::WB + 2 * C::STAGE); // copy[0], copy[1], mma[0], mma[1]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4);
     const int tid = threadIdx.x, warp = tid >> 5;
     const ActDims di = a.din, dd = a.dout;
     const int ntx = (di.nx + TILE - 1) / TILE;
     const int ntiles = ntx * di.nz * di.ny;
     if (tid == 0) {
-        tc::mbar_init(&bars[0], 1);
-        tc::mbar_init(&bars[1], 1);
-        tc::mbar_init(&bars[2], 1);
+        for (int q = 0; q < 4; q++) tc::mbar_init(&bars[q], 1);
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(tslot, C::NCOL);
@@ -113,84 +111,101 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
     };
 
     constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, 0, 0);
+    // Pipeline: in iteration `it` the MMAs of tile `it` (TMEM buffer it&1) run
+    // while the epilogue of tile it-1 (buffer (it-1)&1) reads the other buffer,
+    // and the copies of tile it+1 go into the line stage that tile it-1 used,
+    // issued as soon as its MMAs have completed.  mbarriers: [0], [1] line
+    // stages, [2], [3] MMA completion per TMEM buffer.
     bool ok = true;
-    int it = 0, tile = blockIdx.x;
+    int it = 0, tile = blockIdx.x, prev = -1;
     if (tid == 0 && tile < ntiles) issue(tile, 0, true);
-    for (; tile < ntiles; tile += gridDim.x, it++) {
+    for (;; it++) {
+        const bool have = tile < ntiles;
         const int s = it & 1;
-        if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, s ^ 1, false);
-        const bool got = tc::mbar_wait(&bars[s], (it >> 1) & 1);
-        if (!__syncthreads_and(got)) { ok = false; break; }
-        if (tid == 0) {
+        if (have) {
+            const bool got = tc::mbar_wait(&bars[s], (it >> 1) & 1);
+            if (!__syncthreads_and(got)) { ok = false; break; }
+            if (tid == 0) {
+                tc::fence_after();
+                const uint32_t sb = tc::smem_u32(s ? stg1 : stg0), wb = tc::smem_u32(wsm);
+                uint32_t acc = 0;
+                for (int t = 0; t < 27; t++) {
+                    const int sl = t / 3, dil = t % 3;
+#pragma unroll
+                    for (int c = 0; c < C::GI / 2; c++) {
+                        const uint64_t ad = tc::sdesc(sb + (sl * C::GI + 2 * c) * LG + dil * 16, LG, 128);
+                        const uint64_t bd = tc::sdesc(wb + (t * C::GI + 2 * c) * COUT * 16, COUT * 16, 128);
+                        tc::mma_bf16(tmem + s * COUT, ad, bd, IDESC, acc);
+                        acc = 1;
+                    }
+                }
+                tc::mma_commit(&bars[2 + s]);
+            }
+        }
+        const int nxt = have ? tile + (int)gridDim.x : ntiles;
+        if (it == 0) {
+            if (tid == 0 && nxt < ntiles) issue(nxt, s ^ 1, false); // stage 1 not used yet
+        } else {
+            // tile it-1: its MMAs done -> its line stage is free, its accumulator readable
+            const bool done = tc::mbar_wait(&bars[2 + (s ^ 1)], ((it - 1) >> 1) & 1);
+            if (!__syncthreads_and(done)) { ok = false; break; }
+            if (tid == 0 && nxt < ntiles) issue(nxt, s ^ 1, false);
             tc::fence_after();
-            const uint32_t sb = tc::smem_u32(s ? stg1 : stg0), wb = tc::smem_u32(wsm);
-            uint32_t acc = 0;
-            for (int t = 0; t < 27; t++) {
-                const int sl = t / 3, dil = t % 3;
+            const int tx = prev % ntx, r = prev / ntx, k = r % di.nz, j = r / di.nz;
+            const int i = tx * TILE + tid;
+            const uint32_t acc_col = (uint32_t)((s ^ 1) * COUT);
+            float v[COUT];
 #pragma unroll
-                for (int c = 0; c < C::GI / 2; c++) {
-                    const uint64_t ad = tc::sdesc(sb + (sl * C::GI + 2 * c) * LG + dil * 16, LG, 128);
-                    const uint64_t bd = tc::sdesc(wb + (t * C::GI + 2 * c) * COUT * 16, COUT * 16, 128);
-                    tc::mma_bf16(tmem + s * COUT, ad, bd, IDESC, acc);
-                    acc = 1;
+            for (int q = 0; q < COUT / 16; q++) {
+                float t16[16];
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + acc_col + (uint32_t)(q * 16), t16);
+#pragma unroll
+                for (int e = 0; e < 16; e++) v[q * 16 + e] = t16[e];
+            }
+            if (i < di.nx) {
+                if (a.bias) {
+#pragma unroll
+                    for (int c = 0; c < COUT; c++) v[c] += __ldg(a.bias + c);
                 }
-            }
-            tc::mma_commit(&bars[2]);
-        }
-        const bool done = tc::mbar_wait(&bars[2], it & 1);
-        if (!__syncthreads_and(done)) { ok = false; break; }
-        tc::fence_after();
-        const int tx = tile % ntx, r = tile / ntx, k = r % di.nz, j = r / di.nz;
-        const int i = tx * TILE + tid;
-        float v[COUT];
+                if (a.skip) {
 #pragma unroll
-        for (int q = 0; q < COUT / 16; q++) {
-            float t16[16];
-            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * COUT + q * 16), t16);
+                    for (int g = 0; g < C::GO; g++) {
+                        float f[8];
+                        unpack8(a.skip[act_unit(dd, i, k, j, g)], f);
 #pragma unroll
-            for (int e = 0; e < 16; e++) v[q * 16 + e] = t16[e];
-        }
-        if (i < di.nx) {
-            if (a.bias) {
-#pragma unroll
-                for (int c = 0; c < COUT; c++) v[c] += __ldg(a.bias + c);
-            }
-            if (a.skip) {
-#pragma unroll
-                for (int g = 0; g < C::GO; g++) {
-                    float f[8];
-                    unpack8(a.skip[act_unit(dd, i, k, j, g)], f);
-#pragma unroll
-                    for (int e = 0; e < 8; e++) v[g * 8 + e] += f[e];
+                        for (int e = 0; e < 8; e++) v[g * 8 + e] += f[e];
+                    }
                 }
-            }
-            if (a.relu) {
+                if (a.relu) {
 #pragma unroll
-                for (int c = 0; c < COUT; c++) v[c] = fmaxf(v[c], 0.0f);
-            }
-            if (a.mask) {
-#pragma unroll
-                for (int g = 0; g < C::GO; g++) {
-                    float f[8];
-                    unpack8(a.mask[act_unit(dd, i, k, j, g)], f);
-#pragma unroll
-                    for (int e = 0; e < 8; e++) v[g * 8 + e] = f[e] > 0.0f ? v[g * 8 + e] : 0.0f;
+                    for (int c = 0; c < COUT; c++) v[c] = fmaxf(v[c], 0.0f);
                 }
-            }
-            if (a.out) {
+                if (a.mask) {
 #pragma unroll
-                for (int g = 0; g < C::GO; g++) a.out[act_unit(dd, i, k, j, g)] = pack8(v + g * 8);
+                    for (int g = 0; g < C::GO; g++) {
+                        float f[8];
+                        unpack8(a.mask[act_unit(dd, i, k, j, g)], f);
+#pragma unroll
+                        for (int e = 0; e < 8; e++) v[g * 8 + e] = f[e] > 0.0f ? v[g * 8 + e] : 0.0f;
+                    }
+                }
+                if (a.out) {
+#pragma unroll
+                    for (int g = 0; g < C::GO; g++) a.out[act_unit(dd, i, k, j, g)] = pack8(v + g * 8);
+                }
+                if (a.out0) a.out0[((long long)j * dd.nz + k) * dd.nx + i] = v[0];
             }
-            if (a.out0) a.out0[((long long)j * dd.nz + k) * dd.nx + i] = v[0];
         }
         tc::fence_before();
         __syncthreads();
+        if (!have) break;
+        prev = tile;
+        tile = nxt;
     }
     if (!ok && tid == 0) {
         atomicExch(a.err, 1);
-        // bounded wait for the copies this CTA may still have in flight
-        tc::mbar_wait(&bars[0], 0, 100000000ull);
-        tc::mbar_wait(&bars[1], 0, 100000000ull);
+        // bounded waits for the copies and MMAs this CTA may still have in flight
+        for (int q = 0; q < 4; q++) tc::mbar_wait(&bars[q], (uint32_t)(q < 2 ? (it >> 1) & 1 : (it & 1)), 100000000ull);
     }
     tc::fence_before();
     __syncthreads();
