@@ -29,6 +29,7 @@ EXPORTS = [
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
     "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
     "hicarw_residual_norm_noalloc", "hicarw_nn_act_pitch", "hicarw_nn_conv3", "hicarw_nn_conv3_wgrad",
+    "hicarw_nn_conv3_time",
     "hicarw_unet_create", "hicarw_unet_destroy", "hicarw_unet_grid", "hicarw_unet_num_params",
     "hicarw_unet_get_params", "hicarw_unet_set_params", "hicarw_unet_get_grads", "hicarw_unet_zero_grads",
     "hicarw_unet_features", "hicarw_unet_forward", "hicarw_unet_backward", "hicarw_unet_backward_residual",
@@ -122,6 +123,7 @@ def load(path: str = LIB_PATH):
         "hicarw_nn_act_pitch": (ci, [ci]),
         "hicarw_nn_conv3": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp]),
         "hicarw_nn_conv3_wgrad": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, vp]),
+        "hicarw_nn_conv3_time": (ci, [ci, ci, ci, ci, ci, vp, vp, vp, vp, ci, vp, P(C.c_float)]),
         "hicarw_unet_create": (ci, [ci, ci, ci, C.c_ulonglong, P(vp)]),
         "hicarw_unet_destroy": (ci, [vp]),
         "hicarw_unet_grid": (ci, [vp, P(ci), P(ci), P(ci)]),

@@ -97,16 +97,20 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
     const uint32_t tmem = *tslot;
     const char *inb = reinterpret_cast<const char *>(a.in);
 
+    // called by all lanes of warp 0: lane 0 posts the byte count, then the lanes
+    // issue one bulk copy each
     auto issue = [&](int tile, int s, bool with_w) {
         const int tx = tile % ntx, r = tile / ntx, k = r % di.nz, j = r / di.nz;
+        const int lane = tid & 31;
         uint8_t *dst = s ? stg1 : stg0;
-        tc::mbar_expect_tx(&bars[s], C::STAGE + (with_w ? C::WB : 0));
-        if (with_w) tc::bulk_g2s(wsm, a.w, C::WB, &bars[s]);
-        for (int sl = 0; sl < 9; sl++) {
+        if (lane == 0) tc::mbar_expect_tx(&bars[s], C::STAGE + (with_w ? C::WB : 0));
+        __syncwarp();
+        if (with_w && lane == 31) tc::bulk_g2s(wsm, a.w, C::WB, &bars[s]);
+        for (int q = lane; lane < 31 && q < 9 * C::GI; q += 31) { // lanes 0..30: the line images
+            const int sl = q / C::GI, g = q % C::GI;
             const long long L = (long long)(j + sl / 3) * (di.nz + 2) + (k + sl % 3); // line (j+dj+1, k+dk+1)
-            for (int g = 0; g < C::GI; g++)
-                tc::bulk_g2s(dst + (sl * C::GI + g) * LG, inb + ((L * C::GI + g) * di.PX + (long long)tx * TILE) * 16,
-                             LG, &bars[s]);
+            tc::bulk_g2s(dst + (sl * C::GI + g) * LG, inb + ((L * C::GI + g) * di.PX + (long long)tx * TILE) * 16, LG,
+                         &bars[s]);
         }
     };
 
@@ -118,7 +122,7 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
     // stages, [2], [3] MMA completion per TMEM buffer.
     bool ok = true;
     int it = 0, tile = blockIdx.x, prev = -1;
-    if (tid == 0 && tile < ntiles) issue(tile, 0, true);
+    if (warp == 0 && tile < ntiles) issue(tile, 0, true);
     for (;; it++) {
         const bool have = tile < ntiles;
         const int s = it & 1;
@@ -127,16 +131,17 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
             if (!__syncthreads_and(got)) { ok = false; break; }
             if (tid == 0) {
                 tc::fence_after();
-                const uint32_t sb = tc::smem_u32(s ? stg1 : stg0), wb = tc::smem_u32(wsm);
-                uint32_t acc = 0;
+                // descriptors of the stage / weight bases; every operand is a
+                // compile-time byte offset from them (start field = address >> 4)
+                const uint64_t a0 = tc::sdesc(tc::smem_u32(s ? stg1 : stg0), LG, 128);
+                const uint64_t b0 = tc::sdesc(tc::smem_u32(wsm), COUT * 16, 128);
+#pragma unroll
                 for (int t = 0; t < 27; t++) {
-                    const int sl = t / 3, dil = t % 3;
 #pragma unroll
                     for (int c = 0; c < C::GI / 2; c++) {
-                        const uint64_t ad = tc::sdesc(sb + (sl * C::GI + 2 * c) * LG + dil * 16, LG, 128);
-                        const uint64_t bd = tc::sdesc(wb + (t * C::GI + 2 * c) * COUT * 16, COUT * 16, 128);
-                        tc::mma_bf16(tmem + s * COUT, ad, bd, IDESC, acc);
-                        acc = 1;
+                        const uint64_t ad = a0 + (uint64_t)((((t / 3) * C::GI + 2 * c) * LG + (t % 3) * 16) >> 4);
+                        const uint64_t bd = b0 + (uint64_t)(((t * C::GI + 2 * c) * COUT * 16) >> 4);
+                        tc::mma_bf16(tmem + s * COUT, ad, bd, IDESC, (t | c) ? 1u : 0u);
                     }
                 }
                 tc::mma_commit(&bars[2 + s]);
@@ -144,12 +149,12 @@ __global__ void __launch_bounds__(128) conv3_fwd_kernel(ConvArgs a)
         }
         const int nxt = have ? tile + (int)gridDim.x : ntiles;
         if (it == 0) {
-            if (tid == 0 && nxt < ntiles) issue(nxt, s ^ 1, false); // stage 1 not used yet
+            if (warp == 0 && nxt < ntiles) issue(nxt, s ^ 1, false); // stage 1 not used yet
         } else {
             // tile it-1: its MMAs done -> its line stage is free, its accumulator readable
             const bool done = tc::mbar_wait(&bars[2 + (s ^ 1)], ((it - 1) >> 1) & 1);
             if (!__syncthreads_and(done)) { ok = false; break; }
-            if (tid == 0 && nxt < ntiles) issue(nxt, s ^ 1, false);
+            if (warp == 0 && nxt < ntiles) issue(nxt, s ^ 1, false);
             tc::fence_after();
             const int tx = prev % ntx, r = prev / ntx, k = r % di.nz, j = r / di.nz;
             const int i = tx * TILE + tid;
@@ -254,20 +259,26 @@ __global__ void __launch_bounds__(128) conv3_wgrad_kernel(WgradArgs a)
     const char *xb = reinterpret_cast<const char *>(a.x);
     const char *yb = reinterpret_cast<const char *>(a.dy);
 
+    // called by all lanes of warp 0 (see the forward kernel)
     auto issue = [&](int tile, int s) {
         const int tx = tile % ntx, r = tile / ntx, k = r % dx.nz, j = r / dx.nz;
+        const int lane = tid & 31;
         uint8_t *dst = s ? stg1 : stg0;
-        tc::mbar_expect_tx(&bars[s], 9 * C::GI * LG + C::YR);
-        for (int sl = 0; sl < 9; sl++) {
-            const long long L = (long long)(j + sl / 3) * (dx.nz + 2) + (k + sl % 3);
-            for (int g = 0; g < C::GI; g++)
+        if (lane == 0) tc::mbar_expect_tx(&bars[s], 9 * C::GI * LG + C::YR);
+        __syncwarp();
+        for (int q = lane; q < 9 * C::GI + C::GO; q += 32) {
+            if (q < 9 * C::GI) {
+                const int sl = q / C::GI, g = q % C::GI;
+                const long long L = (long long)(j + sl / 3) * (dx.nz + 2) + (k + sl % 3);
                 tc::bulk_g2s(dst + (sl * C::GI + g) * LG, xb + ((L * C::GI + g) * dx.PX + (long long)tx * TILE) * 16,
                              LG, &bars[s]);
+            } else {
+                const int g = q - 9 * C::GI;
+                const long long L0 = (long long)(j + 1) * (dy.nz + 2) + (k + 1);
+                tc::bulk_g2s(dst + C::XR + g * YG, yb + ((L0 * C::GO + g) * dy.PX + (long long)tx * TILE + 1) * 16,
+                             YG, &bars[s]);
+            }
         }
-        const long long L0 = (long long)(j + 1) * (dy.nz + 2) + (k + 1);
-        for (int g = 0; g < C::GO; g++)
-            tc::bulk_g2s(dst + C::XR + g * YG, yb + ((L0 * C::GO + g) * dy.PX + (long long)tx * TILE + 1) * 16, YG,
-                         &bars[s]);
     };
 
     constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, 1, 1);
@@ -276,23 +287,26 @@ __global__ void __launch_bounds__(128) conv3_wgrad_kernel(WgradArgs a)
     for (int c = 0; c < COUT; c++) db[c] = 0.0f;
     bool ok = true;
     int it = 0, tile = blockIdx.x;
-    if (tid == 0 && tile < ntiles) issue(tile, 0);
+    if (warp == 0 && tile < ntiles) issue(tile, 0);
     for (; tile < ntiles; tile += gridDim.x, it++) {
         const int s = it & 1;
-        if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, s ^ 1);
+        if (warp == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, s ^ 1);
         const bool got = tc::mbar_wait(&bars[s], (it >> 1) & 1);
         if (!__syncthreads_and(got)) { ok = false; break; }
         const uint8_t *st = s ? stg1 : stg0;
         if (tid == 0) {
             tc::fence_after();
-            const uint32_t sx = tc::smem_u32(st), sy = sx + C::XR;
+            const uint64_t a0 = tc::sdesc(tc::smem_u32(st), 128, LG);
+            const uint64_t b0 = tc::sdesc(tc::smem_u32(st) + C::XR, 128, YG);
+#pragma unroll
             for (int dil = 0; dil < 3; dil++)
+#pragma unroll
                 for (int mc = 0; mc < C::NMC; mc++) {
                     const uint32_t d = tmem + (uint32_t)((dil * C::NMC + mc) * COUT);
 #pragma unroll
                     for (int kc = 0; kc < TILE / 16; kc++) {
-                        const uint64_t ad = tc::sdesc(sx + mc * 16 * LG + dil * 16 + kc * 256, 128, LG);
-                        const uint64_t bd = tc::sdesc(sy + kc * 256, 128, YG);
+                        const uint64_t ad = a0 + (uint64_t)((mc * 16 * LG + dil * 16 + kc * 256) >> 4);
+                        const uint64_t bd = b0 + (uint64_t)((kc * 256) >> 4);
                         tc::mma_bf16(d, ad, bd, IDESC, (it > 0 || kc > 0) ? 1u : 0u);
                     }
                 }

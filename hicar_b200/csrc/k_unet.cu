@@ -854,6 +854,50 @@ extern "C" int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const 
     return HICARW_OK;
 }
 
+// Mean duration (ms, CUDA events on `stream`) of `reps` forward launches of one
+// convolution (bias + ReLU epilogue) on caller-owned act tensors, weights packed once.
+extern "C" int hicarw_nn_conv3_time(int cin, int cout, int nx, int ny, int nz, const void *in, const float *w,
+                                    const float *bias, void *out, int reps, void *stream, float *ms)
+{
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !in || !w || !out || reps < 1 || !ms) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint4 *img = nullptr;
+    int *err = nullptr;
+    cudaEvent_t e0, e1;
+    if (cudaMalloc((void **)&img, conv_wimage_bytes(cin, cout)) != cudaSuccess) return HICARW_ERR_CUDA;
+    if (cudaMalloc((void **)&err, sizeof(int)) != cudaSuccess) { cudaFree(img); return HICARW_ERR_CUDA; }
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemsetAsync(err, 0, sizeof(int), s);
+    conv_pack_fwd(w, cin, cout, img, s);
+    ConvArgs a{};
+    a.in = (const uint4 *)in;
+    a.out = (uint4 *)out;
+    a.w = img;
+    a.bias = bias;
+    a.din = act_dims(nx, ny, nz, cin);
+    a.dout = act_dims(nx, ny, nz, cout);
+    a.relu = 1;
+    a.err = err;
+    int rc = conv3_fwd(cin, cout, a, s); // warm-up
+    cudaEventRecord(e0, s);
+    for (int q = 0; q < reps && rc == 0; q++) rc = conv3_fwd(cin, cout, a, s);
+    cudaEventRecord(e1, s);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(img);
+    cudaFree(err);
+    if (rc == -2) return HICARW_ERR_ARG;
+    if (rc != 0 || e != cudaSuccess || herr) return HICARW_ERR_CUDA;
+    return HICARW_OK;
+}
+
 // Accumulate the weight and bias gradients of one convolution (caller zeroes dw, db).
 extern "C" int hicarw_nn_conv3_wgrad(int cin, int cout, int nx, int ny, int nz, const void *x, const void *dy, float *dw,
                                      float *db, void *stream)

@@ -276,9 +276,9 @@ def train(net: UNet, pairs, steps: int, lr: float = 1e-3, batch: int = 4, seed: 
 
 
 def conv_benchmark(cin: int, cout: int, nx: int, ny: int, nz: int, reps: int = 5, seed: int = 0):
-    """Time the tensor-core convolution (forward) on random act-layout data:
-    returns ms per call, achieved TFLOP/s (54 cin cout flop per cell) and GB/s
-    (2 (cin + cout) bytes per cell)."""
+    """Time the tensor-core convolution (forward, bias + ReLU) on random act-layout
+    data with CUDA events around `reps` launches: returns ms per launch, achieved
+    TFLOP/s (54 cin cout flop per cell) and GB/s (2 (cin + cout) bytes per cell)."""
     torch = _torch()
     g = torch.Generator(device="cuda").manual_seed(seed)
     x = act_empty(nx, ny, nz, cin)
@@ -290,21 +290,12 @@ def conv_benchmark(cin: int, cout: int, nx: int, ny: int, nz: int, reps: int = 5
     lib = _capi.load()
     s = torch.cuda.current_stream().cuda_stream
 
-    def call():
-        rc = lib.hicarw_nn_conv3(cin, cout, nx, ny, nz, _ptr(x), _ptr(w), _ptr(b), None, None, 1, 0, _ptr(out), None,
-                                 C.c_void_p(s))
-        if rc != 0:
-            raise RuntimeError(f"hicarw_nn_conv3 failed ({rc})")
-
-    call()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(reps):
-        call()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+    t = C.c_float()
+    rc = lib.hicarw_nn_conv3_time(cin, cout, nx, ny, nz, _ptr(x), _ptr(w), _ptr(b), _ptr(out), reps, C.c_void_p(s),
+                                  C.byref(t))
+    if rc != 0:
+        raise RuntimeError(f"hicarw_nn_conv3_time failed ({rc})")
+    ms = t.value
     cells = nx * ny * nz
     return {"cin": cin, "cout": cout, "grid": [nx, ny, nz], "ms": ms,
             "tflops": 54.0 * cin * cout * cells / (ms * 1e-3) / 1e12,

@@ -317,6 +317,9 @@ int hicarw_nn_act_pitch(int nx);
  * FP32 at the interior index (j*nz + k)*nx + i. */
 int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const void *in, const float *w, const float *bias,
                     const void *skip, const void *mask, int relu, int transpose, void *out, float *out0, void *stream);
+/* Mean duration in ms (CUDA events) of `reps` forward launches (bias + ReLU), weights packed once. */
+int hicarw_nn_conv3_time(int cin, int cout, int nx, int ny, int nz, const void *in, const float *w, const float *bias,
+                         void *out, int reps, void *stream, float *ms);
 /* dw[t][ci][co] += sum_v dy[v][co] x[v + off(t)][ci];  db[co] += sum_v dy[v][co]. */
 int hicarw_nn_conv3_wgrad(int cin, int cout, int nx, int ny, int nz, const void *x, const void *dy, float *dw,
                           float *db, void *stream);
