@@ -56,9 +56,11 @@ WORKLOADS = {
 # from these.
 # mixed1024: 1245, the count of the same method (plain BiCGStab, FP64 Krylov) on the GPU.
 REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
-# DRAM bytes per launch of the dominant kernel from one ncu capture
-# (profiles/*.md give the command and the figures); keyed workload:solver:kernel.
-TRAFFIC = {}
+# DRAM bytes per interior cell of one launch of a dominant kernel, from one ncu
+# capture on a smaller case (profiles/mg_post_l0_mid256.md: 290.45 MB for the
+# 256x256x48 = 3145728 cells of that launch); the kernel reads and writes each
+# cell's data once, so its traffic scales with the cells of the workload.
+TRAFFIC_PER_CELL = {"mg_post_l0": 290.454272e6 / (256 * 256 * 48)}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
@@ -242,7 +244,7 @@ def run_reference(args, wl):
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
-def profile_roofline(lib, h, stream, ncu_range: bool, traffic_key: str):
+def profile_roofline(lib, h, stream, ncu_range: bool, cells: int):
     """Per-launch CUDA-event profile of one solve iteration of handle h (every
     kernel of the iteration launched on its own, timed on `stream`) -> the
     roofline object of the dominant kernel."""
@@ -271,7 +273,8 @@ def profile_roofline(lib, h, stream, ncu_range: bool, traffic_key: str):
     peak, peak_kind = peaks()
     ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
-            "frac": ach / peak, "peak_kind": peak_kind, "traffic": TRAFFIC.get(f"{traffic_key}:{dom_k['kernel']}"),
+            "frac": ach / peak, "peak_kind": peak_kind,
+            "traffic": (TRAFFIC_PER_CELL[dom_k["kernel"]] * cells if dom_k["kernel"] in TRAFFIC_PER_CELL else None),
             "share": dom_k["share_ms"] / tot,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
 
@@ -435,7 +438,7 @@ def run_ours(args, wl):
     e2e_value = world * e2e_steps / (te / 1000.0)
 
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
-    roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", f"{args.workload}:{args.solver}")
+    roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", dom.nx * dom.ny * dom.nz)
 
     # ---- accuracy: this solver's lambda / winds / final divergence against a tight FP64 solve ----
     accuracy = None
@@ -581,7 +584,8 @@ def run_batch(args, wl):
         te = float(tt.item())
     e2e_value = world * e2e_steps * bs.n / (te / 1000.0)
     big = max(range(bs.n), key=lambda i: bs.domains[i].nx * bs.domains[i].ny * bs.domains[i].nz)
-    roofline = profile_roofline(lib, bs.handles[big], stream, False, f"{args.workload}:batch")
+    d_big = bs.domains[big]
+    roofline = profile_roofline(lib, bs.handles[big], stream, False, d_big.nx * d_big.ny * d_big.nz)
     if roofline:
         d = bs.domains[big]
         roofline["profiled_subdomain"] = [d.nx, d.ny, d.nz]
