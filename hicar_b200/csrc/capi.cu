@@ -617,15 +617,11 @@ static void fgmres_enqueue_cycle(const FgmresCtx &f, cudaStream_t s)
     fgmres_enqueue_finish(f, s);
 }
 
-static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
+// buffers, launch context and (learned preconditioner) operator features of an FGMRES solve
+static int fgmres_ready(hicarw_handle *h, int sweeps, cudaStream_t s, FgmresCtx *f)
 {
-    FgmresCtx f;
-    int rc = fgmres_prepare(h, sweeps, &f);
+    int rc = fgmres_prepare(h, sweeps, f);
     if (rc) return rc;
-    const int m = f.m;
-    fgmres_reset(h->gst, m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
-    CK(cudaEventRecord(h->t0, s));
-    // one restart cycle = one graph
     if (h->use_learned && h->unet_dirty) {
         if (unet_prepare_operator(h->unet, opctx(h), s) != 0) {
             h->err = "learned preconditioner grid mismatch";
@@ -633,6 +629,39 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
         }
         h->unet_dirty = 0;
     }
+    return 0;
+}
+
+// the FGMRES device state mapped onto the solve-state mirror (stats), with the
+// FP64 true residual of the solution
+static int fgmres_map_state(hicarw_handle *h, int stalled, cudaStream_t s)
+{
+    GmresState gh;
+    CK(cudaMemcpyAsync(&gh, h->gst, sizeof(GmresState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+    int rc;
+    if ((rc = fetch_state(h, s)) != 0) return rc;
+    h->hst->status = stalled ? 4 : gh.status;
+    h->hst->it = gh.it_total;
+    h->hst->res0 = gh.res0;
+    h->hst->rnorm = gh.res;
+    h->hst->bnorm2 = gh.bnorm * gh.bnorm;
+    h->hst->target = gh.target;
+    return 0;
+}
+
+static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
+{
+    FgmresCtx f;
+    int rc = fgmres_ready(h, sweeps, s, &f);
+    if (rc) return rc;
+    const int m = f.m;
+    fgmres_reset(h->gst, m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
+    CK(cudaEventRecord(h->t0, s));
+    // one restart cycle = one graph
     const int pkind = h->use_learned ? HICARW_PRECOND_LEARNED : (h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI);
     GraphKey key{HICARW_KRYLOV_F64, sweeps, m, HICARW_SOLVER_FGMRES, 0, pkind};
     auto it = h->graphs.find(key);
@@ -673,21 +702,7 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
         // not converged within the cycle: the next launch restarts from the current x
     }
     CK(cudaEventRecord(h->t1, s));
-    // map onto the BiCGStab state mirror for stats
-    GmresState gh;
-    CK(cudaMemcpyAsync(&gh, h->gst, sizeof(GmresState), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    OpCtx c = opctx(h);
-    RedBuf rb{h->partials, h->red_blocks};
-    launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
-    if ((rc = fetch_state(h, s)) != 0) return rc;
-    h->hst->status = stalled ? 4 : gh.status;
-    h->hst->it = gh.it_total;
-    h->hst->res0 = gh.res0;
-    h->hst->rnorm = gh.res;
-    h->hst->bnorm2 = gh.bnorm * gh.bnorm;
-    h->hst->target = gh.target;
-    return 0;
+    return fgmres_map_state(h, stalled, s);
 }
 
 static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retries)
@@ -1404,6 +1419,7 @@ struct hicarw_batch {
     long long nodes = 0;
     std::vector<hicarw_batch_item> built;
     int built_lanes = -1, built_chunk = -1, built_cold = -1;
+    std::vector<FgmresCtx> fg; // launch contexts of the FGMRES subdomains
     int *counters = nullptr; // device: WHILE-body executions per subdomain
     unsigned long long *stamps = nullptr; // device: %globaltimer at each solve's end, [n] = batch start
     cudaStream_t cap = nullptr;
@@ -1434,6 +1450,15 @@ static cudaError_t batch_stamp_node(hicarw_batch *b, cudaGraph_t g, const cudaGr
     e = cudaGraphAddChildGraphNode(out, g, dep, ndep, sg);
     cudaGraphDestroy(sg);
     return e;
+}
+
+// FGMRES subdomains loop over restart cycles until converged or out of iterations
+__global__ void batch_fg_cond_kernel(cudaGraphConditionalHandle hc, const GmresState *g, int *count, int limit)
+{
+    const int c = *count + 1;
+    *count = c;
+    const int more = g->status != 0 && g->it_total < g->max_iters && c < limit;
+    cudaGraphSetConditional(hc, more ? 1u : 0u);
 }
 
 __global__ void batch_cond_kernel(cudaGraphConditionalHandle hc, const SolveState *st, int *count, int limit)
@@ -1471,11 +1496,16 @@ static void batch_enqueue_setup(hicarw_batch *b, int i, const hicarw_batch_item 
     cudaMemcpyAsync(h->div, it.div, n_cell(d) * 4, cudaMemcpyDeviceToDevice, s);
     if (cold) cudaMemsetAsync(h->vec[V_X], 0, (size_t)d.npad * 8, s);
     prepare_system(h, s);
-    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->use_mg ? h->opt.stall_iters : 0, s);
-    OpCtx c = opctx(h);
-    RedBuf rb{h->partials, h->red_blocks};
-    launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R), V<double>(h, V_RHAT),
-                                 V<double>(h, V_P), h->st, h->hist, rb, s);
+    if (h->opt.solver == HICARW_SOLVER_FGMRES) {
+        fgmres_reset(h->gst, b->fg[i].m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
+    } else {
+        launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->use_mg ? h->opt.stall_iters : 0,
+                           s);
+        OpCtx c = opctx(h);
+        RedBuf rb{h->partials, h->red_blocks};
+        launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
+                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+    }
     batch_count_reset_kernel<<<1, 1, 0, s>>>(b->counters + i);
     count_launch(1);
 }
@@ -1535,10 +1565,14 @@ static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold
         g_capture_nodes = 0;
         e = cudaStreamBeginCaptureToGraph(b->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) { g_capturing = 0; break; }
-        for (int q = 0; q < b->chunk; q++)
-            enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, b->cap);
-        const int limit = h->opt.max_iters / b->chunk + 2;
-        batch_cond_kernel<<<1, 1, 0, b->cap>>>(hc, h->st, b->counters + i, limit);
+        if (h->opt.solver == HICARW_SOLVER_FGMRES) { // body: one restart cycle
+            fgmres_enqueue_cycle(b->fg[i], b->cap);
+            batch_fg_cond_kernel<<<1, 1, 0, b->cap>>>(hc, h->gst, b->counters + i, h->opt.max_iters / b->fg[i].m + 2);
+        } else {
+            for (int q = 0; q < b->chunk; q++)
+                enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, b->cap);
+            batch_cond_kernel<<<1, 1, 0, b->cap>>>(hc, h->st, b->counters + i, h->opt.max_iters / b->chunk + 2);
+        }
         count_launch(1);
         e = cudaStreamEndCapture(b->cap, &body);
         g_capturing = 0;
@@ -1571,11 +1605,13 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
     int rc;
     bool rebuild = !b->exec || !same_items(b, items) || b->built_lanes != b->lanes || b->built_chunk != b->chunk ||
                    b->built_cold != cold;
+    b->fg.resize(n);
     for (int i = 0; i < n; i++) {
         hicarw_handle *h = b->hs[i];
         h->launches_at_call = g_launches.load();
         h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed;
-        h->use_learned = 0;
+        h->use_learned = h->opt.solver == HICARW_SOLVER_FGMRES && h->opt.precond == HICARW_PRECOND_LEARNED &&
+                         h->operator_probed && h->unet != nullptr;
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
             h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
         h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
@@ -1585,6 +1621,13 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
             }
             h->mg_dirty = 0;
             rebuild = true;
+        }
+        if (h->opt.solver == HICARW_SOLVER_FGMRES) {
+            const bool dirty = h->use_learned && h->unet_dirty;
+            FgmresCtx f;
+            if ((rc = fgmres_ready(h, h->precond_n_sweeps, s, &f)) != 0) return rc;
+            if (dirty || b->fg[i].V != f.V || b->fg[i].m != f.m) rebuild = true;
+            b->fg[i] = f;
         }
     }
     if (rebuild) {
@@ -1601,10 +1644,12 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         BCK(cudaMemcpyAsync(b->hs[i]->hst, b->hs[i]->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     BCK(cudaStreamSynchronize(s));
     BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
+    for (int i = 0; i < n; i++) // FGMRES state -> the solve-state mirror
+        if (b->hs[i]->opt.solver == HICARW_SOLVER_FGMRES && (rc = fgmres_map_state(b->hs[i], 0, s)) != 0) return rc;
     std::vector<int> fell(n, 0);
     for (int i = 0; i < n; i++) { // a stalled or failed preconditioned solve: the reference solve decides
         hicarw_handle *h = b->hs[i];
-        if (h->hst->status != 0 && h->use_mg) {
+        if (h->hst->status != 0 && (h->use_mg || h->use_learned)) {
             if ((rc = zero_solution(h, s)) != 0 || (rc = bicgstab_solve(h, h->precond_n_sweeps, s, 0)) != 0) {
                 fprintf(stderr, "hicarw batch: fallback solve of subdomain %d: %s\n", i, h->err.c_str());
                 return rc;
@@ -1616,9 +1661,12 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         hicarw_handle *h = b->hs[i];
         OpCtx c = opctx(h);
         RedBuf rb{h->partials, h->red_blocks};
-        launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+        if (h->opt.solver != HICARW_SOLVER_FGMRES || fell[i])
+            launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0,
+                                                 rb, s);
         if (apply) enqueue_winds(h, adv_den ? items[i].density : nullptr, adv_den, items[i].u, items[i].v, items[i].w, s);
-        BCK(cudaMemcpyAsync(h->hst, h->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+        if (h->opt.solver != HICARW_SOLVER_FGMRES || fell[i]) // FGMRES stats were mapped above
+            BCK(cudaMemcpyAsync(h->hst, h->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     }
     BCK(cudaStreamSynchronize(s));
     if (stats)
@@ -1638,9 +1686,10 @@ extern "C" int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_
     if (n < 1 || !handles || !out) return HICARW_ERR_ARG;
     for (int i = 0; i < n; i++) {
         hicarw_handle *h = handles[i];
-        if (!h || !h->operator_probed || h->opt.solver != HICARW_SOLVER_REFERENCE ||
-            h->opt.krylov_precision != HICARW_KRYLOV_F64)
-            return HICARW_ERR_ARG; // calibrated handles with the reference schedule and FP64 Krylov vectors
+        const bool bicg = h && h->opt.solver == HICARW_SOLVER_REFERENCE && h->opt.krylov_precision == HICARW_KRYLOV_F64;
+        const bool fgm = h && h->opt.solver == HICARW_SOLVER_FGMRES;
+        if (!h || !h->operator_probed || !(bicg || fgm))
+            return HICARW_ERR_ARG; // calibrated handles: FP64 BiCGStab (reference schedule) or FGMRES
         for (int q = 0; q < i; q++)
             if (handles[q] == h) return HICARW_ERR_ARG;
         if (ensure_vectors(h, HICARW_KRYLOV_F64) != 0) return HICARW_ERR_CUDA;

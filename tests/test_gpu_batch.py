@@ -100,3 +100,43 @@ def test_batch_stall_falls_back():
         assert np.isfinite(bs.lambda_of(0).cpu().numpy()).all()
     finally:
         bs.close()
+
+
+def test_batch_mixes_fgmres_and_learned_with_bicgstab():
+    """One batch holding a Jacobi BiCGStab ("plain") subdomain, an MG BiCGStab one,
+    an MG-FGMRES one and a learned-FGMRES one: each matches its own single solve
+    (same kernels, same order: bit-exact)."""
+    from hicar_b200 import learned as L
+    from hicar_b200.batch import BatchSolver
+    from hicar_b200.train_unet import load_params
+    from hicar_b200.wind_iterative import WindOptions
+    cs = _cases()[:4]
+    bs = BatchSolver(cs)
+    try:
+        lib = _capi.load()
+        opts = [WindOptions(tol_rel=1e-6, wind_solver_iterations=3000),
+                WindOptions(tol_rel=1e-6, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50),
+                WindOptions(tol_rel=1e-6, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                            solver=_capi.SOLVER_FGMRES),
+                WindOptions(tol_rel=1e-6, wind_solver_iterations=3000, precond=_capi.PRECOND_LEARNED,
+                            solver=_capi.SOLVER_FGMRES, stall_iters=100)]
+        nets = []
+        for h, o, d in zip(bs.handles, opts, bs.domains):
+            _capi.check(lib.hicarw_set_options(h, C.byref(o.to_c())), h)
+            if o.precond == _capi.PRECOND_LEARNED:
+                net = L.UNet(d.nx, d.ny, d.nz)
+                net.set_params(torch.from_numpy(load_params()))
+                net.attach(h)
+                nets.append(net)
+        stats = bs.step()
+        lam_b = [bs.lambda_of(i).cpu() for i in range(bs.n)]
+        kinds = [s["precond"] for s in stats]
+        assert kinds == [_capi.PRECOND_JACOBI, _capi.PRECOND_MG, _capi.PRECOND_MG, _capi.PRECOND_LEARNED]
+        for i in range(bs.n):
+            st, lam, _ = _single(bs, i)
+            assert stats[i]["status"] == 0 and st["status"] == 0
+            assert stats[i]["iterations"] == st["iterations"]
+            assert stats[i]["true_res"] <= 1.05 * stats[i]["target"]
+            assert torch.equal(lam_b[i], lam)
+    finally:
+        bs.close()
