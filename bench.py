@@ -64,6 +64,7 @@ TRAFFIC_PER_CELL = {"mg_post_l0": 290.454272e6 / (256 * 256 * 48)}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
+FGMRES_RESTART = None  # --fgmres-restart
 
 
 def peaks():
@@ -101,6 +102,8 @@ def solver_options(name: str):
         kw["mg_coarse_scale"] = MG_COARSE_SCALE
     if MG_OMEGA is not None and "precond" in kw:
         kw["mg_omega"] = MG_OMEGA
+    if FGMRES_RESTART is not None and "fgmres_restart" in kw:
+        kw["fgmres_restart"] = FGMRES_RESTART
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
 
 
@@ -623,7 +626,7 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL, MG_COARSE_SCALE, MG_OMEGA
+    global TOL, MG_COARSE_SCALE, MG_OMEGA, FGMRES_RESTART
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -637,6 +640,8 @@ def main():
                     help="override the V-cycle's coarse-correction scale of the solver preset")
     ap.add_argument("--mg-omega", type=float, default=None,
                     help="override the V-cycle's smoother damping of the solver preset")
+    ap.add_argument("--fgmres-restart", type=int, default=None,
+                    help="override the restart length of the FGMRES presets")
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=None,
                     help="iterations of the reference method on the workload (reference arm)")
@@ -648,6 +653,7 @@ def main():
     TOL = args.tol
     MG_COARSE_SCALE = args.mg_coarse_scale
     MG_OMEGA = args.mg_omega
+    FGMRES_RESTART = args.fgmres_restart
     wl = WORKLOADS[args.workload]
     if "batch" in wl:
         if args.impl == "reference":

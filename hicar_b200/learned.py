@@ -214,28 +214,56 @@ def calibrated_handle(case):
     return dom, wi.handle(dom.nest_indx)
 
 
-def training_pairs(case, net: UNet, n_samples: int, seed: int = 0, solve: bool = False, tol: float = 1e-8):
-    """Training samples of one terrain case: for random residuals r (random_residual)
-    the network input features x0, the unit-rms residual rhat = r / rms(r) (FP32,
-    (ny, nz, nx)) and the operator's FP32 coefficients (15, ny, nz, nx), which the
-    residual loss ||A z - rhat||^2 needs.  With solve=True also the exact step
-    e = A^-1 r (FGMRES + multigrid to `tol`) as the target e * coef_A / rms(r) of
-    the supervised loss.  Each sample is (x0, rhat, coefs, target or None).
-    The handles made here are released again."""
+SOLVER_ITERS = (1, 3, 8, 16, 32, 64, 128, 256)  # plain-solver iterations whose residuals are logged
+
+
+def training_pairs(case, net: UNet, n_samples: int, seed: int = 0, solve: bool = False, tol: float = 1e-8,
+                   source: str = "random"):
+    """Training samples of one terrain case: the network input features x0 of a
+    residual r, the unit-rms residual rhat = r / rms(r) (FP32, (ny, nz, nx)) and the
+    operator's FP32 coefficients (15, ny, nz, nx), which the residual loss
+    ||A z - rhat||^2 needs.  source="random": r from random_residual;
+    source="solver": r = b - A x_k, the residual after k = SOLVER_ITERS[(q + seed) % 8] iterations
+    of the plain (Jacobi-preconditioned) BiCGStab on the case's own right-hand
+    side b = -2 div(u, v, w), i.e. the residuals the solver itself produces.  With
+    solve=True also the exact step e = A^-1 r (FGMRES + multigrid to `tol`) as the
+    target e * coef_A / rms(r) of the supervised loss.  Each sample is
+    (x0, rhat, coefs, target or None).  The handles made here are released again."""
     torch = _torch()
     from . import wind, wind_iterative as wi
     dom, h = calibrated_handle(case)
     lib = _capi.load()
-    wi.set_options(wi.WindOptions(tol_rel=tol, wind_solver_iterations=2000, solver=_capi.SOLVER_FGMRES,
-                                  precond=_capi.PRECOND_MG))
+    exact = wi.WindOptions(tol_rel=tol, wind_solver_iterations=2000, solver=_capi.SOLVER_FGMRES,
+                           precond=_capi.PRECOND_MG)
+    wi.set_options(exact)
     coefs = torch.empty((15, dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
     _capi.check(lib.hicarw_get_coefs(h, _ptr(coefs), _capi.MEM_DEVICE, None), h)
     diag = coefs[0].double()
     gen = torch.Generator().manual_seed(seed)
+    b = None
+    if source == "solver":
+        div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+        dom.set_winds(case.u, case.v, case.w)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        b = torch.zeros((dom.ny + 2, dom.nz + 2, dom.nx + 2), dtype=torch.float64, device="cuda")
+        b[1:-1, 1:-1, 1:-1] = -2.0 * div.double()  # compute_rhs_3d (wind_iterative.F90:1513-1530)
     out = []
     st = _capi.Stats()
-    for _ in range(n_samples):
-        r = random_residual(dom.nx, dom.ny, dom.nz, gen)
+    for q in range(n_samples):
+        if source == "solver":
+            k = SOLVER_ITERS[(q + seed) % len(SOLVER_ITERS)]
+            wi.set_options(wi.WindOptions(tol_rel=1e-30, tol_abs=0.0, wind_solver_iterations=k))
+            lib.hicarw_reset_solution(h, None)
+            _capi.check(lib.hicarw_solve_rhs(h, _ptr(b), _capi.MEM_DEVICE, None, C.byref(st)), h)
+            xk = torch.empty_like(b)
+            _capi.check(lib.hicarw_get_lambda(h, _ptr(xk), _capi.MEM_DEVICE, None), h)
+            ax = torch.empty_like(b)
+            _capi.check(lib.hicarw_apply_operator(h, _ptr(xk), _ptr(ax), _capi.MEM_DEVICE, None), h)
+            r = b - ax
+            r[0], r[-1], r[:, 0], r[:, -1], r[:, :, 0], r[:, :, -1] = 0, 0, 0, 0, 0, 0
+            wi.set_options(exact)
+        else:
+            r = random_residual(dom.nx, dom.ny, dom.nz, gen)
         x0, rms = net.features(h, r)
         rhat = (r[1:-1, 1:-1, 1:-1] / rms).float().contiguous()
         target = None

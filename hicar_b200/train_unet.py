@@ -5,8 +5,9 @@ parameters (FP32 .npy), e.g.
         --samples 8 --steps 2000 --out hicar_b200/weights/unet_128x128x32.npy
 
 Terrains are the seeded generator's cases (hicar_b200.cases, seeds
---seed0 .. --seed0 + terrains - 1); every sample is a random residual of one
-terrain's calibrated operator, and the loss is the residual loss
+--seed0 .. --seed0 + terrains - 1); the samples of a terrain are random
+residuals and/or the residuals of the plain solver's iterates on the terrain's
+own right-hand side (--source), and the loss is the residual loss
 mean((A z - rhat)^2) of hicar_b200.learned.train.  The network is
 convolutional, so parameters trained on one grid size serve any other
 (load_params / UNet.set_params)."""
@@ -42,6 +43,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed0", type=int, default=1000)
     ap.add_argument("--hills", type=int, default=20)
+    ap.add_argument("--source", default="random", choices=["random", "solver", "mixed"],
+                    help="residuals: random fields, the plain solver's iterates, or half of each")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     args = ap.parse_args(argv)
 
@@ -53,7 +56,12 @@ def main(argv=None):
     pairs = []
     for t in range(args.terrains):
         case = cases.build_case(args.nx, args.ny, args.nz, seed=args.seed0 + t, adv_den=True, n_hills=args.hills)
-        pairs += L.training_pairs(case, net, args.samples, seed=args.seed0 + t)
+        if args.source in ("random", "mixed"):
+            pairs += L.training_pairs(case, net, args.samples if args.source == "random" else args.samples // 2,
+                                      seed=args.seed0 + t)
+        if args.source in ("solver", "mixed"):
+            pairs += L.training_pairs(case, net, args.samples if args.source == "solver" else args.samples // 2,
+                                      seed=args.seed0 + t, source="solver")
     torch.cuda.synchronize()
     t_data = time.time() - t0
     t0 = time.time()
@@ -68,6 +76,7 @@ def main(argv=None):
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.save(args.out, p)
     info = {"grid": [args.nx, args.ny, args.nz], "terrains": args.terrains, "samples": args.samples,
+            "source": args.source,
             "steps": args.steps, "batch": args.batch, "lr": args.lr, "seed0": args.seed0,
             "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
             "data_s": t_data, "train_s": t_train, "params": int(p.size)}
