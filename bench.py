@@ -163,6 +163,21 @@ def dist_setup():
     return rank, world, local
 
 
+def reduce_max(value: float, dist, device) -> float:
+    """The maximum of `value` over all ranks (the job's time is the slowest rank's)."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def subdomain_seed(rank: int) -> int:
+    """Each rank solves its own independent subdomain(s): seeds 1, 2, ... by rank."""
+    return 1 + rank
+
+
 def build_inputs(wl: dict, seed: int):
     from hicar_b200 import cases
     return cases.build_case(wl["nx"], wl["ny"], wl["nz"], wl["dx"], wl["n_hills"], seed=seed,
@@ -333,7 +348,7 @@ def run_ours(args, wl):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     lib = _capi.load()
-    case = build_inputs(wl, seed=1 + rank)
+    case = build_inputs(wl, seed=subdomain_seed(rank))
     dom = DeviceDomain.from_case(case, f"cuda:{local}")
     u0, v0, w0 = dom.u_dqdt.clone(), dom.v_dqdt.clone(), dom.w_dqdt.clone()
     stream = torch.cuda.current_stream()
@@ -397,10 +412,7 @@ def run_ours(args, wl):
     launches = lib.hicarw_kernel_launches() - l0
     clocks = sampler.stop()
     t_ms = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([t_ms], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = reduce_max(t_ms, dist, f"cuda:{local}")
     value = world * args.steps / (t_ms / 1000.0)
 
     # ---- e2e: the same step with host (pinned) winds copied in and out every step ----
@@ -434,10 +446,7 @@ def run_ours(args, wl):
     e1.record()
     torch.cuda.synchronize()
     te = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([te], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = reduce_max(te, dist, f"cuda:{local}")
     e2e_value = world * e2e_steps / (te / 1000.0)
 
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
@@ -505,7 +514,8 @@ def run_batch(args, wl):
     stream = torch.cuda.current_stream()
     opts = WindOptions(tol_rel=TOL, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50,
                        advect_density=wl["adv_den"])
-    bs = BatchSolver(subdomain_cases(wl["batch"], seed=1 + rank, nxy=wl["nxy"], nz=wl["nz"], n_hills=wl["n_hills"],
+    bs = BatchSolver(subdomain_cases(wl["batch"], seed=subdomain_seed(rank), nxy=wl["nxy"], nz=wl["nz"],
+                                     n_hills=wl["n_hills"],
                                      dx=wl["dx"]), options=opts, stream=stream.cuda_stream)
     tuned_ms = bs.autotune()
     lanes, chunk = bs.config()
@@ -545,10 +555,7 @@ def run_batch(args, wl):
     launches = lib.hicarw_kernel_launches() - l0
     clocks = sampler.stop()
     t_ms = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([t_ms], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = reduce_max(t_ms, dist, f"cuda:{local}")
     value = world * args.steps * bs.n / (t_ms / 1000.0)
     # e2e: every subdomain's winds from pinned host memory in, corrected winds out
     host = [[torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in sv] for sv in bs.saved]
@@ -581,10 +588,7 @@ def run_batch(args, wl):
     e1.record()
     torch.cuda.synchronize()
     te = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([te], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = reduce_max(te, dist, f"cuda:{local}")
     e2e_value = world * e2e_steps * bs.n / (te / 1000.0)
     big = max(range(bs.n), key=lambda i: bs.domains[i].nx * bs.domains[i].ny * bs.domains[i].nz)
     d_big = bs.domains[big]
