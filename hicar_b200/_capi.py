@@ -27,7 +27,7 @@ EXPORTS = [
     "hicarw_probe_apply_corrections", "hicarw_probe_record", "hicarw_probe_finalize",
     "hicarw_calibrate_projection_operator", "hicarw_reset_solution", "hicarw_get_lambda", "hicarw_get_coefs",
     "hicarw_set_coefs", "hicarw_apply_operator", "hicarw_apply_precond", "hicarw_solve_rhs", "hicarw_set_options",
-    "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_profile_iteration",
+    "hicarw_get_history", "hicarw_last_error", "hicarw_kernel_launches", "hicarw_mg_tma_launches", "hicarw_profile_iteration",
     "hicarw_residual_norm_noalloc", "hicarw_nn_act_pitch", "hicarw_nn_conv3", "hicarw_nn_conv3_wgrad",
     "hicarw_nn_conv3_time",
     "hicarw_unet_create", "hicarw_unet_destroy", "hicarw_unet_grid", "hicarw_unet_num_params",
@@ -118,6 +118,7 @@ def load(path: str = LIB_PATH):
         "hicarw_get_history": (ci, [vp, vp, ci]),
         "hicarw_last_error": (C.c_char_p, [vp]),
         "hicarw_kernel_launches": (C.c_longlong, []),
+        "hicarw_mg_tma_launches": (C.c_longlong, []),
         "hicarw_profile_iteration": (ci, [vp, ci, vp, vp, vp, vp, ci, vp]),
         "hicarw_residual_norm_noalloc": (ci, [vp, vp, vp, vp, vp]),
         "hicarw_nn_act_pitch": (ci, [ci]),

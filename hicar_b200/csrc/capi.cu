@@ -477,6 +477,10 @@ static int fetch_state(hicarw_handle *h, cudaStream_t s)
 {
     CK(cudaMemcpyAsync(h->hst, h->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (h->hst->err) {
+        h->err = "a bounded device-side wait timed out (multigrid smoother copies)";
+        return HICARW_ERR_CUDA;
+    }
     return 0;
 }
 
@@ -1152,6 +1156,11 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
             mg_apply<double>(h->mg, bx, by, nullptr, s);
             rc = get_padded(h, by, y, mem_kind, s);
         }
+        int herr = 0;
+        if (!rc && cudaMemcpy(&herr, h->mg.err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && herr) {
+            h->err = "a bounded device-side wait timed out (multigrid smoother copies)";
+            rc = HICARW_ERR_CUDA;
+        }
     } else if (!rc) {
         launch_diag<double>(d, h->coef, h->dz_if, bd, h->operator_probed, s);
         OpCtx c = opctx(h);
@@ -1210,6 +1219,7 @@ extern "C" int hicarw_get_history(hicarw_handle *h, double *out, int cap)
 extern "C" const char *hicarw_last_error(hicarw_handle *h) { return h ? h->err.c_str() : g_err_noh.c_str(); }
 
 extern "C" long long hicarw_kernel_launches(void) { return g_launches.load(); }
+extern "C" long long hicarw_mg_tma_launches(void) { return mg_tma_posts(); }
 
 // ---- per-kernel profile of one solve iteration ------------------------------
 __global__ void prof_state_kernel(SolveState *s, int on)
@@ -1644,6 +1654,11 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         BCK(cudaMemcpyAsync(b->hs[i]->hst, b->hs[i]->st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     BCK(cudaStreamSynchronize(s));
     BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
+    for (int i = 0; i < n; i++)
+        if (b->hs[i]->hst->err) {
+            fprintf(stderr, "hicarw batch: subdomain %d: a bounded device-side wait timed out\n", i);
+            return HICARW_ERR_CUDA;
+        }
     for (int i = 0; i < n; i++) // FGMRES state -> the solve-state mirror
         if (b->hs[i]->opt.solver == HICARW_SOLVER_FGMRES && (rc = fgmres_map_state(b->hs[i], 0, s)) != 0) return rc;
     std::vector<int> fell(n, 0);

@@ -16,11 +16,18 @@
 // Internals run in FP32 (the preconditioner precision); the outer BiCGStab
 // vectors it reads and writes stay FP64.  The V-cycle is a fixed linear map
 // (deterministic kernels, fixed level count), so plain BiCGStab applies.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <stdlib.h>
+
+#include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "common.cuh"
 #include "kernels.h"
 #include "mg.h"
+#include "tc05.cuh"
 
 namespace hw {
 
@@ -100,18 +107,50 @@ __global__ void factor_kernel(Dims d, const float *__restrict__ coef, float *__r
 
 // Thomas recurrences of one column held in shared memory ([k][c] layout, stride tc):
 // res <- T^-1 res, with T = tridiag(C, 1/m-form factors) and couplings to the ghost planes dropped.
+// The operands of THOMAS_U levels are read ahead into registers, so that only
+// the multiply-add chain is serial (the same operations in the same order as
+// a level-by-level loop).
+constexpr int THOMAS_U = 8;
+
 __device__ __forceinline__ void thomas_column(float *s_res, const float *s_c, const float *s_m, const float *s_cp,
                                               int c, int tc, int nz)
 {
     float dprev = 0.0f;
-    for (int k = 0; k < nz; k++) {
+    int k = 0;
+    for (; k + THOMAS_U <= nz; k += THOMAS_U) {
+        float rv[THOMAS_U], cv[THOMAS_U], mv[THOMAS_U];
+#pragma unroll
+        for (int u = 0; u < THOMAS_U; u++) {
+            int t = (k + u) * tc + c;
+            rv[u] = s_res[t]; cv[u] = s_c[t]; mv[u] = s_m[t];
+        }
+#pragma unroll
+        for (int u = 0; u < THOMAS_U; u++) {
+            dprev = (rv[u] - cv[u] * dprev) * mv[u];
+            s_res[(k + u) * tc + c] = dprev;
+        }
+    }
+    for (; k < nz; k++) {
         int t = k * tc + c;
-        float dv = (s_res[t] - s_c[t] * dprev) * s_m[t];
-        s_res[t] = dv;
-        dprev = dv;
+        dprev = (s_res[t] - s_c[t] * dprev) * s_m[t];
+        s_res[t] = dprev;
     }
     float y = 0.0f;
-    for (int k = nz - 1; k >= 0; k--) {
+    k = nz - 1;
+    for (; k + 1 >= THOMAS_U; k -= THOMAS_U) {
+        float rv[THOMAS_U], pv[THOMAS_U];
+#pragma unroll
+        for (int u = 0; u < THOMAS_U; u++) {
+            int t = (k - u) * tc + c;
+            rv[u] = s_res[t]; pv[u] = s_cp[t];
+        }
+#pragma unroll
+        for (int u = 0; u < THOMAS_U; u++) {
+            y = rv[u] - pv[u] * y;
+            s_res[(k - u) * tc + c] = y;
+        }
+    }
+    for (; k >= 0; k--) {
         int t = k * tc + c;
         y = s_res[t] - s_cp[t] * y;
         s_res[t] = y;
@@ -237,8 +276,10 @@ __device__ __forceinline__ void stage_window(const Dims &d, const float *__restr
 
 // Post-smoothing: out = x2 + w T^-1 (r - A x2) with x2 = x1 + P xc, x2 of the
 // tile and its one-column ring staged in shared memory first.
+constexpr int POST_CELLS = 4; // (column, level) residuals per thread in flight; 3 CTAs per SM by registers
+
 template <typename TR, typename TO, int TX, int TY>
-__global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *__restrict__ coef,
+__global__ void __launch_bounds__(MG_THREADS, 3) post_kernel(Dims d, const float *__restrict__ coef,
                                                           const float *__restrict__ cp,
                                                           const float *__restrict__ minv, const TR *__restrict__ r,
                                                           const float *__restrict__ x1, Dims dc,
@@ -253,10 +294,10 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
     stage_window<SX, SY>(d, x1, dc, xc, i0 - 1, j0 - 1, s_x, cscale);
     __syncthreads();
-    for (int base = threadIdx.x; base < n; base += MG_THREADS * 2) {
-        float res2[2], vc[2], vm[2], vp[2];
+    for (int base = threadIdx.x; base < n; base += MG_THREADS * POST_CELLS) {
+        float res2[POST_CELLS], vc[POST_CELLS], vm[POST_CELLS], vp[POST_CELLS];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < POST_CELLS; u++) {
             int t = base + u * MG_THREADS;
             int c = t % TC, k = t / TC + 1;
             int lx = c % TX, ly = c / TX;
@@ -275,7 +316,7 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
             }
         }
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < POST_CELLS; u++) {
             int t = base + u * MG_THREADS;
             if (t < n) { s_res[t] = res2[u]; s_c[t] = vc[u]; s_m[t] = vm[u]; s_cp[t] = vp[u]; }
         }
@@ -293,6 +334,216 @@ __global__ void __launch_bounds__(MG_THREADS) post_kernel(Dims d, const float *_
         if (i > d.nx || j > d.ny) continue;
         float base = s_x[k * SP + (ly + 1) * SX + (lx + 1)];
         out[kidx(d, i, k, j)] = (TO)((double)base + (double)omega * (double)s_res[t]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Post-smoothing fed by tensor copies.  The same arithmetic as post_kernel
+// (bit-identical results), reorganised so that the loads need no registers:
+// a persistent CTA per SM walks tiles of 32 columns (one j row) and, within a
+// tile, chunks of PT_KC levels.  A producer warp streams every chunk's operands
+// (15 coefficient rows, minv, cp, r, the x1 window and the coarse-correction
+// window) into a PT_NS-stage shared-memory ring with cp.async.bulk.tensor; eight
+// consumer warps form x2 = x1 + s P xc on the chunk's window and the residuals
+// r - A x2 (one (column, level) cell per thread); warp 0 runs the forward
+// Thomas recurrence of the chunk before releasing its stage, and the backward
+// recurrence at the end of the tile, while the ring already fills with the
+// next tile's chunks.  Every wait is bounded: on timeout the kernel sets *err,
+// stops waiting and finishes its loops, so the CTA never hangs.
+// ---------------------------------------------------------------------------
+namespace pt {
+constexpr int TX = 32;                  // columns per tile (x), one j row
+constexpr int KC = 8;                   // levels per chunk: one per consumer warp
+constexpr int NS = 3;                   // ring stages (two CTAs per SM)
+constexpr int CW = 32 * KC;             // consumer threads
+constexpr int THREADS = CW + 32;        // + the producer warp
+constexpr int WX = TX + 2;              // x2 window row: i0-1 .. i0+TX
+constexpr int WK = KC + 2;              // window levels: k0-1 .. k0+KC
+constexpr int X1W = TX + 8;             // staged x1 row: i0-4 .. i0+TX+3 (16-byte aligned start)
+constexpr int XCW = 24;                 // staged coarse row: I0-3 .. I0+20, I0 = i0 >> 1
+constexpr int B_COEF = 15 * KC * TX * 4;
+constexpr int B_ROW = KC * TX * 4;      // minv / cp
+constexpr int B_X1 = 3 * WK * X1W * 4;
+constexpr int B_XC = 2 * WK * XCW * 4;
+constexpr int up128(int b) { return (b + 127) / 128 * 128; }
+constexpr int O_COEF = 0;
+constexpr int O_MINV = O_COEF + B_COEF;
+constexpr int O_CP = O_MINV + B_ROW;
+constexpr int O_X1 = O_CP + B_ROW;
+constexpr int O_XC = O_X1 + up128(B_X1);
+constexpr int O_R = O_XC + up128(B_XC);
+template <typename TR> constexpr int stage_bytes() { return O_R + up128(KC * TX * (int)sizeof(TR)); }
+template <typename TR> constexpr uint32_t tx_bytes() { return B_COEF + 2 * B_ROW + B_X1 + B_XC + KC * TX * sizeof(TR); }
+static_assert(B_COEF % 128 == 0 && B_ROW % 128 == 0, "stage offsets must stay 128-byte aligned");
+
+// dynamic shared memory of a launch for nz levels
+template <typename TR> size_t smem_bytes(int nz)
+{
+    return 128 + (size_t)NS * stage_bytes<TR>() + (size_t)3 * nz * TX * 4 + (size_t)up128(3 * WK * WX * 4) +
+           2 * NS * 8 + 16;
+}
+}  // namespace pt
+
+template <typename TR, typename TO>
+__global__ void __launch_bounds__(pt::THREADS, 2)
+    post_tma_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
+                    const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
+                    const __grid_constant__ CUtensorMap tm_x1, const __grid_constant__ CUtensorMap tm_xc, Dims d,
+                    TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, const SolveState *gate,
+                    int *err)
+{
+    using namespace pt;
+    constexpr int SB = stage_bytes<TR>();
+    extern __shared__ unsigned char pt_smem[];
+    unsigned char *base = (unsigned char *)(((uintptr_t)pt_smem + 127) & ~(uintptr_t)127);
+    const int nz = d.nz, nch = (nz + KC - 1) / KC;
+    float *s_res = (float *)(base + NS * SB);
+    float *s_cp = s_res + nz * TX;
+    float *s_x2c = s_cp + nz * TX;
+    float *s_x2w = s_x2c + nz * TX;
+    uint64_t *full = (uint64_t *)((unsigned char *)s_x2w + up128(3 * WK * WX * 4));
+    uint64_t *empty = full + NS;
+    int *s_skip = (int *)(empty + NS);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
+        for (int q = 0; q < NS; q++) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&empty[q], 1);
+        }
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (s_skip[0]) return; // the same value for every thread
+
+    if (warp == KC) { // ---- producer ----
+        if (lane != 0) return;
+        bool ok = true;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
+            for (int ch = 0; ch < nch; ch++, it++) {
+                const int s = it % NS;
+                if (it >= NS && !tc::mbar_wait(&empty[s], ((it / NS) - 1) & 1)) {
+                    atomicExch(err, 1);
+                    ok = false;
+                    break;
+                }
+                unsigned char *st = base + s * SB;
+                const int k0 = 1 + ch * KC, row = j * d.mz + k0;
+                tc::mbar_expect_tx(&full[s], tx_bytes<TR>());
+                tc::tma_load_3d(st + O_COEF, &tm_coef, i0 + XO, row, 0, &full[s]);
+                tc::tma_load_2d(st + O_MINV, &tm_minv, i0 + XO, row, &full[s]);
+                tc::tma_load_2d(st + O_CP, &tm_cp, i0 + XO, row, &full[s]);
+                tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
+                tc::tma_load_3d(st + O_XC, &tm_xc, (i0 >> 1) + XO - 3, k0 - 1, j >> 1, &full[s]);
+                tc::tma_load_2d(st + O_R, &tm_r, i0 + XO, row, &full[s]);
+            }
+        }
+        // no copy may still be in flight when the CTA ends: wait for the last stages issued
+        for (int q = it > NS ? it - NS : 0; q < it; q++)
+            if (!tc::mbar_wait(&full[q % NS], (q / NS) & 1)) atomicExch(err, 1);
+        return;
+    }
+
+    // ---- consumers: warp w owns level k0 + w of each chunk, lane = column ----
+    bool ok = true;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
+        const int i = i0 + lane;
+        const bool col = i <= d.nx;
+        float dprev = 0.0f; // warp 0: carry of the forward recurrence
+        for (int ch = 0; ch < nch; ch++, it++) {
+            const int s = it % NS;
+            const unsigned char *st = base + s * SB;
+            if (ok && !tc::mbar_wait(&full[s], (it / NS) & 1)) {
+                atomicExch(err, 1);
+                ok = false;
+            }
+            const int k0 = 1 + ch * KC;
+            // x2 = x1 + s P xc on the chunk's window, zero outside the interior
+            const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
+            for (int e = tid; e < 3 * WK * WX; e += CW) {
+                const int cc = e % WX, kw = (e / WX) % WK, jj = e / (WX * WK);
+                const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
+                float a = 0.0f;
+                if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
+                    a = sx1[(jj * WK + kw) * X1W + cc + 3];
+                    a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
+                }
+                s_x2w[e] = a;
+            }
+            tc::named_sync(1, CW);
+            const int k = k0 + warp;
+            if (k <= nz) {
+                const int t = (k - 1) * TX + lane;
+                float res = 0.0f, x2c = 0.0f, cpv = 0.0f;
+                if (col) {
+                    const float *sco = (const float *)(st + O_COEF);
+                    float cv[15];
+#pragma unroll
+                    for (int q = 0; q < 15; q++) cv[q] = sco[(q * KC + warp) * TX + lane];
+                    const float *xs = s_x2w + (WK + warp + 1) * WX + lane + 1;
+                    const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
+                    res = (float)(rv - stencil_regs<WK * WX, WX>(cv, xs));
+                    x2c = xs[0];
+                    cpv = ((const float *)(st + O_CP))[warp * TX + lane];
+                }
+                s_res[t] = res;
+                s_cp[t] = cpv;
+                s_x2c[t] = x2c;
+            }
+            tc::named_sync(1, CW);
+            if (warp == 0) { // forward recurrence over the chunk, then release the stage
+                if (col) {
+                    const float *sco = (const float *)(st + O_COEF), *smv = (const float *)(st + O_MINV);
+                    float rv[KC], cv[KC], mv[KC];
+#pragma unroll
+                    for (int u = 0; u < KC; u++) {
+                        const int kq = k0 + u;
+                        const bool v = kq <= nz;
+                        rv[u] = v ? s_res[(kq - 1) * TX + lane] : 0.0f;
+                        cv[u] = v && kq > 1 ? sco[(CC * KC + u) * TX + lane] : 0.0f;
+                        mv[u] = v ? smv[u * TX + lane] : 0.0f;
+                    }
+#pragma unroll
+                    for (int u = 0; u < KC; u++) {
+                        if (k0 + u > nz) break;
+                        dprev = (rv[u] - cv[u] * dprev) * mv[u];
+                        s_res[(k0 + u - 1) * TX + lane] = dprev;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&empty[s]);
+            }
+        }
+        if (warp == 0 && col) { // backward recurrence of the tile's columns
+            float y = 0.0f;
+            int k = nz - 1;
+            for (; k + 1 >= THOMAS_U; k -= THOMAS_U) {
+                float rv[THOMAS_U], pv[THOMAS_U];
+#pragma unroll
+                for (int u = 0; u < THOMAS_U; u++) {
+                    rv[u] = s_res[(k - u) * TX + lane];
+                    pv[u] = s_cp[(k - u) * TX + lane];
+                }
+#pragma unroll
+                for (int u = 0; u < THOMAS_U; u++) {
+                    y = rv[u] - pv[u] * y;
+                    s_res[(k - u) * TX + lane] = y;
+                }
+            }
+            for (; k >= 0; k--) {
+                y = s_res[k * TX + lane] - s_cp[k * TX + lane] * y;
+                s_res[k * TX + lane] = y;
+            }
+        }
+        tc::named_sync(1, CW);
+        for (int t = tid; t < nz * TX; t += CW) {
+            const int c = t % TX, k = t / TX + 1, ii = i0 + c;
+            if (ii <= d.nx) out[kidx(d, ii, k, j)] = (TO)((double)s_x2c[t] + (double)omega * (double)s_res[t]);
+        }
     }
 }
 
@@ -391,7 +642,13 @@ void mg_free(Mg &mg)
     }
     mg.nlev = 0;
     mg.ready = 0;
+    if (mg.err) cudaFree(mg.err);
+    mg.err = nullptr;
 }
+
+static int sm_count();
+static int smem_optin();
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
 {
@@ -422,6 +679,17 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
             ny = (ny + 1) / 2;
         }
         mg.nlev = l;
+    }
+    if (!mg.err) {
+        if (cudaMalloc((void **)&mg.err, sizeof(int)) != cudaSuccess) return -1;
+        cudaMemsetAsync(mg.err, 0, sizeof(int), s);
+    }
+    const char *tma = getenv("HICARW_MG_TMA");
+    mg.use_tma = tma && tma[0] == '1';
+    if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
+        sm_count();
+        smem_optin();
+        if (!tensor_map_encoder()) mg.use_tma = 0;
     }
     mg.lev[0].coef = fine_coef;
     for (int l = 0; l < mg.nlev; l++) {
@@ -492,14 +760,112 @@ static void post_t(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, flo
                                                             omega, cscale, gate);
 }
 
+static std::atomic<long long> g_tma_posts{0};
+long long mg_tma_posts() { return g_tma_posts.load(); }
+
+static int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    return n;
+}
+
+static int smem_optin()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
+    return n;
+}
+
+// The driver's tensor-map encoder, looked up through the runtime so that the
+// library does not link the driver library itself (nullptr if unavailable).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// Tiled tensor map of a row-major array (innermost dimension first, strides in
+// bytes of dimensions 1..rank-1), no swizzle, zero fill out of bounds.
+static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, cuuint32_t rank, const void *ptr, const cuuint64_t *dims,
+                     const cuuint64_t *strides, const cuuint32_t *box)
+{
+    if (!ptr || ((uintptr_t)ptr & 15) != 0) return false;
+    for (cuuint32_t q = 0; q + 1 < rank; q++)
+        if (strides[q] % 16 != 0) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return false;
+    const cuuint32_t es[3] = {1, 1, 1};
+    return encode(m, dt, rank, const_cast<void *>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launch post_tma_kernel on a wide level; false (nothing launched) when its
+// conditions do not hold: shared memory for nz levels, 16-byte aligned arrays
+// and row pitches.  Box x coordinates: i0 + XO = 32 bx + 8, i0 + XO - 4 and
+// (i0 >> 1) + XO - 3 = 16 bx + 4, all multiples of 4 floats (2 doubles).
+template <typename TR, typename TO>
+static bool post_tma(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, float omega, float cscale,
+                     const SolveState *gate, int *err, cudaStream_t s)
+{
+    using namespace pt;
+    const Dims &d = L.d, &dc = C.d;
+    const size_t smem = smem_bytes<TR>(d.nz);
+    if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
+    const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
+    const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15}, sco[2] = {(cuuint64_t)d.P * 4, (cuuint64_t)d.npad * 4};
+    const cuuint64_t drow[2] = {(cuuint64_t)d.P, rows}, srow[1] = {(cuuint64_t)d.P * 4},
+                     srr[1] = {(cuuint64_t)d.P * sizeof(TR)};
+    const cuuint64_t dx1[3] = {(cuuint64_t)d.P, (cuuint64_t)d.mz, (cuuint64_t)d.my},
+                     sx1[2] = {(cuuint64_t)d.P * 4, (cuuint64_t)d.plane * 4};
+    const cuuint64_t dxc[3] = {(cuuint64_t)dc.P, (cuuint64_t)dc.mz, (cuuint64_t)dc.my},
+                     sxc[2] = {(cuuint64_t)dc.P * 4, (cuuint64_t)dc.plane * 4};
+    const cuuint32_t bco[3] = {TX, KC, 15}, brow[2] = {TX, KC}, bx1[3] = {X1W, WK, 3}, bxc[3] = {XCW, WK, 2};
+    const CUtensorMapDataType f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const CUtensorMapDataType fr = sizeof(TR) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap m[6];
+    if (!make_map(&m[0], f32, 3, L.coef, dco, sco, bco) || !make_map(&m[1], f32, 2, L.minv, drow, srow, brow) ||
+        !make_map(&m[2], f32, 2, L.cp, drow, srow, brow) || !make_map(&m[3], fr, 2, r, drow, srr, brow) ||
+        !make_map(&m[4], f32, 3, L.x1, dx1, sx1, bx1) || !make_map(&m[5], f32, 3, C.x3, dxc, sxc, bxc))
+        return false;
+    const int ntx = (d.nx + TX - 1) / TX, ntiles = ntx * d.ny;
+    const int grid = std::min(ntiles, 2 * sm_count());
+    cudaFuncSetAttribute(post_tma_kernel<TR, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int *e = gate ? const_cast<int *>(&gate->err) : err;
+    post_tma_kernel<TR, TO><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega, cscale,
+                                                        ntx, ntiles, gate, e);
+    g_tma_posts++;
+    return true;
+}
+
 template <typename TR, typename TO>
 static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel &C, TO *out, float omega,
-                        float cscale, const SolveState *gate, cudaStream_t s)
+                        float cscale, const SolveState *gate, int use_tma, int *err, cudaStream_t s)
 {
     const double N = (double)L.d.nx * L.d.ny * L.d.nz;
     ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + 60.0 + 4.0 + 1.0 + 8.0) * N, s);
     if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, r, C, out, omega, cscale, gate, s);
-    else post_t<TR, TO, 32, 1>(L, r, C, out, omega, cscale, gate, s);
+    else if (!(use_tma && post_tma<TR, TO>(L, r, C, out, omega, cscale, gate, err, s)))
+        post_t<TR, TO, 32, 1>(L, r, C, out, omega, cscale, gate, s);
     count_launch(1);
 }
 
@@ -546,8 +912,8 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     for (int l = L - 2; l >= 0; l--) {
         const MgLevel &F = mg.lev[l];
         const MgLevel &C = mg.lev[l + 1];
-        if (l == 0) launch_post<V, V>(F, 0, in, C, out, w, mg.cscale, gate, s);
-        else launch_post<float, float>(F, l, F.r, C, F.x3, w, mg.cscale, gate, s);
+        if (l == 0) launch_post<V, V>(F, 0, in, C, out, w, mg.cscale, gate, mg.use_tma, mg.err, s);
+        else launch_post<float, float>(F, l, F.r, C, F.x3, w, mg.cscale, gate, mg.use_tma, mg.err, s);
     }
 }
 

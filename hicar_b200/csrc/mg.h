@@ -21,11 +21,14 @@ struct Mg {
     int ready = 0;
     float omega = 0.8f;  // damping of the z-line Jacobi smoother
     float cscale = 1.0f; // scale of the prolongated coarse-grid correction (over-correction > 1)
+    int use_tma = 0;     // post-smoothers of the wide levels fed by tensor copies (HICARW_MG_TMA=1 at build)
+    int *err = nullptr;  // device flag: a bounded copy wait of a smoother timed out (calls without a solve state)
     MgLevel lev[MG_MAX_LEVELS];
 };
 
 int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s);
 void mg_free(Mg &mg);
+long long mg_tma_posts(); // post-smoother launches enqueued through the tensor-copy kernel
 template <typename V>
 void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStream_t s);
 template <typename V>

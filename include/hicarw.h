@@ -278,6 +278,11 @@ int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int a
 
 /* Number of kernels this library has launched since load (graph nodes included). */
 long long hicarw_kernel_launches(void);
+/* Multigrid post-smoother launches enqueued through the tensor-copy (TMA) kernel
+ * since load (a launch captured into a CUDA graph counts once).  Wide levels use
+ * it when the environment sets HICARW_MG_TMA=1 as the V-cycle is built (the
+ * default is the register-fed kernel; both give bit-identical results). */
+long long hicarw_mg_tma_launches(void);
 
 /* ---- the steps either side of the solve in update_winds (wind.F90) ----
  * Device pointers only (mem_kind must be HICARW_MEM_DEVICE); caller layouts as

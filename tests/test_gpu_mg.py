@@ -120,3 +120,73 @@ def test_stall_falls_back_to_reference_solve(case):
     assert st["status"] == _capi.HICARW_FELL_BACK
     assert st["precond"] == _capi.PRECOND_JACOBI
     assert st["true_res"] <= 1.01e-6 * st["b_norm"]
+
+
+def _fresh_handle(case, monkeypatch, tma):
+    """A new handle whose V-cycle is built with the tensor-copy post-smoother
+    switched on (tma=True) or off (the register-fed kernel)."""
+    from hicar_b200 import wind, wind_iterative as wi
+    monkeypatch.setenv("HICARW_MG_TMA", "1" if tma else "0")
+    wi.finalize_iter_winds()
+    wind.reset()
+    return _calibrated(case)
+
+
+@pytest.mark.parametrize("shape", [(131, 75, 21), (128, 96, 16)])
+def test_tma_post_smoother_matches_register_path(shape, monkeypatch):
+    """The post-smoother fed by tensor copies (wide levels: here the finest)
+    against the register-fed kernel on the same V-cycle input: bit-identical,
+    on a ragged grid (nx not a multiple of the 32-column tile, odd nx and ny,
+    nz not a multiple of the 8-level chunk) and a regular one; and against the
+    numpy restatement of the V-cycle."""
+    import mg_ref
+    from hicar_b200 import wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=7, adv_den=True, n_hills=12)
+    lib = _capi.load()
+    rng = np.random.default_rng(5)
+    x = np.zeros((ny + 2, nz + 2, nx + 2))
+    x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
+    out = {}
+    for tma in (False, True):
+        dom, _, _, _ = _fresh_handle(case, monkeypatch, tma)
+        h = wi.handle(dom.nest_indx)
+        n0 = lib.hicarw_mg_tma_launches()
+        y = np.empty_like(x)
+        _capi.check(lib.hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
+        out[tma] = (y, lib.hicarw_mg_tma_launches() - n0, _coefs(dom))
+    assert out[False][1] == 0 and out[True][1] >= 1
+    np.testing.assert_array_equal(out[True][2], out[False][2])
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    ref = mg_ref.VCycle(out[True][2], 0.8)(x[1:-1, 1:-1, 1:-1])
+    assert _rel(out[True][0][1:-1, 1:-1, 1:-1], ref) < 1e-5
+    y = out[True][0]
+    assert not y[0].any() and not y[-1].any() and not y[:, 0].any() and not y[:, -1].any()
+    assert not y[:, :, 0].any() and not y[:, :, -1].any()
+
+
+def test_tma_post_smoother_solve_identical(monkeypatch):
+    """A whole multigrid-preconditioned solve (BiCGStab, CUDA graphs of
+    iterations) with and without the tensor-copy post-smoother: the same
+    iteration count and the same lambda, bit for bit."""
+    from hicar_b200 import wind, wind_iterative as wi
+    case = cases.build_case(131, 75, 21, seed=8, adv_den=True, n_hills=12)
+    lib = _capi.load()
+    res = {}
+    for tma in (False, True):
+        dom, _, div, _ = _fresh_handle(case, monkeypatch, tma)
+        h = wi.handle(dom.nest_indx)
+        wi.set_options(wi.WindOptions(tol_rel=1e-8, precond=_capi.PRECOND_MG, stall_iters=50))
+        n0 = lib.hicarw_mg_tma_launches()
+        dom.set_winds(case.u, case.v, case.w)
+        lib.hicarw_reset_solution(h, None)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+        lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+        _capi.check(lib.hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None), h)
+        res[tma] = (st, lam, lib.hicarw_mg_tma_launches() - n0)
+    assert res[False][2] == 0 and res[True][2] >= 1
+    for tma in (False, True):
+        assert res[tma][0]["status"] == 0 and res[tma][0]["precond"] == _capi.PRECOND_MG
+    assert res[True][0]["iterations"] == res[False][0]["iterations"]
+    np.testing.assert_array_equal(res[True][1], res[False][1])
