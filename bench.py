@@ -57,10 +57,13 @@ WORKLOADS = {
 # mixed1024: 1245, the count of the same method (plain BiCGStab, FP64 Krylov) on the GPU.
 REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
 # DRAM bytes per interior cell of one launch of a dominant kernel, from one ncu
-# capture on a smaller case (profiles/mg_post_l0_mid256.md: 290.45 MB for the
-# 256x256x48 = 3145728 cells of that launch); the kernel reads and writes each
-# cell's data once, so its traffic scales with the cells of the workload.
-TRAFFIC_PER_CELL = {"mg_post_l0": 290.454272e6 / (256 * 256 * 48)}
+# capture on a smaller case (256x256x48 = 3145728 cells); the kernel reads and
+# writes each cell's data once, so its traffic scales with the cells of the
+# workload.  mg_post_l0 is the tensor-copy post-smoother (291.86 MB per launch
+# of that case), or the register-fed one when the environment sets
+# HICARW_MG_TMA=0 (290.45 MB).
+TRAFFIC_PER_CELL = {"mg_post_l0": (290.454272e6 if os.environ.get("HICARW_MG_TMA", "1")[:1] == "0"
+                                   else 291.858944e6) / (256 * 256 * 48)}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
@@ -477,7 +480,8 @@ def run_ours(args, wl):
                        "iterations": it[0], "ref_method_iterations": ref_iters, "true_res_rel": max(tr),
                        "plain_gpu_solves_per_s": 1000.0 / plain_ms,
                        "speedup_vs_plain_gpu": value / world / (1000.0 / plain_ms), "accuracy": accuracy,
-                       "l2": "inputs larger than L2 (15 FP32 coefficient arrays, 0.8 GB)",
+                       "l2": "inputs larger than L2 (15 FP32 coefficient arrays, %.2f GB)"
+                             % (15 * 4 * (dom.nx + 2) * (dom.ny + 2) * (dom.nz + 2) / 1e9),
                        "parallelism": f"{world} independent subdomains" if world > 1 else "1 GPU"},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

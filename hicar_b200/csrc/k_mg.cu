@@ -685,7 +685,7 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
         cudaMemsetAsync(mg.err, 0, sizeof(int), s);
     }
     const char *tma = getenv("HICARW_MG_TMA");
-    mg.use_tma = tma && tma[0] == '1';
+    mg.use_tma = !(tma && tma[0] == '0');
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
         sm_count();
         smem_optin();

@@ -4,7 +4,7 @@
  * Drop-in replacement for HICAR's Fortran module `wind_iterative`
  * (src/physics/wind_iterative.F90).  Each entry point below names the
  * reference routine it replaces.  The Fortran side binds these functions
- * with ISO_C_BINDING; every argument is a plain pointer,
+ * with ISO_C_BINDING (bind(C) interfaces); every argument is a plain pointer,
  * an int or a float/double, every array uses the reference's Fortran layout
  * (i fastest, then k, then j), and every function returns an int status:
  *
@@ -280,8 +280,8 @@ int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int a
 long long hicarw_kernel_launches(void);
 /* Multigrid post-smoother launches enqueued through the tensor-copy (TMA) kernel
  * since load (a launch captured into a CUDA graph counts once).  Wide levels use
- * it when the environment sets HICARW_MG_TMA=1 as the V-cycle is built (the
- * default is the register-fed kernel; both give bit-identical results). */
+ * it unless the environment sets HICARW_MG_TMA=0 as the V-cycle is built (then
+ * the register-fed kernel runs; both give bit-identical results). */
 long long hicarw_mg_tma_launches(void);
 
 /* ---- the steps either side of the solve in update_winds (wind.F90) ----
