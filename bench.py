@@ -67,6 +67,7 @@ TRAFFIC_PER_CELL = {"mg_post_l0": (290.454272e6 if os.environ.get("HICARW_MG_TMA
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
+MG_SKIP_FINE_PRE = False  # --mg-skip-fine-presmooth
 FGMRES_RESTART = None  # --fgmres-restart
 
 
@@ -105,6 +106,8 @@ def solver_options(name: str):
         kw["mg_coarse_scale"] = MG_COARSE_SCALE
     if MG_OMEGA is not None and "precond" in kw:
         kw["mg_omega"] = MG_OMEGA
+    if MG_SKIP_FINE_PRE and "precond" in kw:
+        kw["mg_skip_fine_presmooth"] = True
     if FGMRES_RESTART is not None and "fgmres_restart" in kw:
         kw["fgmres_restart"] = FGMRES_RESTART
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
@@ -634,7 +637,7 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL, MG_COARSE_SCALE, MG_OMEGA, FGMRES_RESTART
+    global TOL, MG_COARSE_SCALE, MG_OMEGA, MG_SKIP_FINE_PRE, FGMRES_RESTART
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -646,6 +649,8 @@ def main():
     ap.add_argument("--tol", type=float, default=TOL, help="relative residual tolerance of the timed solves")
     ap.add_argument("--mg-coarse-scale", type=float, default=None,
                     help="override the V-cycle's coarse-correction scale of the solver preset")
+    ap.add_argument("--mg-skip-fine-presmooth", action="store_true",
+                    help="V(0,1) on the finest level of the V-cycle (no pre-smoothing there)")
     ap.add_argument("--mg-omega", type=float, default=None,
                     help="override the V-cycle's smoother damping of the solver preset")
     ap.add_argument("--fgmres-restart", type=int, default=None,
@@ -661,6 +666,7 @@ def main():
     TOL = args.tol
     MG_COARSE_SCALE = args.mg_coarse_scale
     MG_OMEGA = args.mg_omega
+    MG_SKIP_FINE_PRE = args.mg_skip_fine_presmooth
     FGMRES_RESTART = args.fgmres_restart
     wl = WORKLOADS[args.workload]
     if "batch" in wl:

@@ -171,6 +171,15 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->mg_omega = 0.8f;
     o->fgmres_restart = 30;
     o->mg_coarse_scale = 1.35f; // over-correction of the aggregation coarse grid: 35 -> 25 iterations at 512x512x48
+    o->mg_skip_fine_presmooth = 0;
+}
+
+// V-cycle parameters from the options (read when its launches are enqueued).
+static void mg_params(hicarw_handle *h)
+{
+    h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
+    h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
+    h->mg.pre0 = h->opt.mg_skip_fine_presmooth ? 0 : 1;
 }
 
 static Metrics metrics_of(const hicarw_handle *h)
@@ -367,8 +376,12 @@ extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     // V-cycle parameters are read when its launches are enqueued (the graphs were just dropped)
-    h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
-    h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
+    const int pre0_was = h->mg.pre0;
+    mg_params(h);
+    if (pre0_was && !h->mg.pre0 && h->mg.nlev > 0 && h->mg.lev[0].x1) { // the finest x1 must read as zero from now on
+        cudaDeviceSynchronize();
+        cudaMemset(h->mg.lev[0].x1, 0, (size_t)h->mg.lev[0].d.npad * sizeof(float));
+    }
     return rc;
 }
 
@@ -479,7 +492,7 @@ static int fetch_state(hicarw_handle *h, cudaStream_t s)
     CK(cudaStreamSynchronize(s));
     if (h->hst->err) {
         h->err = "a bounded device-side wait timed out (multigrid smoother copies)";
-        return HICARW_ERR_CUDA;
+        return HICARW_ERR_TIMEOUT;
     }
     return 0;
 }
@@ -495,8 +508,7 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     h->use_learned = allow_mg && h->opt.precond == HICARW_PRECOND_LEARNED && h->operator_probed &&
                      h->opt.solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
-        h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
-        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
+        mg_params(h);
         if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
         h->mg_dirty = 0;
     }
@@ -1147,8 +1159,7 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
     int rc = put_padded(h, x, bx, mem_kind, s);
     if (!rc && sweeps <= 0) {
         if (h->mg_dirty || !h->mg.ready) {
-            h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
-        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
+            mg_params(h);
             if (mg_build(h->mg, d, h->coef, s) != 0) rc = HICARW_ERR_CUDA;
             else h->mg_dirty = 0;
         }
@@ -1159,7 +1170,7 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
         int herr = 0;
         if (!rc && cudaMemcpy(&herr, h->mg.err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && herr) {
             h->err = "a bounded device-side wait timed out (multigrid smoother copies)";
-            rc = HICARW_ERR_CUDA;
+            rc = HICARW_ERR_TIMEOUT;
         }
     } else if (!rc) {
         launch_diag<double>(d, h->coef, h->dz_if, bd, h->operator_probed, s);
@@ -1623,8 +1634,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         h->use_learned = h->opt.solver == HICARW_SOLVER_FGMRES && h->opt.precond == HICARW_PRECOND_LEARNED &&
                          h->operator_probed && h->unet != nullptr;
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
-            h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
-        h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
+            mg_params(h);
             if (mg_build(h->mg, h->d, h->coef, s) != 0) {
                 fprintf(stderr, "hicarw batch: multigrid build of subdomain %d failed\n", i);
                 return HICARW_ERR_CUDA;
@@ -1657,7 +1667,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
     for (int i = 0; i < n; i++)
         if (b->hs[i]->hst->err) {
             fprintf(stderr, "hicarw batch: subdomain %d: a bounded device-side wait timed out\n", i);
-            return HICARW_ERR_CUDA;
+            return HICARW_ERR_TIMEOUT;
         }
     for (int i = 0; i < n; i++) // FGMRES state -> the solve-state mirror
         if (b->hs[i]->opt.solver == HICARW_SOLVER_FGMRES && (rc = fgmres_map_state(b->hs[i], 0, s)) != 0) return rc;

@@ -552,7 +552,9 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // the children and their ring staged in shared memory; one thread sums the four
 // children of a coarse cell), then out_c = w T_c^-1 r_c (w = 1 on the
 // single-column level: the exact coarse solve).
-template <typename TR, int TX, int TY>
+// NOX: the fine iterate is zero (no pre-smoothing on level f), so r_c = R^T r_f
+// and neither the fine coefficients nor x1 are read.
+template <typename TR, int TX, int TY, bool NOX>
 __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
     Dims f, const float *__restrict__ coef_f, const TR *__restrict__ r_f, const float *__restrict__ x1_f, Dims dc,
     const float *__restrict__ coef_c, const float *__restrict__ cp_c, const float *__restrict__ minv_c,
@@ -564,7 +566,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
     const int nz = f.nz, n = TC * nz;
     float *s_res = sm, *s_c = sm + n, *s_m = sm + 2 * n, *s_cp = sm + 3 * n, *s_x = sm + 4 * n;
     const int I0 = blockIdx.x * TX + 1, J0 = blockIdx.y * TY + 1;
-    stage_window<FX, FY>(f, x1_f, f, nullptr, 2 * I0 - 2, 2 * J0 - 2, s_x);
+    if (!NOX) stage_window<FX, FY>(f, x1_f, f, nullptr, 2 * I0 - 2, 2 * J0 - 2, s_x);
     __syncthreads();
     const long long cofs = (long long)CC * dc.npad;
     for (int t = threadIdx.x; t < n; t += MG_THREADS) {
@@ -583,6 +585,11 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
             if (j > f.ny) continue;
             const bool has1 = i0c + 1 <= f.nx;
             const long long o0 = kidx(f, i0c, k, j), o1 = o0 + 1;
+            if (NOX) {
+                acc += (double)r_f[o0];
+                if (has1) acc += (double)r_f[o1];
+                continue;
+            }
             float cv0[15], cv1[15];
             load_coefs(coef_f, f.npad, o0, cv0);
             double r0 = (double)r_f[o0], r1 = 0.0;
@@ -684,6 +691,8 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
         if (cudaMalloc((void **)&mg.err, sizeof(int)) != cudaSuccess) return -1;
         cudaMemsetAsync(mg.err, 0, sizeof(int), s);
     }
+    if (!mg.pre0 && mg.nlev > 0) // V(0,1) on the finest level: its x1 must read as zero
+        cudaMemsetAsync(mg.lev[0].x1, 0, (size_t)mg.lev[0].d.npad * sizeof(float), s);
     const char *tma = getenv("HICARW_MG_TMA");
     mg.use_tma = !(tma && tma[0] == '0');
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
@@ -869,44 +878,52 @@ static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel 
     count_launch(1);
 }
 
-template <typename TR, int TX, int TY>
+template <typename TR, int TX, int TY, bool NOX>
 static void restrict_t(const MgLevel &F, const TR *r, const MgLevel &C, float *out, float omega,
                        const SolveState *gate, cudaStream_t s)
 {
     dim3 g((C.d.nx + TX - 1) / TX, (C.d.ny + TY - 1) / TY);
-    size_t smem = ((size_t)4 * TX * TY * C.d.nz + (size_t)(2 * TX + 2) * (2 * TY + 2) * (C.d.nz + 2)) *
+    size_t smem = ((size_t)4 * TX * TY * C.d.nz + (NOX ? 0 : (size_t)(2 * TX + 2) * (2 * TY + 2) * (C.d.nz + 2))) *
                   sizeof(float);
-    set_smem(restrict_pre_kernel<TR, TX, TY>, smem);
-    restrict_pre_kernel<TR, TX, TY><<<g, MG_THREADS, smem, s>>>(F.d, F.coef, r, F.x1, C.d, C.coef, C.cp, C.minv,
-                                                                C.r, out, omega, gate);
+    set_smem(restrict_pre_kernel<TR, TX, TY, NOX>, smem);
+    restrict_pre_kernel<TR, TX, TY, NOX><<<g, MG_THREADS, smem, s>>>(F.d, F.coef, r, F.x1, C.d, C.coef, C.cp,
+                                                                     C.minv, C.r, out, omega, gate);
 }
 
+// nox: level f was not pre-smoothed (its x1 is zero): restrict r_f alone.
 template <typename TR>
 static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C, int clevel, float *out, float omega,
-                                const SolveState *gate, cudaStream_t s)
+                                const SolveState *gate, cudaStream_t s, bool nox = false)
 {
-    const double N = (double)F.d.nx * F.d.ny * F.d.nz;
-    ProfScope ps_(kLevelName[2][clevel], (60.0 + sizeof(TR) + 4.0) * N, s);
-    if (small_level(C.d, 16)) restrict_t<TR, 2, 2>(F, r, C, out, omega, gate, s);
-    else restrict_t<TR, 16, 1>(F, r, C, out, omega, gate, s);
+    const double N = (double)F.d.nx * F.d.ny * F.d.nz, Nc = (double)C.d.nx * C.d.ny * C.d.nz;
+    ProfScope ps_(kLevelName[2][clevel], nox ? sizeof(TR) * N + 20.0 * Nc : (60.0 + sizeof(TR) + 4.0) * N, s);
+    if (small_level(C.d, 16)) {
+        if (nox) restrict_t<TR, 2, 2, true>(F, r, C, out, omega, gate, s);
+        else restrict_t<TR, 2, 2, false>(F, r, C, out, omega, gate, s);
+    } else {
+        if (nox) restrict_t<TR, 16, 1, true>(F, r, C, out, omega, gate, s);
+        else restrict_t<TR, 16, 1, false>(F, r, C, out, omega, gate, s);
+    }
     count_launch(1);
 }
 
 // out = V-cycle(in); in/out are outer Krylov vectors of type V on the fine level.
 // Launches: pre(0), restrict+pre(1..L-1) (exact solve on the last), post(L-2..0).
+// Without fine pre-smoothing (mg.pre0 == 0) pre(0) is not launched, level 1
+// restricts `in` itself, and the finest post-smoother reads the zero x1.
 template <typename V>
 void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStream_t s)
 {
     const int L = mg.nlev;
     const float w = mg.omega;
-    launch_pre<V>(mg.lev[0], 0, in, mg.lev[0].x1, w, gate, s);
+    if (mg.pre0) launch_pre<V>(mg.lev[0], 0, in, mg.lev[0].x1, w, gate, s);
     for (int l = 1; l < L; l++) {
         const MgLevel &F = mg.lev[l - 1];
         MgLevel &C = const_cast<MgLevel &>(mg.lev[l]);
         const bool last = l == L - 1;
         float *o = last ? C.x3 : C.x1;
         float wl = last ? 1.0f : w;
-        if (l == 1) launch_restrict_pre<V>(F, in, C, l, o, wl, gate, s);
+        if (l == 1) launch_restrict_pre<V>(F, in, C, l, o, wl, gate, s, !mg.pre0);
         else launch_restrict_pre<float>(F, F.r, C, l, o, wl, gate, s);
     }
     for (int l = L - 2; l >= 0; l--) {

@@ -53,6 +53,7 @@ class WindOptions:
     mg_omega: float = 0.8
     fgmres_restart: int = 30
     mg_coarse_scale: float = 1.35          # V-cycle over-correction of the aggregation coarse grid
+    mg_skip_fine_presmooth: bool = False   # V-cycle: V(0,1) on the finest level (no pre-smoothing there)
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -70,6 +71,7 @@ class WindOptions:
         o.mg_omega = float(self.mg_omega)
         o.fgmres_restart = int(self.fgmres_restart)
         o.mg_coarse_scale = float(self.mg_coarse_scale)
+        o.mg_skip_fine_presmooth = int(bool(self.mg_skip_fine_presmooth))
         return o
 
 

@@ -114,6 +114,9 @@ typedef struct hicarw_options {
     int fgmres_restart;   /* FGMRES restart length m (1..32, default 30) */
     float mg_coarse_scale; /* V-cycle: scale of the prolongated coarse-grid correction; over-correction
                               of the piecewise-constant aggregation (default 1.35) */
+    int mg_skip_fine_presmooth; /* V-cycle: 0 = pre-smooth the finest level (default); 1 = restrict the
+                                   right-hand side directly there (V(0,1) on the finest level: one
+                                   smoother and one operator pass fewer per cycle) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),

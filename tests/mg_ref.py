@@ -110,9 +110,13 @@ def post(C, cp, mi, r, x2, omega):
 
 
 class VCycle:
-    def __init__(self, coefs, omega=0.8, cscale=1.35):
+    """fine_presmooth=False: V(0,1) on the finest level (its x1 is zero, level 1
+    restricts the input itself)."""
+
+    def __init__(self, coefs, omega=0.8, cscale=1.35, fine_presmooth=True):
         self.omega = omega
         self.cscale = cscale
+        self.fine_presmooth = fine_presmooth
         self.lev = [np.asarray(coefs, f32)]
         while self.lev[-1].shape[1] > 1 or self.lev[-1].shape[3] > 1:
             self.lev.append(coarsen(self.lev[-1]))
@@ -124,7 +128,7 @@ class VCycle:
         rs = [np.asarray(r0, np.float64)]
         x1 = []
         cp, mi = self.fac[0]
-        x1.append(pre(self.lev[0], cp, mi, rs[0], w))
+        x1.append(pre(self.lev[0], cp, mi, rs[0], w) if self.fine_presmooth else np.zeros(rs[0].shape, f32))
         for l in range(1, L):
             C = self.lev[l - 1]
             res = rs[l - 1] - apply(C, x1[l - 1])
