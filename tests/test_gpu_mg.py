@@ -192,12 +192,14 @@ def test_tma_post_smoother_solve_identical(monkeypatch):
     np.testing.assert_array_equal(res[True][1], res[False][1])
 
 
-@pytest.mark.parametrize("shape", [(48, 40, 20), (131, 75, 21)])
+@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13)])
 def test_vcycle_without_fine_presmoothing(shape):
     """V(0,1) on the finest level (mg_skip_fine_presmooth): level 1 restricts
     the input itself and the finest post-smoother starts from the coarse
-    correction alone; against the numpy restatement, on a grid whose finest
-    level uses the small-level tiles and on one that uses the wide ones."""
+    correction alone; against the numpy restatement, on a grid whose levels 0
+    and 1 use the small-level tiles and on a ragged one whose level 0 uses the
+    tensor-copy post-smoother and level 1 the wide restriction tiles
+    (99 x 51 coarse columns, nz not a multiple of 8)."""
     import mg_ref
     from hicar_b200 import wind_iterative as wi
     nx, ny, nz = shape
