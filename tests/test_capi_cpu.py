@@ -32,6 +32,24 @@ def test_default_options_are_reference_constants(lib):
     assert o.solver == _capi.SOLVER_REFERENCE
 
 
+def test_options_mirror_matches_the_c_struct(lib):
+    """The ctypes mirror of hicarw_options has the C struct's size and field
+    order: the library's defaults land in the expected fields and nothing is
+    written past the mirror's end."""
+    n = C.sizeof(_capi.Options)
+    buf = (C.c_ubyte * (n + 64))(*([0xA5] * (n + 64)))
+    lib.hicarw_default_options(C.cast(buf, C.POINTER(_capi.Options)))
+    assert bytes(buf[n:]) == b"\xa5" * 64
+    o = _capi.Options.from_buffer_copy(bytes(buf[:n]))
+    assert o.check_every == 8 and o.replace_every == 50 and o.precond == _capi.PRECOND_JACOBI
+    assert o.stall_iters == 0 and o.fgmres_restart == 30
+    assert abs(o.mg_omega - 0.8) < 1e-7 and abs(o.mg_coarse_scale - 1.35) < 1e-7
+    assert o.mg_skip_fine_presmooth == 0
+    from hicar_b200 import wind_iterative as wi
+    c = wi.WindOptions(mg_skip_fine_presmooth=True, mg_omega=1.0).to_c()
+    assert c.mg_skip_fine_presmooth == 1 and c.mg_omega == 1.0
+
+
 def test_bad_arguments_are_errors_not_aborts(lib):
     h = C.c_void_p()
     g = _capi.Grid(1, 1, 1, 250.0, 1)     # too small: rejected before any CUDA call
