@@ -68,6 +68,7 @@ TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
 MG_SKIP_FINE_PRE = False  # --mg-skip-fine-presmooth
+MG_W_LEVELS = ()  # --mg-w-levels
 FGMRES_RESTART = None  # --fgmres-restart
 
 
@@ -108,6 +109,8 @@ def solver_options(name: str):
         kw["mg_omega"] = MG_OMEGA
     if MG_SKIP_FINE_PRE and "precond" in kw:
         kw["mg_skip_fine_presmooth"] = True
+    if MG_W_LEVELS and "precond" in kw:
+        kw["mg_w_levels"] = tuple(MG_W_LEVELS)
     if FGMRES_RESTART is not None and "fgmres_restart" in kw:
         kw["fgmres_restart"] = FGMRES_RESTART
     return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
@@ -637,7 +640,7 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL, MG_COARSE_SCALE, MG_OMEGA, MG_SKIP_FINE_PRE, FGMRES_RESTART
+    global TOL, MG_COARSE_SCALE, MG_OMEGA, MG_SKIP_FINE_PRE, MG_W_LEVELS, FGMRES_RESTART
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -651,6 +654,8 @@ def main():
                     help="override the V-cycle's coarse-correction scale of the solver preset")
     ap.add_argument("--mg-skip-fine-presmooth", action="store_true",
                     help="V(0,1) on the finest level of the V-cycle (no pre-smoothing there)")
+    ap.add_argument("--mg-w-levels", default="",
+                    help="comma-separated V-cycle levels (>= 1) that correct twice from the coarse grid")
     ap.add_argument("--mg-omega", type=float, default=None,
                     help="override the V-cycle's smoother damping of the solver preset")
     ap.add_argument("--fgmres-restart", type=int, default=None,
@@ -667,6 +672,7 @@ def main():
     MG_COARSE_SCALE = args.mg_coarse_scale
     MG_OMEGA = args.mg_omega
     MG_SKIP_FINE_PRE = args.mg_skip_fine_presmooth
+    MG_W_LEVELS = tuple(int(x) for x in args.mg_w_levels.split(",") if x.strip())
     FGMRES_RESTART = args.fgmres_restart
     wl = WORKLOADS[args.workload]
     if "batch" in wl:

@@ -172,6 +172,7 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->fgmres_restart = 30;
     o->mg_coarse_scale = 1.35f; // over-correction of the aggregation coarse grid: 35 -> 25 iterations at 512x512x48
     o->mg_skip_fine_presmooth = 0;
+    o->mg_w_levels = 0;
 }
 
 // V-cycle parameters from the options (read when its launches are enqueued).
@@ -180,6 +181,7 @@ static void mg_params(hicarw_handle *h)
     h->mg.omega = h->opt.mg_omega > 0.0f ? h->opt.mg_omega : 0.8f;
     h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
     h->mg.pre0 = h->opt.mg_skip_fine_presmooth ? 0 : 1;
+    h->mg.wmask = h->opt.mg_w_levels & ~1;
 }
 
 static Metrics metrics_of(const hicarw_handle *h)

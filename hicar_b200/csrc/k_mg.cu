@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -907,8 +908,38 @@ static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C,
     count_launch(1);
 }
 
+// Coarse part of the cycle below level l >= 1, whose right-hand side r and
+// first iterate x1 (pre-smoothed from zero by the restriction kernel) are in
+// place; returns the buffer that holds level l's result.  A level whose bit
+// is set in mg.wmask corrects twice from the coarse grid (a W-cycle there):
+// the second restriction subtracts A times the first post-smoothed iterate,
+// and the two post-smoothings alternate between the level's x1 and x3 buffers.
+// With no bit set the launches are those of the V-cycle: all restrictions
+// top-down, then all post-smoothings bottom-up, results in x3.
+static const float *coarse_cycle(const Mg &mg, int l, const SolveState *gate, cudaStream_t s)
+{
+    const int L = mg.nlev;
+    const MgLevel &F = mg.lev[l];
+    if (l == L - 1) return F.x3; // exact column solve, written by the restriction from level l - 1
+    const MgLevel &C = mg.lev[l + 1];
+    const bool last = l + 1 == L - 1;
+    const int reps = (mg.wmask >> l) & 1 ? 2 : 1;
+    float *cur = F.x1, *other = F.x3;
+    for (int rep = 0; rep < reps; rep++) {
+        MgLevel Fi = F;
+        Fi.x1 = cur; // the iterate whose residual is restricted and which the post-smoother corrects
+        launch_restrict_pre<float>(Fi, F.r, C, l + 1, last ? C.x3 : C.x1, last ? 1.0f : mg.omega, gate, s);
+        MgLevel Cr = C;
+        Cr.x3 = const_cast<float *>(coarse_cycle(mg, l + 1, gate, s));
+        launch_post<float, float>(Fi, l, F.r, Cr, other, mg.omega, mg.cscale, gate, mg.use_tma, mg.err, s);
+        std::swap(cur, other);
+    }
+    return cur;
+}
+
 // out = V-cycle(in); in/out are outer Krylov vectors of type V on the fine level.
-// Launches: pre(0), restrict+pre(1..L-1) (exact solve on the last), post(L-2..0).
+// Launches: pre(0), restrict+pre(1..L-1) (exact solve on the last), post(L-2..0),
+// with the repeated coarse corrections of the levels in mg.wmask (coarse_cycle).
 // Without fine pre-smoothing (mg.pre0 == 0) pre(0) is not launched, level 1
 // restricts `in` itself, and the finest post-smoother reads the zero x1.
 template <typename V>
@@ -917,21 +948,14 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     const int L = mg.nlev;
     const float w = mg.omega;
     if (mg.pre0) launch_pre<V>(mg.lev[0], 0, in, mg.lev[0].x1, w, gate, s);
-    for (int l = 1; l < L; l++) {
-        const MgLevel &F = mg.lev[l - 1];
-        MgLevel &C = const_cast<MgLevel &>(mg.lev[l]);
-        const bool last = l == L - 1;
-        float *o = last ? C.x3 : C.x1;
-        float wl = last ? 1.0f : w;
-        if (l == 1) launch_restrict_pre<V>(F, in, C, l, o, wl, gate, s, !mg.pre0);
-        else launch_restrict_pre<float>(F, F.r, C, l, o, wl, gate, s);
-    }
-    for (int l = L - 2; l >= 0; l--) {
-        const MgLevel &F = mg.lev[l];
-        const MgLevel &C = mg.lev[l + 1];
-        if (l == 0) launch_post<V, V>(F, 0, in, C, out, w, mg.cscale, gate, mg.use_tma, mg.err, s);
-        else launch_post<float, float>(F, l, F.r, C, F.x3, w, mg.cscale, gate, mg.use_tma, mg.err, s);
-    }
+    if (L < 2) return;
+    const MgLevel &F = mg.lev[0];
+    const MgLevel &C = mg.lev[1];
+    const bool last = L == 2;
+    launch_restrict_pre<V>(F, in, C, 1, last ? C.x3 : C.x1, last ? 1.0f : w, gate, s, !mg.pre0);
+    MgLevel Cr = C;
+    Cr.x3 = const_cast<float *>(coarse_cycle(mg, 1, gate, s));
+    launch_post<V, V>(F, 0, in, Cr, out, w, mg.cscale, gate, mg.use_tma, mg.err, s);
 }
 
 template void mg_apply<double>(const Mg &, const double *, double *, const SolveState *, cudaStream_t);

@@ -22,6 +22,7 @@ struct Mg {
     float omega = 0.8f;  // damping of the z-line Jacobi smoother
     float cscale = 1.0f; // scale of the prolongated coarse-grid correction (over-correction > 1)
     int pre0 = 1;        // pre-smooth the finest level (0: V(0,1) there, its x1 kept at zero)
+    int wmask = 0;       // bit l (l >= 1): level l corrects twice from the coarse grid (W-cycle there)
     int use_tma = 1;     // post-smoothers of the wide levels fed by tensor copies (HICARW_MG_TMA=0: register-fed)
     int *err = nullptr;  // device flag: a bounded copy wait of a smoother timed out (calls without a solve state)
     MgLevel lev[MG_MAX_LEVELS];

@@ -54,6 +54,7 @@ class WindOptions:
     fgmres_restart: int = 30
     mg_coarse_scale: float = 1.35          # V-cycle over-correction of the aggregation coarse grid
     mg_skip_fine_presmooth: bool = False   # V-cycle: V(0,1) on the finest level (no pre-smoothing there)
+    mg_w_levels: tuple = ()                # levels (>= 1) that correct twice from the coarse grid (W-cycle)
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -72,6 +73,7 @@ class WindOptions:
         o.fgmres_restart = int(self.fgmres_restart)
         o.mg_coarse_scale = float(self.mg_coarse_scale)
         o.mg_skip_fine_presmooth = int(bool(self.mg_skip_fine_presmooth))
+        o.mg_w_levels = sum(1 << int(l) for l in self.mg_w_levels if 1 <= int(l) < 31)
         return o
 
 

@@ -117,6 +117,8 @@ typedef struct hicarw_options {
     int mg_skip_fine_presmooth; /* V-cycle: 0 = pre-smooth the finest level (default); 1 = restrict the
                                    right-hand side directly there (V(0,1) on the finest level: one
                                    smoother and one operator pass fewer per cycle) */
+    int mg_w_levels;      /* V-cycle: bit l (l >= 1) makes level l correct twice from its coarse grid
+                             (a W-cycle on those levels; bit 0 is ignored); 0 = V-cycle (default) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),

@@ -111,43 +111,55 @@ def post(C, cp, mi, r, x2, omega):
 
 class VCycle:
     """fine_presmooth=False: V(0,1) on the finest level (its x1 is zero, level 1
-    restricts the input itself)."""
+    restricts the input itself).  wlevels: levels (>= 1) that correct twice from
+    their coarse grid per visit (W-cycle there): the second restriction takes the
+    residual of the first post-smoothed iterate, stored in FP32 as on the GPU."""
 
-    def __init__(self, coefs, omega=0.8, cscale=1.35, fine_presmooth=True):
+    def __init__(self, coefs, omega=0.8, cscale=1.35, fine_presmooth=True, wlevels=()):
         self.omega = omega
         self.cscale = cscale
         self.fine_presmooth = fine_presmooth
+        self.wlevels = {int(l) for l in wlevels if int(l) >= 1}
         self.lev = [np.asarray(coefs, f32)]
         while self.lev[-1].shape[1] > 1 or self.lev[-1].shape[3] > 1:
             self.lev.append(coarsen(self.lev[-1]))
         self.fac = [factors(C) for C in self.lev]
 
-    def __call__(self, r0):
+    @staticmethod
+    def _restrict(res):
+        ny, nz, nx = res.shape
+        rc = np.zeros(((ny + 1) // 2, nz, (nx + 1) // 2))
+        for pj in (0, 1):
+            for pi in (0, 1):
+                sub = res[pj::2, :, pi::2]
+                rc[:sub.shape[0], :, :sub.shape[2]] += sub
+        return rc.astype(f32)
+
+    def _level(self, l, r, x):
+        """Coarse corrections and post-smoothing of level l < L-1 from iterate x
+        (FP32); returns level l's result (FP64 on level 0, FP32 below)."""
         L = len(self.lev)
         w = float(self.omega)
-        rs = [np.asarray(r0, np.float64)]
-        x1 = []
+        C = self.lev[l]
+        cp, mi = self.fac[l]
+        for _ in range(2 if l in self.wlevels else 1):
+            rc = self._restrict(np.asarray(r, np.float64) - apply(C, x))
+            cpc, mic = self.fac[l + 1]
+            if l + 1 == L - 1:
+                xc = pre(self.lev[l + 1], cpc, mic, rc, 1.0)        # exact column solve
+            else:
+                xc = self._level(l + 1, rc, pre(self.lev[l + 1], cpc, mic, rc, w))
+            up = np.repeat(np.repeat(xc, 2, axis=0), 2, axis=2)
+            ny, nz, nx = x.shape
+            x2 = (x + f32(self.cscale) * up[:ny, :, :nx].astype(f32)).astype(f32)
+            out = post(C, cp, mi, r, x2, w)
+            x = out if l == 0 else out.astype(f32)
+        return x
+
+    def __call__(self, r0):
+        r0 = np.asarray(r0, np.float64)
         cp, mi = self.fac[0]
-        x1.append(pre(self.lev[0], cp, mi, rs[0], w) if self.fine_presmooth else np.zeros(rs[0].shape, f32))
-        for l in range(1, L):
-            C = self.lev[l - 1]
-            res = rs[l - 1] - apply(C, x1[l - 1])
-            ny, nz, nx = res.shape
-            rc = np.zeros(((ny + 1) // 2, nz, (nx + 1) // 2))
-            for pj in (0, 1):
-                for pi in (0, 1):
-                    sub = res[pj::2, :, pi::2]
-                    rc[:sub.shape[0], :, :sub.shape[2]] += sub
-            rs.append(rc.astype(f32))
-            cp, mi = self.fac[l]
-            x1.append(pre(self.lev[l], cp, mi, rs[l], 1.0 if l == L - 1 else w))
-        x3 = x1[L - 1]
-        for l in range(L - 2, -1, -1):
-            C = self.lev[l]
-            cp, mi = self.fac[l]
-            up = np.repeat(np.repeat(x3, 2, axis=0), 2, axis=2)
-            ny, nz, nx = x1[l].shape
-            x2 = (x1[l] + f32(self.cscale) * up[:ny, :, :nx].astype(f32)).astype(f32)
-            out = post(C, cp, mi, rs[l], x2, w)
-            x3 = out if l == 0 else out.astype(f32)
-        return x3
+        x1 = pre(self.lev[0], cp, mi, r0, float(self.omega)) if self.fine_presmooth else np.zeros(r0.shape, f32)
+        if len(self.lev) == 1:
+            return x1
+        return self._level(0, r0, x1)

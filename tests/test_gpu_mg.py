@@ -243,3 +243,55 @@ def test_mg_solve_without_fine_presmoothing(oracle_mod, case):
     s.set_tolerance(1e-9)
     assert s.bicgstab(3000)["status"] == 0
     assert _rel(lam, s.vec("x")) < 1e-5
+
+
+@pytest.mark.parametrize("shape,wlev", [((48, 40, 20), (1, 2)), ((197, 101, 13), (2, 3))])
+def test_vcycle_w_levels(shape, wlev):
+    """W-cycle on chosen coarse levels (mg_w_levels; with V(0,1) on the finest
+    level and omega = 1) against the numpy restatement, then back to the plain
+    V-cycle on the same handle."""
+    import mg_ref
+    from hicar_b200 import wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=13, adv_den=True, n_hills=10)
+    dom, _, _, _ = _calibrated(case)
+    h = wi.handle(dom.nest_indx)
+    lib = _capi.load()
+    rng = np.random.default_rng(17)
+    x = np.zeros((ny + 2, nz + 2, nx + 2))
+    x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
+    coefs = _coefs(dom)
+    for opt, ref in ((dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=wlev),
+                      dict(omega=1.0, fine_presmooth=False, wlevels=wlev)),
+                     (dict(), dict(omega=0.8))):
+        wi.set_options(wi.WindOptions(**opt))
+        y = np.empty_like(x)
+        _capi.check(lib.hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
+        want = mg_ref.VCycle(coefs, **ref)(x[1:-1, 1:-1, 1:-1])
+        assert _rel(y[1:-1, 1:-1, 1:-1], want) < 1e-5, opt
+        assert not y[0].any() and not y[:, 0].any() and not y[:, :, 0].any()
+
+
+def test_mg_solve_w_levels(oracle_mod, case):
+    """The multigrid-preconditioned solve with a W-cycle on levels 1-2 (V(0,1)
+    on the finest level, omega = 1) converges to the oracle's lambda."""
+    from hicar_b200 import wind, wind_iterative as wi
+    dom, opt, div, _ = _calibrated(case)
+    h = wi.handle(dom.nest_indx)
+    wi.set_options(wi.WindOptions(tol_rel=1e-9, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                                  stall_iters=50, mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(1, 2)))
+    dom.set_winds(case.u, case.v, case.w)
+    _capi.load().hicarw_reset_solution(h, None)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+    assert st["status"] == 0 and st["precond"] == _capi.PRECOND_MG
+    assert st["true_res"] <= 1.01 * st["target"]
+    lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+    _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
+    s = oracle_mod.OracleSolver(case.domain)
+    s.set_coefs(_coefs(dom), probed=True)
+    s.prepare(div.cpu().numpy())
+    s.set_vec("x", np.zeros_like(lam))
+    s.set_tolerance(1e-9)
+    assert s.bicgstab(3000)["status"] == 0
+    assert _rel(lam, s.vec("x")) < 1e-5
