@@ -13,6 +13,10 @@
 // host synchronisation.  Kernels read the `stop`/`halt` flags and return at once
 // when the solve has ended, which lets the host replay a fixed CUDA graph of
 // several iterations and read the flag only once per graph.
+#include <stdlib.h>
+
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "krylov_dev.cuh"
@@ -39,10 +43,45 @@ __global__ void __launch_bounds__(ROWT) spmv_kernel(OpCtx c, const V *__restrict
 }
 
 template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_march_kernel(OpCtx c, const V *__restrict__ x, V *__restrict__ y,
+                                                          const SolveState *gate)
+{
+    if (gated(gate)) return;
+    march_rows<V>(c, x, [&](long long o, double v) { y[o] = (V)v; });
+}
+
+// Column-marching operator kernels for the probed operator when the
+// environment sets HICARW_SPMV_MARCH=1 (read at every launch, so at graph
+// capture for the captured ones).
+static bool use_march(const OpCtx &c)
+{
+    const char *e = getenv("HICARW_SPMV_MARCH");
+    return c.probed && e && e[0] == '1';
+}
+
+// One wave of resident CTAs (the kernel's occupancy, cached), at most `cap`.
+template <typename K>
+static int march_grid(K *kernel, const Dims &d, int cap)
+{
+    static int resident = 0;
+    if (!resident) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, ROWT, 0);
+        resident = std::max(1, sms * std::max(1, per_sm));
+    }
+    const long long n = (march_strips(d) + MARCH_WARPS - 1) / MARCH_WARPS;
+    return (int)std::min<long long>(n, std::min(cap, resident));
+}
+
+template <typename V>
 void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaStream_t st)
 {
     ProfScope ps_("spmv", coef_bytes(c.d) + rows(c.d) * 2.0 * sizeof(V), st);
-    spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
+    if (use_march(c))
+        spmv_march_kernel<V><<<march_grid(spmv_march_kernel<V>, c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
+    else spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     count_launch(1);
 }
 
@@ -97,6 +136,45 @@ void launch_setup(const OpCtx &c, const X *x, const V *rhs, V *r, V *rhat, V *p,
     count_launch(1);
 }
 
+// alpha = rho / sigma (:657-688), on the last CTA of the sigma reduction.
+__device__ __forceinline__ void sigma_step(SolveState *stt, double sigma)
+{
+    stt->sigma = sigma;
+    stt->it += 1;
+    if (fabs(sigma) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; }
+    else stt->alpha = stt->rho / sigma;
+}
+
+// omega, rho, beta, the recurrence norm and the stop / breakdown / stall tests
+// (:703-783), on the last CTA of the five-dot reduction.
+__device__ __forceinline__ void dot5_step(SolveState *stt, double *hist, const double (&tot)[5])
+{
+    double ts = tot[0], tt = tot[1], rs = tot[2], rt = tot[3], ss = tot[4];
+    stt->upd_r = 0;
+    stt->upd_p = 0;
+    if (tt < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; return; } // :737
+    double omega = ts / tt;
+    double rho_new = rs - omega * rt;
+    double rn2 = ss - 2.0 * omega * ts + omega * omega * tt; // :748
+    if (rn2 < 0.0) rn2 = 0.0;
+    double rn = sqrt(rn2);
+    stt->omega = omega;
+    stt->rnorm = rn;
+    hist[stt->it] = rn;
+    if (rn <= stt->target) { stt->status = 0; stt->stop = 1; return; }         // :758 (after x update)
+    if (stt->stall_k > 0) { // stall detector: no 1% decrease within stall_k iterations
+        if (rn < 0.99 * stt->best_rn) { stt->best_rn = rn; stt->best_it = stt->it; }
+        else if (stt->it - stt->best_it >= stt->stall_k) { stt->status = 4; stt->stop = 1; return; }
+    }
+    if (fabs(omega) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :763
+    stt->upd_r = 1;
+    if (fabs(stt->rho) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :774
+    stt->beta = (rho_new / stt->rho) * (stt->alpha / omega);
+    stt->upd_p = 1;
+    stt->rho = rho_new;
+    if (stt->it >= stt->max_iters) { stt->status = 1; stt->stop = 1; } // loop ends after this iteration
+}
+
 // ---- v = A p^ and sigma = <r^, v> (:657-688) ----
 template <typename V>
 __global__ void __launch_bounds__(ROWT) spmv_sigma_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
@@ -115,13 +193,25 @@ __global__ void __launch_bounds__(ROWT) spmv_sigma_kernel(OpCtx c, const V *__re
     }
     double tot[1];
     if (!grid_reduce<1>(acc, partials, &stt->ticket[1], tot)) return;
-    if (threadIdx.x == 0) {
-        double sigma = tot[0];
-        stt->sigma = sigma;
-        stt->it += 1;
-        if (fabs(sigma) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; }
-        else stt->alpha = stt->rho / sigma;
-    }
+    if (threadIdx.x == 0) sigma_step(stt, tot[0]);
+}
+
+// The same with column-marching rows (probed operator).
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_sigma_march_kernel(OpCtx c, const V *__restrict__ phat,
+                                                                V *__restrict__ v, const V *__restrict__ rhat,
+                                                                SolveState *stt, double *partials)
+{
+    if (gated(stt)) return;
+    double acc[1] = {0.0};
+    march_rows<V>(c, phat, [&](long long o, double y) {
+        const V vv = (V)y;
+        v[o] = vv;
+        acc[0] += (double)rhat[o] * (double)vv;
+    });
+    double tot[1];
+    if (!grid_reduce<1>(acc, partials, &stt->ticket[1], tot)) return;
+    if (threadIdx.x == 0) sigma_step(stt, tot[0]);
 }
 
 template <typename V>
@@ -129,7 +219,10 @@ void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, Solve
                        cudaStream_t st)
 {
     ProfScope ps_("spmv_sigma", coef_bytes(c.d) + rows(c.d) * 3.0 * sizeof(V), st);
-    spmv_sigma_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, phat, v, rhat, stt, rb.partials);
+    if (use_march(c))
+        spmv_sigma_march_kernel<V><<<march_grid(spmv_sigma_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+            c, phat, v, rhat, stt, rb.partials);
+    else spmv_sigma_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, phat, v, rhat, stt, rb.partials);
     count_launch(1);
 }
 
@@ -157,32 +250,31 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_kernel(OpCtx c, const V *__res
     }
     double tot[5];
     if (!grid_reduce<5>(acc, partials, &stt->ticket[2], tot)) return;
-    if (threadIdx.x == 0) {
-        double ts = tot[0], tt = tot[1], rs = tot[2], rt = tot[3], ss = tot[4];
-        stt->upd_r = 0;
-        stt->upd_p = 0;
-        if (tt < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; stt->halt = 1; return; } // :737
-        double omega = ts / tt;
-        double rho_new = rs - omega * rt;
-        double rn2 = ss - 2.0 * omega * ts + omega * omega * tt; // :748
-        if (rn2 < 0.0) rn2 = 0.0;
-        double rn = sqrt(rn2);
-        stt->omega = omega;
-        stt->rnorm = rn;
-        hist[stt->it] = rn;
-        if (rn <= stt->target) { stt->status = 0; stt->stop = 1; return; }         // :758 (after x update)
-        if (stt->stall_k > 0) { // stall detector: no 1% decrease within stall_k iterations
-            if (rn < 0.99 * stt->best_rn) { stt->best_rn = rn; stt->best_it = stt->it; }
-            else if (stt->it - stt->best_it >= stt->stall_k) { stt->status = 4; stt->stop = 1; return; }
-        }
-        if (fabs(omega) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :763
-        stt->upd_r = 1;
-        if (fabs(stt->rho) < BREAKDOWN_EPS) { stt->status = 2; stt->stop = 1; return; } // :774
-        stt->beta = (rho_new / stt->rho) * (stt->alpha / omega);
-        stt->upd_p = 1;
-        stt->rho = rho_new;
-        if (stt->it >= stt->max_iters) { stt->status = 1; stt->stop = 1; } // loop ends after this iteration
-    }
+    if (threadIdx.x == 0) dot5_step(stt, hist, tot);
+}
+
+// The same with column-marching rows (probed operator).
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_dot5_march_kernel(OpCtx c, const V *__restrict__ shat,
+                                                               V *__restrict__ t, const V *__restrict__ sv,
+                                                               const V *__restrict__ rhat, SolveState *stt,
+                                                               double *hist, double *partials)
+{
+    if (gated(stt)) return;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    march_rows<V>(c, shat, [&](long long o, double y) {
+        const V tv = (V)y;
+        t[o] = tv;
+        const double td = (double)tv, sd = (double)sv[o], rd = (double)rhat[o];
+        acc[0] += td * sd;
+        acc[1] += td * td;
+        acc[2] += rd * sd;
+        acc[3] += rd * td;
+        acc[4] += sd * sd;
+    });
+    double tot[5];
+    if (!grid_reduce<5>(acc, partials, &stt->ticket[2], tot)) return;
+    if (threadIdx.x == 0) dot5_step(stt, hist, tot);
 }
 
 template <typename V>
@@ -190,7 +282,10 @@ void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *
                       const RedBuf &rb, cudaStream_t st)
 {
     ProfScope ps_("spmv_dot5", coef_bytes(c.d) + rows(c.d) * 4.0 * sizeof(V), st);
-    spmv_dot5_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, shat, t, s, rhat, stt, hist, rb.partials);
+    if (use_march(c))
+        spmv_dot5_march_kernel<V><<<march_grid(spmv_dot5_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+            c, shat, t, s, rhat, stt, hist, rb.partials);
+    else spmv_dot5_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, shat, t, s, rhat, stt, hist, rb.partials);
     count_launch(1);
 }
 

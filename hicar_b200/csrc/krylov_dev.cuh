@@ -161,5 +161,104 @@ __host__ __device__ __forceinline__ long long nsegs(const Dims &d)
     return (long long)((d.mx + ROWT - 1) / ROWT) * d.mz * d.my;
 }
 
+// ---- column-marching rows of y = A x for the probed operator ----
+// A warp owns a strip of 32 consecutive columns i of one j row and marches k
+// from the bottom ghost plane to the top one.  x at k-1, k, k+1 of its own
+// column and of the columns j-1 and j+1 stay in registers (one new load of
+// each per level); the i-1 / i+1 neighbours come from the adjacent lanes by
+// shuffles, lanes 0 and 31 keeping their own window of the column beyond the
+// strip.  Each interior row sums the 15 terms in spmv_row's order (the same
+// FP64 value); lateral columns and ghost planes are identity rows.  f(o, y) is
+// called for every row of the system, in k order within a column.
+constexpr int MARCH_WARPS = 4; // warps per CTA of the marching kernels (blockDim ROWT)
+
+__host__ __device__ __forceinline__ long long march_strips(const Dims &d) { return (long long)((d.mx + 31) / 32) * d.my; }
+
+template <typename V, typename F>
+__device__ __forceinline__ void march_rows(const OpCtx &c, const V *__restrict__ x, F &&f)
+{
+    const Dims &d = c.d;
+    const int nbx = (d.mx + 31) / 32;
+    const long long nstrips = (long long)nbx * d.my;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const long long P = d.P, PL = d.plane, N = d.npad;
+    for (long long w = (long long)blockIdx.x * wpb + wib; w < nstrips; w += (long long)gridDim.x * wpb) {
+        const int bx = (int)(w % nbx), j = (int)(w / nbx);
+        const int i = bx * 32 + lane;
+        const bool live = i < d.mx;
+        const long long ob = ((long long)j * d.mz) * P + i + XO; // row k = 0 of the column
+        if (j == 0 || j == d.my - 1) { // lateral j rows: identity (warp-uniform)
+            if (live)
+                for (int k = 0; k < d.mz; k++) f(ob + k * P, (double)x[ob + k * P]);
+            continue;
+        }
+        const bool ident = i == 0 || i == d.mx - 1; // lateral i columns: identity
+        const bool west = lane == 0 && live && !ident, east = lane == 31 && live && !ident;
+        // windows (k-1, k, k+1) of the own, j-1, j+1, i-1 (lane 0) and i+1 (lane 31) columns
+        double c_m = 0.0, c_0 = 0.0, s_m = 0.0, s_0 = 0.0, n_m = 0.0, n_0 = 0.0, w_m = 0.0, w_0 = 0.0, e_m = 0.0,
+               e_0 = 0.0;
+        if (live) {
+            c_m = (double)x[ob];
+            c_0 = (double)x[ob + P];
+            s_m = (double)x[ob - PL];
+            s_0 = (double)x[ob - PL + P];
+            n_m = (double)x[ob + PL];
+            n_0 = (double)x[ob + PL + P];
+            f(ob, c_m); // bottom ghost plane
+        }
+        if (west) { w_m = (double)x[ob - 1]; w_0 = (double)x[ob - 1 + P]; }
+        if (east) { e_m = (double)x[ob + 1]; e_0 = (double)x[ob + 1 + P]; }
+        for (int k = 1; k <= d.nz; k++) {
+            const long long o = ob + k * P;
+            double c_p = 0.0, s_p = 0.0, n_p = 0.0;
+            if (live) {
+                c_p = (double)x[o + P];
+                s_p = (double)x[o - PL + P];
+                n_p = (double)x[o + PL + P];
+            }
+            double w_p = 0.0, e_p = 0.0;
+            if (west) w_p = (double)x[o - 1 + P];
+            if (east) e_p = (double)x[o + 1 + P];
+            // i-1 and i+1 columns from the neighbouring lanes
+            const double lm = __shfl_up_sync(0xffffffffu, c_m, 1), l0 = __shfl_up_sync(0xffffffffu, c_0, 1),
+                         lp = __shfl_up_sync(0xffffffffu, c_p, 1);
+            const double rm = __shfl_down_sync(0xffffffffu, c_m, 1), r0 = __shfl_down_sync(0xffffffffu, c_0, 1),
+                         rp = __shfl_down_sync(0xffffffffu, c_p, 1);
+            const double xwm = lane == 0 ? w_m : lm, xw0 = lane == 0 ? w_0 : l0, xwp = lane == 0 ? w_p : lp;
+            const double xem = lane == 31 ? e_m : rm, xe0 = lane == 31 ? e_0 : r0, xep = lane == 31 ? e_p : rp;
+            if (live) {
+                double y;
+                if (ident) {
+                    y = c_0;
+                } else { // probed 15-point interior (:883-907), reference term order
+                    const float *cf = c.coef + o;
+                    y = (double)cf[CO * N] * s_m;
+                    y += (double)cf[CG * N] * s_0;
+                    y += (double)cf[CM * N] * s_p;
+                    y += (double)cf[CK * N] * xwm;
+                    y += (double)cf[CC * N] * c_m;
+                    y += (double)cf[CJ * N] * xem;
+                    y += (double)cf[CE * N] * xw0;
+                    y += (double)cf[CA * N] * c_0;
+                    y += (double)cf[CD * N] * xe0;
+                    y += (double)cf[CI * N] * xwp;
+                    y += (double)cf[CB * N] * c_p;
+                    y += (double)cf[CH * N] * xep;
+                    y += (double)cf[CN * N] * n_m;
+                    y += (double)cf[CF * N] * n_0;
+                    y += (double)cf[CL * N] * n_p;
+                }
+                f(o, y);
+            }
+            c_m = c_0; c_0 = c_p;
+            s_m = s_0; s_0 = s_p;
+            n_m = n_0; n_0 = n_p;
+            w_m = w_0; w_0 = w_p;
+            e_m = e_0; e_0 = e_p;
+        }
+        if (live) f(ob + (long long)(d.mz - 1) * P, c_0); // top ghost plane (c_0 = x at k = nz + 1)
+    }
+}
+
 
 }  // namespace hw

@@ -3,6 +3,7 @@ their numpy restatement (tests/mg_ref.py), the preconditioned solve against
 the oracle's solution, and the stall detector's fallback to the reference
 Jacobi-preconditioned solve."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -295,3 +296,56 @@ def test_mg_solve_w_levels(oracle_mod, case):
     s.set_tolerance(1e-9)
     assert s.bicgstab(3000)["status"] == 0
     assert _rel(lam, s.vec("x")) < 1e-5
+
+
+_MARCH = pytest.mark.skipif(os.environ.get("HICARW_TEST_SPMV_MARCH") != "1",
+                            reason="opt-in column-marching operator kernels: run with HICARW_TEST_SPMV_MARCH=1")
+
+
+@_MARCH
+@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13)])
+def test_column_marching_operator_matches_row_kernels(shape, monkeypatch):
+    """The column-marching operator apply (HICARW_SPMV_MARCH=1) gives the row
+    kernels' FP64 values bit for bit, identity rows included, on a grid
+    narrower than one strip of 32 columns in places and on a ragged one."""
+    from hicar_b200 import wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=19, adv_den=True, n_hills=10)
+    dom, _, _, _ = _calibrated(case)
+    h = wi.handle(dom.nest_indx)
+    lib = _capi.load()
+    x = np.random.default_rng(23).standard_normal((ny + 2, nz + 2, nx + 2))
+    out = {}
+    for march in ("0", "1"):
+        monkeypatch.setenv("HICARW_SPMV_MARCH", march)
+        y = np.empty_like(x)
+        _capi.check(lib.hicarw_apply_operator(h, x.ctypes.data, y.ctypes.data, _capi.MEM_HOST, None), h)
+        out[march] = y
+    np.testing.assert_array_equal(out["1"], out["0"])
+
+
+@_MARCH
+def test_column_marching_solve(case, monkeypatch):
+    """The multigrid-preconditioned solve with the column-marching sigma and
+    five-dot kernels: the same lambda as with the row kernels (the reductions
+    sum in another order, so to the solve tolerance), iterations within one."""
+    from hicar_b200 import wind, wind_iterative as wi
+    res = {}
+    for march in ("0", "1"):
+        monkeypatch.setenv("HICARW_SPMV_MARCH", march)
+        wi.finalize_iter_winds()
+        wind.reset()
+        dom, _, div, _ = _calibrated(case)
+        h = wi.handle(dom.nest_indx)
+        wi.set_options(wi.WindOptions(tol_rel=1e-9, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                                      stall_iters=50))
+        dom.set_winds(case.u, case.v, case.w)
+        _capi.load().hicarw_reset_solution(h, None)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+        lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+        _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
+        res[march] = (st, lam)
+    assert res["1"][0]["status"] == 0
+    assert abs(res["1"][0]["iterations"] - res["0"][0]["iterations"]) <= 1
+    assert _rel(res["1"][1], res["0"][1]) < 1e-6
