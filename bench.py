@@ -81,8 +81,48 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def solver_options(name: str):
-    from hicar_b200 import _capi, wind_iterative as wi
+# Cycle shapes among which the mg preset picks on the problem at hand (in the
+# untimed warm-up): the V-cycle with pre- and post-smoothing on every level
+# (omega 0.8), V(0,1) on the finest level with omega 1, and the same with two
+# coarse-grid corrections (a W-cycle) on levels 2-3 or 2-4.
+MG_CYCLES = {
+    "V(1,1)": dict(),
+    "V(0,1)": dict(mg_skip_fine_presmooth=True, mg_omega=1.0),
+    "V(0,1)+W2-3": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
+    "V(0,1)+W2-4": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)),
+}
+MG_CYCLE = "auto"  # --mg-cycle
+
+
+def pick_cycle(wi, step, base: dict):
+    """Two solves of the workload with each cycle of MG_CYCLES (the second one
+    timed with CUDA events, so that graph capture is not counted); returns the
+    options of the fastest that converged without falling back, its name and
+    the table of times (ms; None for a candidate that did not converge)."""
+    import torch
+    table = {}
+    for name, kw in MG_CYCLES.items():
+        o = wi.WindOptions(**{**base, **kw})
+        wi.set_options(o)
+        st = step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        st = step()
+        e1.record()
+        torch.cuda.synchronize()
+        ok = st["status"] == 0 and st["precond"] == 1
+        table[name] = round(e0.elapsed_time(e1), 3) if ok else None
+    good = {k: v for k, v in table.items() if v is not None}
+    best = min(good, key=good.get) if good else "V(1,1)"
+    opt = wi.WindOptions(**{**base, **MG_CYCLES[best]})
+    wi.set_options(opt)
+    return opt, best, table
+
+
+def solver_kwargs(name: str) -> dict:
+    """WindOptions keyword arguments of a solver preset (with the command-line overrides)."""
+    from hicar_b200 import _capi
     presets = {
         # the reference's method and kernel schedule, FP64 Krylov vectors
         "plain": dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64),
@@ -113,7 +153,12 @@ def solver_options(name: str):
         kw["mg_w_levels"] = tuple(MG_W_LEVELS)
     if FGMRES_RESTART is not None and "fgmres_restart" in kw:
         kw["fgmres_restart"] = FGMRES_RESTART
-    return wi.WindOptions(tol_rel=TOL, wind_solver_iterations=3000, **kw)
+    return dict(tol_rel=TOL, wind_solver_iterations=3000, **kw)
+
+
+def solver_options(name: str):
+    from hicar_b200 import wind_iterative as wi
+    return wi.WindOptions(**solver_kwargs(name))
 
 
 class ClockSampler:
@@ -306,7 +351,7 @@ def profile_roofline(lib, h, stream, ncu_range: bool, cells: int):
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
 
 
-def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, solver):
+def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, solver, opts=None):
     """Relative L2 differences of lambda and u/v/w between one solve of `solver`
     (tolerance TOL) and a tight FP64 solve of the same system (FGMRES + V-cycle to
     1e-11), and the final divergence of both corrected wind fields relative to the
@@ -327,7 +372,7 @@ def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, solver):
         wind.calc_divergence(div, dom, use_dqdt=True)
         return st, lam, winds, float(div.double().norm()) / d0
 
-    st_a, lam_a, w_a, div_a = solve_with(solver_options(solver))
+    st_a, lam_a, w_a, div_a = solve_with(opts if opts is not None else solver_options(solver))
     tight = solver_options("fgmres")
     tight.tol_rel, tight.wind_solver_iterations, tight.stall_iters = 1e-11, 6000, 0
     st_t, lam_t, w_t, div_t = solve_with(tight)
@@ -397,6 +442,18 @@ def run_ours(args, wl):
         wind.calc_divergence(div, dom, use_dqdt=True)
         return wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
 
+    cycle = None
+    if args.solver == "mg":
+        overridden = MG_COARSE_SCALE is not None or MG_OMEGA is not None or MG_SKIP_FINE_PRE or bool(MG_W_LEVELS)
+        if MG_CYCLE == "auto" and not overridden:
+            opt, name, table = pick_cycle(wi, step, solver_kwargs(args.solver))
+            cycle = {"chosen": name, "warmup_solve_ms": table, **{k: v for k, v in MG_CYCLES[name].items()}}
+        elif MG_CYCLE != "auto":
+            opt = wi.WindOptions(**{**solver_kwargs(args.solver), **MG_CYCLES[MG_CYCLE]})
+            wi.set_options(opt)
+            cycle = {"chosen": MG_CYCLE, **MG_CYCLES[MG_CYCLE]}
+        if cycle is not None:
+            cycle = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cycle.items()}
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -464,7 +521,7 @@ def run_ours(args, wl):
     # ---- accuracy: this solver's lambda / winds / final divergence against a tight FP64 solve ----
     accuracy = None
     if not args.no_accuracy:
-        accuracy = accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, args.solver)
+        accuracy = accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, args.solver, opt)
         wi.set_options(opt)
 
     cpu = None
@@ -482,7 +539,7 @@ def run_ours(args, wl):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {wl['nx']}x{wl['ny']}x{wl['nz']} terrain case, "
                                    f"{wl['n_hills']} hills, alpha={wl['alpha']}, adv_den={wl['adv_den']}",
-                       "solver": args.solver, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
+                       "solver": args.solver, "mg_cycle": cycle, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
                        "iterations": it[0], "ref_method_iterations": ref_iters, "true_res_rel": max(tr),
                        "plain_gpu_solves_per_s": 1000.0 / plain_ms,
                        "speedup_vs_plain_gpu": value / world / (1000.0 / plain_ms), "accuracy": accuracy,
@@ -640,7 +697,7 @@ def run_batch(args, wl):
 
 
 def main():
-    global TOL, MG_COARSE_SCALE, MG_OMEGA, MG_SKIP_FINE_PRE, MG_W_LEVELS, FGMRES_RESTART
+    global TOL, MG_COARSE_SCALE, MG_OMEGA, MG_SKIP_FINE_PRE, MG_W_LEVELS, MG_CYCLE, FGMRES_RESTART
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -654,6 +711,8 @@ def main():
                     help="override the V-cycle's coarse-correction scale of the solver preset")
     ap.add_argument("--mg-skip-fine-presmooth", action="store_true",
                     help="V(0,1) on the finest level of the V-cycle (no pre-smoothing there)")
+    ap.add_argument("--mg-cycle", default="auto", choices=["auto"] + list(MG_CYCLES),
+                    help="cycle shape of the mg preset (auto: the fastest on the workload, picked in the warm-up)")
     ap.add_argument("--mg-w-levels", default="",
                     help="comma-separated V-cycle levels (>= 1) that correct twice from the coarse grid")
     ap.add_argument("--mg-omega", type=float, default=None,
@@ -673,6 +732,7 @@ def main():
     MG_OMEGA = args.mg_omega
     MG_SKIP_FINE_PRE = args.mg_skip_fine_presmooth
     MG_W_LEVELS = tuple(int(x) for x in args.mg_w_levels.split(",") if x.strip())
+    MG_CYCLE = args.mg_cycle
     FGMRES_RESTART = args.fgmres_restart
     wl = WORKLOADS[args.workload]
     if "batch" in wl:
