@@ -383,6 +383,7 @@ extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
     if (pre0_was && !h->mg.pre0 && h->mg.nlev > 0 && h->mg.lev[0].x1) { // the finest x1 must read as zero from now on
         cudaDeviceSynchronize();
         cudaMemset(h->mg.lev[0].x1, 0, (size_t)h->mg.lev[0].d.npad * sizeof(float));
+        cudaDeviceSynchronize(); // complete before work on any stream, non-blocking ones included
     }
     return rc;
 }
