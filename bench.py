@@ -84,12 +84,14 @@ def peaks():
 # Cycle shapes among which the mg preset picks on the problem at hand (in the
 # untimed warm-up): the V-cycle with pre- and post-smoothing on every level
 # (omega 0.8), V(0,1) on the finest level with omega 1, and the same with two
-# coarse-grid corrections (a W-cycle) on levels 2-3 or 2-4.
+# coarse-grid corrections (a W-cycle) on levels 2-3, 2-4, 3-4 or 4-5.
 MG_CYCLES = {
     "V(1,1)": dict(),
     "V(0,1)": dict(mg_skip_fine_presmooth=True, mg_omega=1.0),
     "V(0,1)+W2-3": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
     "V(0,1)+W2-4": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)),
+    "V(0,1)+W3-4": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(3, 4)),
+    "V(0,1)+W4-5": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(4, 5)),
 }
 MG_CYCLE = "auto"  # --mg-cycle
 

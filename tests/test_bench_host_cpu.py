@@ -37,7 +37,7 @@ def test_cycle_choice_keeps_fastest_converged_candidate(monkeypatch):
     def step():
         o = applied[-1]
         key = tuple(o.mg_w_levels)
-        ms = runs[key] if not (key == () and o.mg_skip_fine_presmooth) else 300.0
+        ms = runs.get(key, 400.0) if not (key == () and o.mg_skip_fine_presmooth) else 300.0
         _Event.clock[0] += ms
         if key == (2, 3, 4):   # this one stalls and falls back to the reference solve
             return {"status": 3, "precond": 0}
