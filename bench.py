@@ -86,12 +86,12 @@ def peaks():
 # (omega 0.8), V(0,1) on the finest level with omega 1, and the same with two
 # coarse-grid corrections (a W-cycle) on levels 2-3, 2-4, 3-4 or 4-5.
 MG_CYCLES = {
-    "V(1,1)": dict(),
-    "V(0,1)": dict(mg_skip_fine_presmooth=True, mg_omega=1.0),
-    "V(0,1)+W2-3": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
-    "V(0,1)+W2-4": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)),
-    "V(0,1)+W3-4": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(3, 4)),
-    "V(0,1)+W4-5": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(4, 5)),
+    "V11": dict(),
+    "V01": dict(mg_skip_fine_presmooth=True, mg_omega=1.0),
+    "V01-W23": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
+    "V01-W24": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)),
+    "V01-W34": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(3, 4)),
+    "V01-W45": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(4, 5)),
 }
 MG_CYCLE = "auto"  # --mg-cycle
 
@@ -116,7 +116,7 @@ def pick_cycle(wi, step, base: dict):
         ok = st["status"] == 0 and st["precond"] == 1
         table[name] = round(e0.elapsed_time(e1), 3) if ok else None
     good = {k: v for k, v in table.items() if v is not None}
-    best = min(good, key=good.get) if good else "V(1,1)"
+    best = min(good, key=good.get) if good else "V11"
     opt = wi.WindOptions(**{**base, **MG_CYCLES[best]})
     wi.set_options(opt)
     return opt, best, table

@@ -45,8 +45,8 @@ def test_cycle_choice_keeps_fastest_converged_candidate(monkeypatch):
 
     base = bench.solver_kwargs("mg")
     opt, name, table = bench.pick_cycle(wi, step, base)
-    assert table["V(0,1)+W2-4"] is None                  # fell back: never chosen although fastest
-    assert name == "V(0,1)+W2-3" and table[name] == 150.0
+    assert table["V01-W24"] is None                  # fell back: never chosen although fastest
+    assert name == "V01-W23" and table[name] == 150.0
     assert opt.mg_w_levels == (2, 3) and opt.mg_skip_fine_presmooth and opt.mg_omega == 1.0
     assert opt.precond == base["precond"] and opt.stall_iters == base["stall_iters"]
     assert applied[-1] is opt                             # the chosen options are left set
@@ -56,5 +56,5 @@ def test_cycle_choice_keeps_fastest_converged_candidate(monkeypatch):
         return {"status": 3, "precond": 0}
 
     opt, name, table = bench.pick_cycle(wi, bad_step, base)
-    assert name == "V(1,1)" and all(v is None for v in table.values())
+    assert name == "V11" and all(v is None for v in table.values())
     assert opt.mg_w_levels == () and not opt.mg_skip_fine_presmooth
