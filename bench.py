@@ -84,13 +84,14 @@ def peaks():
 # Cycle shapes among which the mg preset picks on the problem at hand (in the
 # untimed warm-up): the V-cycle with pre- and post-smoothing on every level
 # (omega 0.8), V(0,1) on the finest level with omega 1, and the same with two
-# coarse-grid corrections (a W-cycle) on levels 2-3, 2-4, 3-4 or 4-5.
+# coarse-grid corrections (a W-cycle) on levels 2-3, 2-4, 3-4, 3-5 or 4-5.
 MG_CYCLES = {
     "V11": dict(),
     "V01": dict(mg_skip_fine_presmooth=True, mg_omega=1.0),
     "V01-W23": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
     "V01-W24": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)),
     "V01-W34": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(3, 4)),
+    "V01-W35": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(3, 4, 5)),
     "V01-W45": dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(4, 5)),
 }
 MG_CYCLE = "auto"  # --mg-cycle
