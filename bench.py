@@ -582,8 +582,9 @@ def run_batch(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lib = _capi.load()
     stream = torch.cuda.current_stream()
+    cyc = MG_CYCLE if MG_CYCLE != "auto" else "V11"  # batches: the cycle named on the command line, else V(1,1)
     opts = WindOptions(tol_rel=TOL, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50,
-                       advect_density=wl["adv_den"])
+                       advect_density=wl["adv_den"], **MG_CYCLES[cyc])
     bs = BatchSolver(subdomain_cases(wl["batch"], seed=subdomain_seed(rank), nxy=wl["nxy"], nz=wl["nz"],
                                      n_hills=wl["n_hills"],
                                      dx=wl["dx"]), options=opts, stream=stream.cuda_stream)
@@ -681,7 +682,8 @@ def run_batch(args, wl):
             "config": {"workload": f"{args.workload}: {bs.n} subdomains, nx,ny in {wl['nxy'][0]}..{wl['nxy'][1]} "
                                    f"step {wl['nxy'][2]}, nz in {wl['nz'][0]}..{wl['nz'][1]} step {wl['nz'][2]}, "
                                    f"{bs.cells} cells, {wl['n_hills']} hills each, adv_den={wl['adv_den']}",
-                       "solver": "batched mg (one graph launch per step)", "tol_rel": TOL, "fields": "f32",
+                       "solver": "batched mg (one graph launch per step)", "mg_cycle": cyc, "tol_rel": TOL,
+                       "fields": "f32",
                        "krylov": "f64", "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms,
                        "sequential_solves_per_s": bs.n / (seq_ms / 1000.0), "iterations_min": min(iters),
                        "iterations_max": max(iters), "statuses": sorted(set(s["status"] for s in stats)),
