@@ -15,7 +15,7 @@ HICARW_OK, HICARW_ITER_CAP, HICARW_BREAKDOWN, HICARW_FELL_BACK = 0, 1, 2, 3
 ERRORS = {-1: "HICARW_ERR_ARG", -2: "HICARW_ERR_STATE", -3: "HICARW_ERR_CUDA", -4: "HICARW_ERR_DIVERGED",
           -5: "HICARW_ERR_NAN", -6: "HICARW_ERR_TIMEOUT"}
 MEM_DEVICE, MEM_HOST = 0, 1
-KRYLOV_F64, KRYLOV_F32 = 0, 1
+KRYLOV_F64, KRYLOV_F32, KRYLOV_F32_X64 = 0, 1, 2
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_FGMRES = 0, 1, 2, 3
 CRIT_RECURRENCE, CRIT_TRUE = 0, 1
 PRECOND_JACOBI, PRECOND_MG, PRECOND_LEARNED = 0, 1, 2

@@ -219,12 +219,19 @@ static int ensure_vectors(hicarw_handle *h, int prec)
 {
     const Dims &d = h->d;
     if (h->vprec == prec) return 0;
-    size_t es = prec == HICARW_KRYLOV_F64 ? 8 : 4;
+    // FP64 vectors for HICARW_KRYLOV_F64; FP32 otherwise, except lambda (V_X),
+    // which HICARW_KRYLOV_F32_X64 accumulates in FP64
+    const bool x_was64 = h->vprec == HICARW_KRYLOV_F64 || h->vprec == HICARW_KRYLOV_F32_X64;
+    const bool x_is64 = prec == HICARW_KRYLOV_F64 || prec == HICARW_KRYLOV_F32_X64;
     void *nv[NVEC] = {};
-    for (int q = 0; q < NVEC; q++) CK(dalloc(&nv[q], (size_t)d.npad * es));
+    for (int q = 0; q < NVEC; q++) {
+        const size_t es = prec == HICARW_KRYLOV_F64 || (q == V_X && x_is64) ? 8 : 4;
+        CK(dalloc(&nv[q], (size_t)d.npad * es));
+    }
     if (h->vprec >= 0) { // carry the warm-start lambda across a precision change
-        if (prec == HICARW_KRYLOV_F64) launch_convert<float, double>(d.npad, (const float *)h->vec[V_X], (double *)nv[V_X], 0);
-        else launch_convert<double, float>(d.npad, (const double *)h->vec[V_X], (float *)nv[V_X], 0);
+        if (x_is64 && !x_was64) launch_convert<float, double>(d.npad, (const float *)h->vec[V_X], (double *)nv[V_X], 0);
+        else if (!x_is64 && x_was64) launch_convert<double, float>(d.npad, (const double *)h->vec[V_X], (float *)nv[V_X], 0);
+        else CK(cudaMemcpy(nv[V_X], h->vec[V_X], (size_t)d.npad * (x_is64 ? 8 : 4), cudaMemcpyDeviceToDevice));
         CK(cudaDeviceSynchronize());
         for (int q = 0; q < NVEC; q++) cudaFree(h->vec[q]);
     }
@@ -237,6 +244,9 @@ static int ensure_vectors(hicarw_handle *h, int prec)
 
 template <typename T>
 static T *V(hicarw_handle *h, int q) { return (T *)h->vec[q]; }
+
+// lambda (V_X) is FP64 for the FP64 vectors and for FP32 vectors with FP64 accumulation
+static bool x64(const hicarw_handle *h) { return h->vprec != HICARW_KRYLOV_F32; }
 
 // Krylov vector precision of the configured solve: the reference schedule takes
 // the option, FGMRES is FP64, the FP32 schedules are FP32.
@@ -262,6 +272,8 @@ extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options
                                       int mem_kind, void *stream, hicarw_handle **out)
 {
     if (!g || !m || !out || g->nx < 3 || g->ny < 3 || g->nz < 2 || !(g->dx > 0.0f)) return HICARW_ERR_ARG;
+    if (opt && (opt->krylov_precision < HICARW_KRYLOV_F64 || opt->krylov_precision > HICARW_KRYLOV_F32_X64))
+        return HICARW_ERR_ARG;
     hicarw_handle *h = new hicarw_handle();
     Dims &d = h->d;
     d.nx = g->nx; d.ny = g->ny; d.nz = g->nz;
@@ -364,7 +376,8 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
 
 extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
 {
-    if (!h || !opt) return HICARW_ERR_ARG;
+    if (!h || !opt || opt->krylov_precision < HICARW_KRYLOV_F64 || opt->krylov_precision > HICARW_KRYLOV_F32_X64)
+        return HICARW_ERR_ARG;
     h->opt = *opt;
     if (h->opt.check_every <= 0) h->opt.check_every = 8;
     if (h->opt.replace_every <= 0) h->opt.replace_every = 50;
@@ -434,6 +447,28 @@ static void enqueue_iteration(hicarw_handle *h, XT *x, int sweeps, cudaStream_t 
     launch_update_xrp<VT, XT>(h->d, x, phat, shat, r, sv, t, p, v, st, s); // :755-783
 }
 
+// One iteration of the reference schedule in the vector precision prec.
+static void enqueue_iteration_prec(hicarw_handle *h, int prec, int sweeps, cudaStream_t s)
+{
+    if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), sweeps, s);
+    else if (prec == HICARW_KRYLOV_F32_X64) enqueue_iteration<float, double>(h, V<double>(h, V_X), sweeps, s);
+    else enqueue_iteration<float, float>(h, V<float>(h, V_X), sweeps, s);
+}
+
+// The set-up kernel (r = b - A x, r^ = p = r and the first dots) in the vector precision prec.
+static void enqueue_setup_prec(hicarw_handle *h, int prec, const OpCtx &c, const RedBuf &rb, cudaStream_t s)
+{
+    if (prec == HICARW_KRYLOV_F64)
+        launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
+                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+    else if (prec == HICARW_KRYLOV_F32_X64)
+        launch_setup<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
+                                    V<float>(h, V_P), h->st, h->hist, rb, s);
+    else
+        launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
+                                   V<float>(h, V_P), h->st, h->hist, rb, s);
+}
+
 static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec **out)
 {
     GraphKey key{prec, sweeps, chunk, h->opt.solver, h->opt.replace_every, h->use_mg};
@@ -445,8 +480,7 @@ static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec
     CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
     for (int q = 0; q < chunk; q++) {
         if (h->opt.solver == HICARW_SOLVER_REFERENCE) {
-            if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), sweeps, h->cap);
-            else enqueue_iteration<float, float>(h, V<float>(h, V_X), sweeps, h->cap);
+            enqueue_iteration_prec(h, prec, sweeps, h->cap);
         } else {
             FusedCtx fc = fused_ctx(h);
             fused_enqueue_iteration(fc, sweeps, h->opt.solver == HICARW_SOLVER_MIXED, h->cap);
@@ -526,12 +560,7 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
                        h->use_mg ? h->opt.stall_iters : 0, s);
     CK(cudaEventRecord(h->t0, s));
     if (solver == HICARW_SOLVER_REFERENCE) {
-        if (prec == HICARW_KRYLOV_F64)
-            launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
-                                         V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
-        else
-            launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R),
-                                       V<float>(h, V_RHAT), V<float>(h, V_P), h->st, h->hist, rb, s);
+        enqueue_setup_prec(h, prec, c, rb, s);
         rc = run_loop(h, prec, sweeps, s);
         if (rc) return rc;
     } else {
@@ -560,6 +589,8 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     if (solver == HICARW_SOLVER_REFERENCE) {
         if (prec == HICARW_KRYLOV_F64)
             launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
+        else if (prec == HICARW_KRYLOV_F32_X64)
+            launch_true_residual<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
         else
             launch_true_residual<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
     } else {
@@ -750,7 +781,7 @@ static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float 
 {
     Metrics m = metrics_of(h);
     if (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES) {
-        if (h->vprec == HICARW_KRYLOV_F64) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
+        if (x64(h)) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
         else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
     } else {
         FusedCtx fc = fused_ctx(h);
@@ -762,7 +793,7 @@ static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float 
 
 static int zero_solution(hicarw_handle *h, cudaStream_t s)
 {
-    size_t es = h->vprec == HICARW_KRYLOV_F64 ? 8 : 4;
+    size_t es = x64(h) ? 8 : 4;
     CK(cudaMemsetAsync(h->vec[V_X], 0, (size_t)h->d.npad * es, s));
     if (h->fb.ready) CK(cudaMemsetAsync(h->fb.x64, 0, (size_t)h->d.npad * 8, s));
     return 0;
@@ -913,7 +944,7 @@ extern "C" int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int
 {
     if (!h || ca < 0 || ca > 2 || cb < 0 || cb > 2 || cc < 0 || cc > 2) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->vprec == HICARW_KRYLOV_F64) launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
+    if (x64(h)) launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
     else launch_probe_pattern<float>(h->d, V<float>(h, V_X), ca, cb, cc, s);
     return HICARW_OK;
 }
@@ -949,7 +980,7 @@ extern "C" int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alp
     if ((rc = stage_in(h, v, &h->sv, n_v(d), mem_kind, s, &dv)) != 0) return rc;
     if ((rc = stage_in(h, w, &h->sw, n_cell(d), mem_kind, s, &dw)) != 0) return rc;
     Metrics m = metrics_of(h);
-    if (h->vprec == HICARW_KRYLOV_F64) launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
+    if (x64(h)) launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
     else launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
     if (mem_kind == HICARW_MEM_HOST) {
         CK(cudaMemcpyAsync(u, du, n_u(d) * 4, cudaMemcpyDeviceToHost, s));
@@ -1023,12 +1054,12 @@ extern "C" int hicarw_calibrate_projection_operator(hicarw_handle *h, const floa
     for (int cc = 0; cc < 3; cc++)
         for (int cb = 0; cb < 3; cb++)
             for (int ca = 0; ca < 3; ca++) {
-                if (h->vprec == HICARW_KRYLOV_F64) launch_probe_pattern<double>(d, V<double>(h, V_X), ca, cb, cc, s);
+                if (x64(h)) launch_probe_pattern<double>(d, V<double>(h, V_X), ca, cb, cc, s);
                 else launch_probe_pattern<float>(d, V<float>(h, V_X), ca, cb, cc, s);
                 CK(cudaMemsetAsync(h->sprobe_u, 0, n_u(d) * 4, s));
                 CK(cudaMemsetAsync(h->sprobe_v, 0, n_v(d) * 4, s));
                 CK(cudaMemsetAsync(h->sprobe_w, 0, n_cell(d) * 4, s));
-                if (h->vprec == HICARW_KRYLOV_F64)
+                if (x64(h))
                     launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
                 else
                     launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
@@ -1056,7 +1087,7 @@ extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind,
     CK(cudaMalloc((void **)&gath, n * 8));
     const double *src64 = nullptr;
     if (h->opt.solver == HICARW_SOLVER_MIXED && h->fb.ready) src64 = h->fb.x64;
-    else if (h->vprec == HICARW_KRYLOV_F64) src64 = V<double>(h, V_X);
+    else if (x64(h)) src64 = V<double>(h, V_X);
     else {
         launch_convert<float, double>(d.npad, V<float>(h, V_X), conv, s);
         src64 = conv;
@@ -1280,12 +1311,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         RedBuf rb{h->partials, h->red_blocks};
         if ((rc = zero_solution(h, s)) != 0) return rc;
         launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, 0, s);
-        if (prec == HICARW_KRYLOV_F64)
-            launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
-                                         V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
-        else
-            launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R),
-                                       V<float>(h, V_RHAT), V<float>(h, V_P), h->st, h->hist, rb, s);
+        enqueue_setup_prec(h, prec, c, rb, s);
     }
     prof_state_kernel<<<1, 1, 0, s>>>(h->st, 1);
     CK(cudaStreamSynchronize(s));
@@ -1296,8 +1322,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         if (solver == HICARW_SOLVER_FGMRES) {
             fgmres_enqueue_cycle(fg, s);
         } else if (solver == HICARW_SOLVER_REFERENCE) {
-            if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), h->precond_n_sweeps, s);
-            else enqueue_iteration<float, float>(h, V<float>(h, V_X), h->precond_n_sweeps, s);
+            enqueue_iteration_prec(h, prec, h->precond_n_sweeps, s);
         } else {
             FusedCtx fc = fused_ctx(h);
             fused_enqueue_iteration(fc, h->precond_n_sweeps, solver == HICARW_SOLVER_MIXED, s);

@@ -349,3 +349,33 @@ def test_column_marching_solve(case, monkeypatch):
     assert res["1"][0]["status"] == 0
     assert abs(res["1"][0]["iterations"] - res["0"][0]["iterations"]) <= 1
     assert _rel(res["1"][1], res["0"][1]) < 1e-6
+
+
+@pytest.mark.parametrize("wlev", [(), (1, 2)])
+def test_mg_solve_fp32_vectors_fp64_lambda(case, wlev):
+    """FP32 Krylov vectors with FP64 reductions and FP64 accumulation of lambda
+    (HICARW_KRYLOV_F32_X64), multigrid-preconditioned, at the benchmark's 1e-6:
+    the FP64 true residual meets the tolerance, and the iterations, lambda and
+    winds follow the FP64-vector solve of the same system."""
+    from hicar_b200 import wind, wind_iterative as wi
+    dom, _, div, _ = _calibrated(case)
+    h = wi.handle(dom.nest_indx)
+    cyc = dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=wlev) if wlev else {}
+    res = {}
+    for prec in (_capi.KRYLOV_F64, _capi.KRYLOV_F32_X64):
+        wi.set_options(wi.WindOptions(tol_rel=1e-6, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                                      stall_iters=50, krylov_precision=prec, **cyc))
+        dom.set_winds(case.u, case.v, case.w)
+        _capi.load().hicarw_reset_solution(h, None)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+        lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+        _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
+        res[prec] = (st, lam, dom.u_dqdt.cpu().numpy().copy())
+    st64, lam64, u64 = res[_capi.KRYLOV_F64]
+    st32, lam32, u32 = res[_capi.KRYLOV_F32_X64]
+    assert st32["status"] == 0 and st32["precond"] == _capi.PRECOND_MG
+    assert 0.0 <= st32["true_res"] <= 1.01 * st32["target"]
+    assert abs(st32["iterations"] - st64["iterations"]) <= 2
+    assert _rel(lam32, lam64) < 1e-5
+    assert _rel(u32, u64) < 1e-5
