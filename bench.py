@@ -341,7 +341,7 @@ def run_reference(args, wl):
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
-def profile_roofline(lib, h, stream, ncu_range: bool, cells: int):
+def profile_roofline(lib, h, stream, ncu_range: bool, cells: int, fp64_vectors: bool = True):
     """Per-launch CUDA-event profile of one solve iteration of handle h (every
     kernel of the iteration launched on its own, timed on `stream`) -> the
     roofline object of the dominant kernel."""
@@ -371,7 +371,9 @@ def profile_roofline(lib, h, stream, ncu_range: bool, cells: int):
     ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
             "frac": ach / peak, "peak_kind": peak_kind,
-            "traffic": (TRAFFIC_PER_CELL[dom_k["kernel"]] * cells if dom_k["kernel"] in TRAFFIC_PER_CELL else None),
+            # the captured traffic is that of the FP64-vector kernels; none for another variant
+            "traffic": (TRAFFIC_PER_CELL[dom_k["kernel"]] * cells
+                        if dom_k["kernel"] in TRAFFIC_PER_CELL and fp64_vectors else None),
             "share": dom_k["share_ms"] / tot,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
 
@@ -541,7 +543,8 @@ def run_ours(args, wl):
     e2e_value = world * e2e_steps / (te / 1000.0)
 
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
-    roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", dom.nx * dom.ny * dom.nz)
+    roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", dom.nx * dom.ny * dom.nz,
+                                fp64_vectors=int(opt.krylov_precision) == 0)
 
     # ---- accuracy: this solver's lambda / winds / final divergence against a tight FP64 solve ----
     accuracy = None
