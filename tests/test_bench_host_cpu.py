@@ -86,3 +86,21 @@ def test_no_candidate_converges(monkeypatch):
     opt, name, table = bench.pick_cycle(wi, bad_step, bench.solver_kwargs("mg"))
     assert name == "V11" and all(v is None for v in table.values())
     assert opt.mg_w_levels == () and not opt.mg_skip_fine_presmooth
+
+
+def test_shorter_graphs_kept_when_faster(monkeypatch):
+    import bench
+    wi, applied = _setup(monkeypatch)
+    inner = _fake_step(applied, 0.9, 9.5e-7)
+
+    def step():
+        t0 = _Event.clock[0]
+        st = inner()
+        if applied[-1].check_every == 4:        # fewer iterations launched past convergence
+            _Event.clock[0] = t0 + 0.95 * (_Event.clock[0] - t0)
+        return st
+
+    opt, name, table = bench.pick_cycle(wi, step, bench.solver_kwargs("mg"))
+    assert name == "V01-W23/f32-vectors/chunk4"
+    assert opt.check_every == 4 and opt.krylov_precision == 2 and opt.mg_w_levels == (2, 3)
+    assert table[name] < table["V01-W23/f32-vectors"] < table["V01-W23"]
