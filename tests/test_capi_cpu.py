@@ -57,3 +57,16 @@ def test_bad_arguments_are_errors_not_aborts(lib):
     assert rc == -1
     assert lib.hicarw_finalize_iter_winds(None) == -1
     assert lib.hicarw_calc_iter_winds(None, None, None, None, 0, None, None, None, 0, None, None) == -1
+
+
+def test_unknown_krylov_precision_is_rejected_before_cuda(lib):
+    """An out-of-range krylov_precision is an argument error, returned before
+    any CUDA call (valid grid and metrics otherwise)."""
+    h = C.c_void_p()
+    g = _capi.Grid(16, 16, 8, 250.0, 1)
+    m = _capi.Metrics()
+    o = _capi.default_options()
+    for bad in (-1, 3, 99):
+        o.krylov_precision = bad
+        assert lib.hicarw_init_iter_winds(C.byref(g), C.byref(o), C.byref(m), 0, None, C.byref(h)) == -1
+        assert not h.value
