@@ -1,9 +1,9 @@
-"""GPU tests of the V-cycle and Krylov options added after the multigrid
-kernels' last full GPU validation: V(0,1) on the finest level, W-cycles on
-chosen coarse levels, FP32 Krylov vectors with FP64 lambda, and the opt-in
-column-marching operator kernels.  Kept in a file that pytest collects after
-every other GPU test except the allocation-free entry point's, so that a
-failure here cannot stop a `-x` run before the rest has run."""
+"""GPU tests of the solver options beyond the default configuration: V(0,1)
+on the finest level, W-cycles on chosen coarse levels, FP32 Krylov vectors with
+FP64 lambda, and the opt-in column-marching operator kernels.  Kept in a file
+that pytest collects after the tests of the default configuration (and before
+the allocation-free entry point's), so that a failure of an option cannot stop
+a `-x` run before those have run."""
 import os
 
 import numpy as np
