@@ -624,6 +624,213 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Fused coarse cycle.  Below a level of at most MG_FUSE_COLS columns the
+// cycle is a chain of restriction and post-smoothing steps on tiny levels
+// whose time is set by launch and memory latency (10-15 us per launch for a
+// few hundred KB).  One thread-block cluster runs the whole chain instead:
+// the host records the steps of coarse_cycle(l0) (levels l0 .. bottom, the
+// W-cycle repeats included) into a kernel parameter, and the cluster's CTAs
+// walk it, each step's column tiles spread over the CTAs, a hardware cluster
+// barrier (arrive.release / wait.acquire) between steps.  Every cell's
+// arithmetic is that of restrict_pre_kernel and post_kernel; only the tiling
+// differs (which does not change any cell's result).  Values written inside
+// the kernel are read back with ld.global.cg (L2), never through the
+// read-only path.
+// ---------------------------------------------------------------------------
+constexpr int MG_FUSE_COLS = 1024;  // first fused level: nx * ny at most this
+constexpr int MG_FUSE_STEPS = 48;   // longest recorded chain (else the per-level launches run)
+constexpr int MG_FUSE_THREADS = 512;
+
+struct CoarseStep {
+    int kind;   // 0: restriction of level f + pre-smoothing of level c; 1: post-smoothing of level f
+    int tx, ty; // tile in columns: of level c (kind 0) or of level f (kind 1)
+    float omega, cscale;
+    Dims f, c;
+    const float *coef_f, *cp_f, *minv_f, *r_f, *x1_f; // level f (x1_f: the iterate restricted / corrected)
+    const float *coef_c, *cp_c, *minv_c;              // kind 0: level c
+    float *r_c, *out_c;                               // kind 0: coarse right-hand side and pre-smoothed iterate
+    const float *xc;                                  // kind 1: coarse correction
+    float *out;                                       // kind 1: post-smoothed iterate
+};
+
+struct CoarseProg {
+    int n;
+    CoarseStep step[MG_FUSE_STEPS];
+};
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// stencil_regs with runtime window strides
+__device__ __forceinline__ double stencil_regs_rt(const float (&cv)[15], const float *xs, int SX, int SP)
+{
+    double y = 0.0;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y += (double)cv[q] * (double)xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]];
+    return y;
+}
+
+// stage_window with a runtime window shape; x1 and xc are read through L2
+__device__ __forceinline__ void stage_window_rt(const Dims &d, const float *x1, const Dims &dc, const float *xc, int ia,
+                                                int ja, int SX, int SY, float *s_x, float cs)
+{
+    const int SP = SX * SY, nst = SP * (d.nz + 2);
+    for (int t = threadIdx.x; t < nst; t += blockDim.x) {
+        const int lx = t % SX, ly = (t / SX) % SY, k = t / SP;
+        const int i = ia + lx, j = ja + ly;
+        float a = 0.0f;
+        if (inside(d, i, k, j)) {
+            a = __ldcg(x1 + kidx(d, i, k, j));
+            if (xc) a += cs * __ldcg(xc + kidx(dc, (i + 1) >> 1, k, (j + 1) >> 1));
+        }
+        s_x[t] = a;
+    }
+}
+
+// restrict_pre_kernel<float, TX, TY, false> on coarse tile (bx, by)
+__device__ void fused_restrict(const CoarseStep &p, int bx, int by, float *sm)
+{
+    const Dims &f = p.f, &dc = p.c;
+    const int TX = p.tx, TY = p.ty, TC = TX * TY, FX = 2 * TX + 2, FY = 2 * TY + 2, FP = FX * FY;
+    const int nz = f.nz, n = TC * nz;
+    float *s_res = sm, *s_c = sm + n, *s_m = sm + 2 * n, *s_cp = sm + 3 * n, *s_x = sm + 4 * n;
+    const int I0 = bx * TX + 1, J0 = by * TY + 1;
+    stage_window_rt(f, p.x1_f, f, nullptr, 2 * I0 - 2, 2 * J0 - 2, FX, FY, s_x, 1.0f);
+    __syncthreads();
+    const long long cofs = (long long)CC * dc.npad;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int c = t % TC, k = t / TC + 1;
+        const int lX = c % TX, lY = c / TX;
+        const int I = I0 + lX, J = J0 + lY;
+        if (I > dc.nx || J > dc.ny) continue;
+        const long long oc = kidx(dc, I, k, J);
+        const float vc = k > 1 ? __ldg(p.coef_c + cofs + oc) : 0.0f;
+        const float vm = __ldg(p.minv_c + oc), vp = __ldg(p.cp_c + oc);
+        double acc = 0.0;
+#pragma unroll
+        for (int pj = 0; pj < 2; pj++) {
+            const int j = 2 * J - 1 + pj, i0c = 2 * I - 1;
+            if (j > f.ny) continue;
+            const bool has1 = i0c + 1 <= f.nx;
+            const long long o0 = kidx(f, i0c, k, j), o1 = o0 + 1;
+            float cv0[15], cv1[15];
+            load_coefs(p.coef_f, f.npad, o0, cv0);
+            double r0 = (double)__ldcg(p.r_f + o0), r1 = 0.0;
+            if (has1) {
+                load_coefs(p.coef_f, f.npad, o1, cv1);
+                r1 = (double)__ldcg(p.r_f + o1);
+            }
+            const float *xs0 = s_x + k * FP + (2 * lY + pj + 1) * FX + (2 * lX + 1);
+            acc += r0 - stencil_regs_rt(cv0, xs0, FX, FP);
+            if (has1) acc += r1 - stencil_regs_rt(cv1, xs0 + 1, FX, FP);
+        }
+        const float rc = (float)acc;
+        p.r_c[oc] = rc;
+        s_res[t] = rc;
+        s_c[t] = vc;
+        s_m[t] = vm;
+        s_cp[t] = vp;
+    }
+    __syncthreads();
+    if (threadIdx.x < TC) {
+        const int c = threadIdx.x;
+        if (I0 + c % TX <= dc.nx && J0 + c / TX <= dc.ny) thomas_column(s_res, s_c, s_m, s_cp, c, TC, nz);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int c = t % TC, k = t / TC + 1;
+        const int I = I0 + c % TX, J = J0 + c / TX;
+        if (I > dc.nx || J > dc.ny) continue;
+        p.out_c[kidx(dc, I, k, J)] = p.omega * s_res[t];
+    }
+    __syncthreads(); // the next tile reuses the shared memory
+}
+
+// post_kernel<float, float, TX, TY> on tile (bx, by) of level f
+__device__ void fused_post(const CoarseStep &p, int bx, int by, float *sm)
+{
+    const Dims &d = p.f;
+    const int TX = p.tx, TY = p.ty, TC = TX * TY, SX = TX + 2, SY = TY + 2, SP = SX * SY;
+    const int nz = d.nz, n = TC * nz;
+    float *s_res = sm, *s_c = sm + n, *s_m = sm + 2 * n, *s_cp = sm + 3 * n, *s_x = sm + 4 * n;
+    const int i0 = bx * TX + 1, j0 = by * TY + 1;
+    stage_window_rt(d, p.x1_f, p.c, p.xc, i0 - 1, j0 - 1, SX, SY, s_x, p.cscale);
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int c = t % TC, k = t / TC + 1;
+        const int lx = c % TX, ly = c / TX;
+        const int i = i0 + lx, j = j0 + ly;
+        float res2 = 0.0f, vc = 0.0f, vm = 0.0f, vp = 0.0f;
+        if (i <= d.nx && j <= d.ny) {
+            const long long o = kidx(d, i, k, j);
+            const float *xs = s_x + k * SP + (ly + 1) * SX + (lx + 1);
+            float cv[15];
+            load_coefs(p.coef_f, d.npad, o, cv);
+            const double rv = (double)__ldcg(p.r_f + o);
+            vm = __ldg(p.minv_f + o);
+            vp = __ldg(p.cp_f + o);
+            vc = k > 1 ? cv[CC] : 0.0f;
+            res2 = (float)(rv - stencil_regs_rt(cv, xs, SX, SP));
+        }
+        s_res[t] = res2;
+        s_c[t] = vc;
+        s_m[t] = vm;
+        s_cp[t] = vp;
+    }
+    __syncthreads();
+    if (threadIdx.x < TC) {
+        const int c = threadIdx.x;
+        if (i0 + c % TX <= d.nx && j0 + c / TX <= d.ny) thomas_column(s_res, s_c, s_m, s_cp, c, TC, nz);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int c = t % TC, k = t / TC + 1;
+        const int lx = c % TX, ly = c / TX;
+        const int i = i0 + lx, j = j0 + ly;
+        if (i > d.nx || j > d.ny) continue;
+        const float base = s_x[k * SP + (ly + 1) * SX + (lx + 1)];
+        p.out[kidx(d, i, k, j)] = (float)((double)base + (double)p.omega * (double)s_res[t]);
+    }
+    __syncthreads();
+}
+
+// One cluster walks the recorded chain.  The stop flag was set (or not) before
+// this launch, so every CTA of the cluster takes the same branch and reaches
+// the same barriers.
+__global__ void __launch_bounds__(MG_FUSE_THREADS) coarse_cycle_kernel(const __grid_constant__ CoarseProg prog,
+                                                                       const SolveState *gate)
+{
+    if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
+    extern __shared__ float sm[];
+    const int rank = (int)cluster_rank(), ncta = (int)cluster_size();
+    for (int q = 0; q < prog.n; q++) {
+        const CoarseStep &p = prog.step[q];
+        const Dims &td = p.kind == 0 ? p.c : p.f;
+        const int ntx = (td.nx + p.tx - 1) / p.tx, nty = (td.ny + p.ty - 1) / p.ty;
+        for (int t = rank; t < ntx * nty; t += ncta) {
+            if (p.kind == 0) fused_restrict(p, t % ntx, t / ntx, sm);
+            else fused_post(p, t % ntx, t / ntx, sm);
+        }
+        __threadfence();
+        cluster_barrier();
+    }
+}
+
+// ---------------------------------------------------------------------------
 static Dims level_dims(int nx, int ny, int nz, float dx)
 {
     Dims d;
@@ -656,6 +863,7 @@ void mg_free(Mg &mg)
 
 static int sm_count();
 static int smem_optin();
+static void fused_setup(Mg &mg);
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
@@ -665,21 +873,27 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
     if (!same) {
         mg_free(mg);
         int nx = fine.nx, ny = fine.ny, l = 0;
+        // a failed allocation releases every level allocated so far (level l included)
+        auto fail = [&mg](int lev) {
+            mg.nlev = lev + 1;
+            mg_free(mg);
+            return -1;
+        };
         while (true) {
             MgLevel &L = mg.lev[l];
             L.d = l == 0 ? fine : level_dims(nx, ny, fine.nz, fine.dx);
             size_t n = (size_t)L.d.npad;
             if (l > 0) {
-                if (cudaMalloc((void **)&L.coef, 15 * n * sizeof(float)) != cudaSuccess) return -1;
+                if (cudaMalloc((void **)&L.coef, 15 * n * sizeof(float)) != cudaSuccess) return fail(l);
                 cudaMemsetAsync((void *)L.coef, 0, 15 * n * sizeof(float), s);
-                if (cudaMalloc((void **)&L.r, n * sizeof(float)) != cudaSuccess) return -1;
+                if (cudaMalloc((void **)&L.r, n * sizeof(float)) != cudaSuccess) return fail(l);
                 cudaMemsetAsync(L.r, 0, n * sizeof(float), s);
-                if (cudaMalloc((void **)&L.x3, n * sizeof(float)) != cudaSuccess) return -1;
+                if (cudaMalloc((void **)&L.x3, n * sizeof(float)) != cudaSuccess) return fail(l);
                 cudaMemsetAsync(L.x3, 0, n * sizeof(float), s);
             }
-            if (cudaMalloc((void **)&L.cp, n * sizeof(float)) != cudaSuccess) return -1;
-            if (cudaMalloc((void **)&L.minv, n * sizeof(float)) != cudaSuccess) return -1;
-            if (cudaMalloc((void **)&L.x1, n * sizeof(float)) != cudaSuccess) return -1;
+            if (cudaMalloc((void **)&L.cp, n * sizeof(float)) != cudaSuccess) return fail(l);
+            if (cudaMalloc((void **)&L.minv, n * sizeof(float)) != cudaSuccess) return fail(l);
+            if (cudaMalloc((void **)&L.x1, n * sizeof(float)) != cudaSuccess) return fail(l);
             cudaMemsetAsync(L.x1, 0, n * sizeof(float), s);
             l++;
             if ((nx == 1 && ny == 1) || l == MG_MAX_LEVELS) break;
@@ -714,8 +928,10 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
         factor_kernel<<<g, b, 0, s>>>(L.d, L.coef, L.cp, L.minv);
         count_launch(1);
     }
+    const cudaError_t e = cudaGetLastError();
+    fused_setup(mg);
     mg.ready = 1;
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return e == cudaSuccess ? 0 : -1;
 }
 
 static const char *kLevelName[3][MG_MAX_LEVELS] = {
@@ -908,6 +1124,165 @@ static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C,
     count_launch(1);
 }
 
+// ---- fused coarse cycle: recording, tiles, launch ----
+static const char *kFusedName[MG_MAX_LEVELS] = {
+    "mg_coarse_l0", "mg_coarse_l1", "mg_coarse_l2",  "mg_coarse_l3",  "mg_coarse_l4",  "mg_coarse_l5",
+    "mg_coarse_l6", "mg_coarse_l7", "mg_coarse_l8",  "mg_coarse_l9",  "mg_coarse_l10", "mg_coarse_l11",
+    "mg_coarse_l12", "mg_coarse_l13", "mg_coarse_l14", "mg_coarse_l15"};
+
+static size_t fused_step_smem(int kind, int tx, int ty, int nz)
+{
+    const size_t win = kind == 0 ? (size_t)(2 * tx + 2) * (2 * ty + 2) : (size_t)(tx + 2) * (ty + 2);
+    return (4 * (size_t)tx * ty * nz + win * (nz + 2)) * sizeof(float);
+}
+
+// Tile of one step: the smallest of the candidates whose tile count fits the
+// cluster (one tile per CTA), else the largest; then the largest that fits the
+// shared memory.  Returns false when not even one column fits.
+static bool fused_tile(int kind, const Dims &td, int nz, int cn, size_t cap, int *tx, int *ty, size_t *smem)
+{
+    static const int cand[7][2] = {{1, 1}, {2, 1}, {2, 2}, {4, 2}, {4, 4}, {8, 4}, {8, 8}};
+    int q = 6;
+    for (int c = 0; c < 7; c++)
+        if ((long long)((td.nx + cand[c][0] - 1) / cand[c][0]) * ((td.ny + cand[c][1] - 1) / cand[c][1]) <= cn) {
+            q = c;
+            break;
+        }
+    for (; q >= 0; q--)
+        if (fused_step_smem(kind, cand[q][0], cand[q][1], nz) <= cap) break;
+    if (q < 0) return false;
+    *tx = cand[q][0];
+    *ty = cand[q][1];
+    *smem = std::max(*smem, fused_step_smem(kind, *tx, *ty, nz));
+    return true;
+}
+
+// The steps of coarse_cycle(mg, l) below, in launch order; returns the buffer
+// that holds level l's result (false in *ok when the chain is too long).
+static const float *record_cycle(const Mg &mg, int l, CoarseProg &prog, bool *ok)
+{
+    const int L = mg.nlev;
+    const MgLevel &F = mg.lev[l];
+    if (l == L - 1) return F.x3;
+    const MgLevel &C = mg.lev[l + 1];
+    const bool last = l + 1 == L - 1;
+    const int reps = (mg.wmask >> l) & 1 ? 2 : 1;
+    float *cur = F.x1, *other = F.x3;
+    for (int rep = 0; rep < reps && *ok; rep++) {
+        if (prog.n >= MG_FUSE_STEPS) { *ok = false; break; }
+        CoarseStep &a = prog.step[prog.n++];
+        a = CoarseStep{};
+        a.kind = 0;
+        a.f = F.d; a.c = C.d;
+        a.coef_f = F.coef; a.r_f = F.r; a.x1_f = cur;
+        a.coef_c = C.coef; a.cp_c = C.cp; a.minv_c = C.minv; a.r_c = C.r;
+        a.out_c = last ? C.x3 : C.x1;
+        a.omega = last ? 1.0f : mg.omega;
+        const float *xc = record_cycle(mg, l + 1, prog, ok);
+        if (!*ok || prog.n >= MG_FUSE_STEPS) { *ok = false; break; }
+        CoarseStep &b = prog.step[prog.n++];
+        b = CoarseStep{};
+        b.kind = 1;
+        b.f = F.d; b.c = C.d;
+        b.coef_f = F.coef; b.cp_f = F.cp; b.minv_f = F.minv; b.r_f = F.r; b.x1_f = cur;
+        b.xc = xc; b.out = other;
+        b.omega = mg.omega; b.cscale = mg.cscale;
+        std::swap(cur, other);
+    }
+    return cur;
+}
+
+// Largest shared memory any step of the levels from l0 down needs.
+static bool fused_smem(const Mg &mg, int l0, int cn, size_t cap, size_t *smem)
+{
+    *smem = 0;
+    for (int l = l0; l + 1 < mg.nlev; l++) {
+        int tx, ty;
+        if (!fused_tile(0, mg.lev[l + 1].d, mg.lev[l].d.nz, cn, cap, &tx, &ty, smem)) return false;
+        if (!fused_tile(1, mg.lev[l].d, mg.lev[l].d.nz, cn, cap, &tx, &ty, smem)) return false;
+    }
+    return true;
+}
+
+static cudaLaunchConfig_t fused_config(int cn, size_t smem, cudaStream_t s, cudaLaunchAttribute *at)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cn);
+    cfg.blockDim = dim3(MG_FUSE_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cn;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Decide at build time (outside any stream capture) whether and where the
+// coarse part is fused, and the cluster size: 16 CTAs where the device can
+// place such a cluster with this shared memory, else 8, else no fusion.
+static void fused_setup(Mg &mg)
+{
+    mg.fuse_level = 0;
+    mg.cluster_n = 0;
+    const char *e = getenv("HICARW_MG_FUSE");
+    if (e && e[0] == '0') return;
+    int l0 = 0;
+    for (int l = 2; l + 1 < mg.nlev; l++)
+        if ((long long)mg.lev[l].d.nx * mg.lev[l].d.ny <= MG_FUSE_COLS) {
+            l0 = l;
+            break;
+        }
+    if (!l0) return;
+    cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int cn : {16, 8}) {
+        size_t smem = 0;
+        if (!fused_smem(mg, l0, cn, (size_t)smem_optin(), &smem)) continue;
+        if (cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            continue;
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = fused_config(cn, smem, nullptr, at);
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_cycle_kernel, &cfg) == cudaSuccess && nclusters >= 1) {
+            mg.fuse_level = l0;
+            mg.cluster_n = cn;
+            return;
+        }
+        cudaGetLastError(); // a refused size leaves no error behind
+    }
+}
+
+// Enqueue coarse_cycle(mg, l) as one cluster launch; false (nothing launched)
+// when the chain does not fit the recorded program or the shared memory.
+static bool launch_fused(const Mg &mg, int l, const SolveState *gate, cudaStream_t s, const float **result)
+{
+    CoarseProg prog;
+    prog.n = 0;
+    bool ok = true;
+    const float *res = record_cycle(mg, l, prog, &ok);
+    if (!ok || prog.n == 0) return false;
+    size_t smem = 0;
+    double bytes = 0.0;
+    for (int q = 0; q < prog.n; q++) {
+        CoarseStep &p = prog.step[q];
+        const Dims &td = p.kind == 0 ? p.c : p.f;
+        if (!fused_tile(p.kind, td, p.f.nz, mg.cluster_n, (size_t)smem_optin(), &p.tx, &p.ty, &smem)) return false;
+        const double N = (double)p.f.nx * p.f.ny * p.f.nz;
+        bytes += p.kind == 0 ? (60.0 + 4.0 + 4.0) * N : (4.0 + 4.0 + 60.0 + 4.0 + 1.0 + 8.0) * N;
+    }
+    ProfScope ps_(kFusedName[l], bytes, s);
+    cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = fused_config(mg.cluster_n, smem, s, at);
+    cudaLaunchKernelEx(&cfg, coarse_cycle_kernel, prog, gate);
+    count_launch(1);
+    *result = res;
+    return true;
+}
+
 // Coarse part of the cycle below level l >= 1, whose right-hand side r and
 // first iterate x1 (pre-smoothed from zero by the restriction kernel) are in
 // place; returns the buffer that holds level l's result.  A level whose bit
@@ -921,6 +1296,8 @@ static const float *coarse_cycle(const Mg &mg, int l, const SolveState *gate, cu
     const int L = mg.nlev;
     const MgLevel &F = mg.lev[l];
     if (l == L - 1) return F.x3; // exact column solve, written by the restriction from level l - 1
+    const float *fused = nullptr;
+    if (mg.fuse_level > 0 && l == mg.fuse_level && launch_fused(mg, l, gate, s, &fused)) return fused;
     const MgLevel &C = mg.lev[l + 1];
     const bool last = l + 1 == L - 1;
     const int reps = (mg.wmask >> l) & 1 ? 2 : 1;

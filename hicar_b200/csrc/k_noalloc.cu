@@ -18,7 +18,9 @@
 //    of every call, and calls that overlap on the GPU race on the array;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (a host-side name is not a device address); make that
-//    first call before any stream capture.
+//    first call before any stream capture.  The address is cached per device for
+//    the life of the process, which assumes the device's primary context is not
+//    reset (cudaDeviceReset) while the library is loaded.
 #include <cuda_runtime.h>
 #include <stdio.h>
 
@@ -153,19 +155,21 @@ __global__ void __launch_bounds__(256) residual_norm_noalloc_kernel(OpCtx c, con
 static std::mutex g_noalloc_mu;
 static NoallocScratch *g_noalloc_addr[64] = {};
 
-static int noalloc_scratch(NoallocScratch **out)
+// Returns nullptr on success, else the reason the address could not be had.
+static const char *noalloc_scratch(NoallocScratch **out)
 {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return "cudaGetDevice failed";
+    if (dev < 0 || dev >= 64) return "device index outside 0..63 (the per-device address cache has 64 entries)";
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) return -1;
+        if (e != cudaSuccess || p == nullptr) return "cudaGetSymbolAddress of the scratch array failed";
         g_noalloc_addr[dev] = (NoallocScratch *)p;
     }
     *out = g_noalloc_addr[dev];
-    return 0;
+    return nullptr;
 }
 
 extern "C" int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm,
@@ -182,8 +186,10 @@ extern "C" int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, c
         return HICARW_ERR_ARG;
     }
     NoallocScratch *scr = nullptr;
-    if (noalloc_scratch(&scr) != 0) {
-        handle_set_error(h, "hicarw_residual_norm_noalloc: cudaGetSymbolAddress of the scratch array failed");
+    if (const char *why = noalloc_scratch(&scr)) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "hicarw_residual_norm_noalloc: %s", why);
+        handle_set_error(h, msg);
         return HICARW_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;

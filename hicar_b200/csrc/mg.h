@@ -24,6 +24,9 @@ struct Mg {
     int pre0 = 1;        // pre-smooth the finest level (0: V(0,1) there, its x1 kept at zero)
     int wmask = 0;       // bit l (l >= 1): level l corrects twice from the coarse grid (W-cycle there)
     int use_tma = 1;     // post-smoothers of the wide levels fed by tensor copies (HICARW_MG_TMA=0: register-fed)
+    int fuse_level = 0;  // first level of the coarse part run by one thread-block cluster (0: every level its own
+                         // launches; HICARW_MG_FUSE=0 at build time)
+    int cluster_n = 0;   // CTAs of that cluster
     int *err = nullptr;  // device flag: a bounded copy wait of a smoother timed out (calls without a solve state)
     MgLevel lev[MG_MAX_LEVELS];
 };

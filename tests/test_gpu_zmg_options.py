@@ -243,3 +243,75 @@ def test_mg_solve_fp32_vectors_fp64_lambda(case, wlev):
     assert abs(st32["iterations"] - st64["iterations"]) <= 2
     assert _rel(lam32, lam64) < 1e-5
     assert _rel(u32, u64) < 1e-5
+
+
+def _profile_names(h):
+    """Kernel names of one profiled solve iteration of the handle's configuration."""
+    import ctypes as C
+    lib = _capi.load()
+    cap = 64
+    names = C.create_string_buffer(32 * cap)
+    ms, by = (C.c_double * cap)(), (C.c_double * cap)()
+    cnt = (C.c_int * cap)()
+    n = lib.hicarw_profile_iteration(h, 1, names, ms, by, cnt, cap, None)
+    assert n > 0
+    return [names.raw[32 * q:32 * q + 32].split(b"\0")[0].decode() for q in range(n)]
+
+
+@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13), (130, 66, 24)])
+def test_fused_coarse_cycle_bitexact(shape, monkeypatch):
+    """The coarse part of the cycle run by one thread-block cluster (levels of
+    at most 1024 columns; the default) gives the per-level launches' V-cycle bit
+    for bit, for the V-cycle and for W-cycles that reach into the fused levels,
+    on a small grid, a ragged one and one with odd coarse extents."""
+    from hicar_b200 import wind, wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=21, adv_den=True, n_hills=8)
+    rng = np.random.default_rng(29)
+    x = np.zeros((ny + 2, nz + 2, nx + 2))
+    x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
+    cycles = [dict(), dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3)),
+              dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4, 5))]
+    out = {}
+    for fuse in ("0", "1"):
+        monkeypatch.setenv("HICARW_MG_FUSE", fuse)
+        wi.finalize_iter_winds()
+        wind.reset()
+        dom, _, _, _ = _calibrated(case, precond=_capi.PRECOND_MG, stall_iters=50)
+        h = wi.handle(dom.nest_indx)
+        lib = _capi.load()
+        for q, cyc in enumerate(cycles):
+            wi.set_options(wi.WindOptions(precond=_capi.PRECOND_MG, stall_iters=50, **cyc))
+            y = np.empty_like(x)
+            _capi.check(lib.hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
+            out[(fuse, q)] = y
+            fused = any(n.startswith("mg_coarse_l") for n in _profile_names(h))
+            assert fused == (fuse == "1"), (fuse, q)
+    for q in range(len(cycles)):
+        np.testing.assert_array_equal(out[("1", q)], out[("0", q)])
+
+
+def test_fused_coarse_cycle_solve(case, monkeypatch):
+    """A multigrid-preconditioned solve (V(0,1), W on levels 2-4) takes the same
+    iterations to the same lambda with and without the fused coarse cycle."""
+    from hicar_b200 import wind, wind_iterative as wi
+    res = {}
+    for fuse in ("0", "1"):
+        monkeypatch.setenv("HICARW_MG_FUSE", fuse)
+        wi.finalize_iter_winds()
+        wind.reset()
+        dom, _, div, _ = _calibrated(case)
+        h = wi.handle(dom.nest_indx)
+        wi.set_options(wi.WindOptions(tol_rel=1e-9, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                                      stall_iters=50, mg_skip_fine_presmooth=True, mg_omega=1.0,
+                                      mg_w_levels=(2, 3, 4)))
+        dom.set_winds(case.u, case.v, case.w)
+        _capi.load().hicarw_reset_solution(h, None)
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+        lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+        _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
+        res[fuse] = (st, lam)
+    assert res["1"][0]["status"] == 0
+    assert res["1"][0]["iterations"] == res["0"][0]["iterations"]
+    np.testing.assert_array_equal(res["1"][1], res["0"][1])

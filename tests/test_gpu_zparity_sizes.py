@@ -1,0 +1,172 @@
+"""Parity at the configured problem sizes, through the C ABI, against the CPU
+oracle's own solve of the same seeded inputs (the oracle calibrates its own
+probed operator, builds its own right-hand side and corrects its own winds).
+
+* The benchmark's solver options (FP32 Krylov vectors with FP64 reductions and
+  FP64 lambda, V(0,1) multigrid with W-cycles on levels 2-4, omega 1,
+  over-correction 1.35) on the generator of the 1024x1024x64 mixed case
+  (smooth alpha in [0.3, 1], density advected) at 192x192x40.  The hill count
+  is 20: that is already ten times the hill density of the 1024^2 case (60
+  hills on 256 km); at 60 hills on 48 km the reference's own Jacobi-BiCGStab no
+  longer converges, so there would be no reference solve to compare with.
+  Against the reference-precision oracle (FP32 fields and coefficients, FP64
+  Krylov) solved to 1e-12: lambda, u, v, w within 1e-5 relative L2 and the
+  final divergence no larger than the oracle's own at the same tolerance.
+  Against the all-FP64 oracle the errors are stated and bounded by the floor
+  of FP32 arithmetic: the oracle's reference-precision build itself is 2e-6
+  (lambda), 2e-6 (u, v) and 1.7e-5 (w) away from its FP64 build on this case.
+* The plain GPU BiCGStab at 512x512x48 (the reference's method and kernel
+  schedule, FP64 Krylov, 2-sweep Jacobi-Richardson) against the oracle's
+  reference-precision solve of the same system: iterations within 10 %, u, v,
+  w within 1e-5 at the 1e-6 tolerance, and lambda within 1e-5 once both are
+  converged to 1e-9.
+
+These tests run the oracle on the host cores (tens of seconds to a few minutes)
+and are collected after the other GPU tests of the solver.
+"""
+import numpy as np
+import pytest
+
+from hicar_b200 import _capi, cases
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+# the benchmark's multigrid cycle and Krylov precision (bench.py: V01-W24 / f32-vectors)
+HEADLINE = dict(precond=_capi.PRECOND_MG, stall_iters=50, krylov_precision=_capi.KRYLOV_F32_X64,
+                mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4), mg_coarse_scale=1.35)
+
+
+@pytest.fixture(autouse=True)
+def _fresh(lib):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hicar_b200 import wind, wind_iterative
+    wind_iterative.finalize_iter_winds()
+    wind.reset()
+    yield
+    wind_iterative.finalize_iter_winds()
+    wind.reset()
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+class OracleSolve:
+    """The oracle's steady-state solve of a case: its own analytic operator,
+    27-colour calibration, divergence, right-hand side, BiCGStab (continued
+    from one tolerance to the next, as a warm start) and wind correction."""
+
+    def __init__(self, oracle_mod, case, precision):
+        self.case = case
+        s = self.s = oracle_mod.OracleSolver(case.domain, precision, max_iters=20000)
+        self.dt = s.dt
+        s.set_alpha(case.alpha)
+        u, v, w = self._winds()
+        s.build_analytic(case.alpha)
+        s.calibrate(case.adv_den, u, v, w)
+        u, v, w = self._winds()
+        self.div = s.divergence(u, v, w, adv_den=case.adv_den)
+        self.div_norm = float(np.linalg.norm(self.div.astype(np.float64)))
+        s.prepare(self.div)
+        s.set_vec("x", np.zeros((s.ny + 2, s.nz + 2, s.nx + 2)))
+        self.iterations = 0
+
+    def _winds(self):
+        return tuple(np.ascontiguousarray(a, dtype=self.dt).copy() for a in (self.case.u, self.case.v, self.case.w))
+
+    def solve_to(self, tol):
+        """Continue the solve to `tol`; returns lambda, (u, v, w), the final
+        divergence relative to the input's, and the FP64 true residual / |b|."""
+        s = self.s
+        s.set_tolerance(tol)
+        st = s.bicgstab(20000)
+        assert st["status"] == 0, st
+        self.iterations += st["iters"]
+        u, v, w = self._winds()
+        s.updated_winds(self.case.adv_den, u, v, w)
+        d2 = s.divergence(u, v, w, adv_den=self.case.adv_den)
+        return (s.vec("x"), (u, v, w), float(np.linalg.norm(d2.astype(np.float64))) / self.div_norm,
+                s.true_residual() / st["b_norm"])
+
+
+def _gpu_solve(dom, div, case, opts):
+    """One steady-state GPU solve from lambda = 0 of the case's input winds;
+    returns stats, lambda, (u, v, w) and the final divergence relative to the input's."""
+    from hicar_b200 import wind, wind_iterative as wi
+    h = wi.handle(dom.nest_indx)
+    wi.set_options(wi.WindOptions(**opts))
+    dom.set_winds(case.u, case.v, case.w)
+    _capi.load().hicarw_reset_solution(h, None)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    d0 = float(div.double().norm())
+    st = wi.calc_iter_winds(dom, dom.wind_alpha, div, case.adv_den)
+    lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+    _capi.check(_capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None), h)
+    winds = tuple(a.cpu().numpy().copy() for a in (dom.u_dqdt, dom.v_dqdt, dom.w_dqdt))
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    return st, lam, winds, float(div.double().norm()) / d0
+
+
+def _calibrated(case):
+    from hicar_b200 import wind, wind_iterative as wi
+    from hicar_b200.domain import DeviceDomain
+    dom = DeviceDomain.from_case(case, "cuda")
+    opt = wi.WindOptions(advect_density=case.adv_den)
+    wi.init_iter_winds(dom, opt)
+    div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    wind.update_winds_iterative(dom, opt, div)  # analytic solve, calibration, polishing solve
+    return dom, div
+
+
+def test_headline_options_match_oracle_on_mixed_generator(oracle_mod):
+    case = cases.build_case(192, 192, 40, 250.0, 20, seed=1, adv_den=True, alpha="smooth")
+    ref = OracleSolve(oracle_mod, case, "ref")
+    lam_r6, w_r6, div_r6, true_r6 = ref.solve_to(1e-6)
+    lam_r, w_r, div_r, true_r = ref.solve_to(1e-12)
+    assert true_r < 1e-11
+    f64 = OracleSolve(oracle_mod, case, "f64")
+    lam_f, w_f, div_f, _ = f64.solve_to(1e-12)
+
+    dom, div = _calibrated(case)
+    for tol in (1e-6, 1e-9):
+        st, lam, winds, div_g = _gpu_solve(dom, div, case, dict(HEADLINE, tol_rel=tol, wind_solver_iterations=3000))
+        assert st["status"] == 0 and st["precond"] == _capi.PRECOND_MG, st
+        assert 0.0 <= st["true_res"] <= 1.01 * st["target"], st
+        errs = [_rel(lam, lam_r)] + [_rel(g, r) for g, r in zip(winds, w_r)]
+        errs64 = [_rel(lam, lam_f)] + [_rel(g, r) for g, r in zip(winds, w_f)]
+        print(f"tol {tol:g}: {st['iterations']} iterations (oracle {ref.iterations}); vs reference precision "
+              f"lambda/u/v/w {errs}; vs FP64 {errs64}; final divergence {div_g:.3e} "
+              f"(oracle {div_r6:.3e} at 1e-6, {div_r:.3e} converged, FP64 {div_f:.3e})")
+        assert max(errs) < 1e-5, errs
+        assert div_g <= 1.01 * div_r6, (div_g, div_r6)
+        # FP64 statement: lambda, u, v to 1e-5; w carries the FP32 floor of the correction (1.7e-5 here)
+        assert max(errs64[:3]) < 1e-5 and errs64[3] < 5e-5, errs64
+
+
+def test_plain_bicgstab_512_matches_oracle(oracle_mod):
+    """BASELINE's plain-GPU configuration: 512x512x48, 20 hills, alpha 1, density
+    advected, the reference's method and schedule against the oracle's."""
+    case = cases.build_case(512, 512, 48, 250.0, 20, seed=1, adv_den=True, alpha="const")
+    ref = OracleSolve(oracle_mod, case, "ref")
+    lam_r6, w_r6, div_r6, true_r6 = ref.solve_to(1e-6)
+    it6 = ref.iterations
+    lam_r9, w_r9, div_r9, true_r9 = ref.solve_to(1e-9)
+
+    dom, div = _calibrated(case)
+    plain = dict(solver=_capi.SOLVER_REFERENCE, krylov_precision=_capi.KRYLOV_F64, precond=_capi.PRECOND_JACOBI,
+                 wind_solver_iterations=3000)
+    st6, lam6, winds6, div6 = _gpu_solve(dom, div, case, dict(plain, tol_rel=1e-6))
+    st9, lam9, winds9, div9 = _gpu_solve(dom, div, case, dict(plain, tol_rel=1e-9))
+    e6 = [_rel(lam6, lam_r6)] + [_rel(g, r) for g, r in zip(winds6, w_r6)]
+    e9 = [_rel(lam9, lam_r9)] + [_rel(g, r) for g, r in zip(winds9, w_r9)]
+    print(f"1e-6: GPU {st6['iterations']} / oracle {it6} iterations, lambda/u/v/w {e6}, final divergence "
+          f"{div6:.3e} / {div_r6:.3e}; 1e-9: GPU {st9['iterations']} iterations, lambda/u/v/w {e9}")
+    assert st6["status"] == 0 and st9["status"] == 0
+    assert abs(st6["iterations"] - it6) <= 0.1 * it6
+    assert max(e6[1:]) < 1e-5, e6
+    assert abs(div6 - div_r6) <= 0.01 * div_r6
+    assert max(e9) < 1e-5, e9

@@ -2,7 +2,9 @@
 callers that cannot allocate device memory (inside a stream capture, or in a
 host model whose device memory is fixed up front).  It must agree with the
 library's allocating paths on two calls in a row: the FP64 true residual the
-solve reports, and ||rhs - A x|| formed from hicarw_apply_operator.
+solve reports, and ||rhs - A x|| formed from hicarw_apply_operator, for the
+probed operator and for the analytic one (its bottom and top boundary rows
+and constant horizontal terms).
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
@@ -55,5 +57,39 @@ def test_residual_norm_noalloc_matches_allocating_paths(lib):
     ref = float(np.linalg.norm(b - y))
     torch.cuda.synchronize()
     assert abs(out.item() - ref) <= 1e-9 * ref
+    wi.finalize_iter_winds()
+    wind.reset()
+
+
+def test_residual_norm_noalloc_analytic_operator(lib):
+    """The analytic operator of the first solve (before any calibration): two
+    calls in a row against ||rhs - A x|| formed from hicarw_apply_operator."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hicar_b200 import wind, wind_iterative as wi
+    from hicar_b200.domain import DeviceDomain
+    wi.finalize_iter_winds()
+    wind.reset()
+    case = cases.build_case(37, 29, 11, seed=5, adv_den=True, n_hills=4)
+    dom = DeviceDomain.from_case(case, "cuda")
+    opt = wi.WindOptions()
+    wi.init_iter_winds(dom, opt)
+    div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    wi.calc_iter_winds(dom, dom.wind_alpha, div, True)  # builds the analytic coefficients
+    h = wi.handle(dom.nest_indx)
+    shape = (dom.ny + 2, dom.nz + 2, dom.nx + 2)
+    rng = np.random.default_rng(3)
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        x = rng.standard_normal(shape)
+        b = rng.standard_normal(shape)
+        xd, bd = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+        assert lib.hicarw_residual_norm_noalloc(h, xd.data_ptr(), bd.data_ptr(), out.data_ptr(), None) == 0
+        y = np.empty(shape)
+        assert lib.hicarw_apply_operator(h, x.ctypes.data, y.ctypes.data, _capi.MEM_HOST, None) == 0
+        ref = float(np.linalg.norm(b - y))
+        torch.cuda.synchronize()
+        assert abs(out.item() - ref) <= 1e-9 * ref, (call, out.item(), ref)
     wi.finalize_iter_winds()
     wind.reset()
