@@ -495,32 +495,46 @@ def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, opts, to
     the final divergence of the corrected winds relative to the input's.  The
     converged solution is a tight FP64 GPU solve (FGMRES + V-cycle to 1e-11)
     certified by the CPU oracle: its FP64 residual in the oracle's operator,
-    and the reference winds are the oracle's correction of that lambda."""
+    and the reference winds are the oracle's correction of that lambda.
+    Returns the report and compare(): the same differences for the solution
+    and corrected winds the handle and domain hold after any later solve of
+    the workload."""
     import torch
     from hicar_b200 import _capi
+
+    def state():
+        lam = torch.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2), dtype=torch.float64, device=div.device)
+        lib.hicarw_get_lambda(h, lam.data_ptr(), _capi.MEM_DEVICE, stream.cuda_stream)
+        winds = [a.clone() for a in (dom.u_dqdt, dom.v_dqdt, dom.w_dqdt)]
+        wind.calc_divergence(div, dom, use_dqdt=True)
+        return lam, winds, float(div.double().norm())
 
     def solve_with(opt):
         wi.set_options(opt)
         dom.set_winds(u0, v0, w0)
         lib.hicarw_reset_solution(h, stream.cuda_stream)
         wind.calc_divergence(div, dom, use_dqdt=True)
-        d0 = float(div.double().norm())
         st = wi.calc_iter_winds(dom, dom.wind_alpha, div, wl["adv_den"])
-        lam = torch.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2), dtype=torch.float64, device=div.device)
-        lib.hicarw_get_lambda(h, lam.data_ptr(), _capi.MEM_DEVICE, stream.cuda_stream)
-        winds = [a.clone() for a in (dom.u_dqdt, dom.v_dqdt, dom.w_dqdt)]
-        wind.calc_divergence(div, dom, use_dqdt=True)
-        return st, lam, winds, float(div.double().norm()) / d0
+        return (st,) + state()
 
+    dom.set_winds(u0, v0, w0)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    d0 = float(div.double().norm())
     tight = solver_options("fgmres")
     tight.tol_rel, tight.wind_solver_iterations, tight.stall_iters = 1e-11, 6000, 0
     st_t, lam_t, _, _ = solve_with(tight)
-    lam_np = lam_t.cpu().numpy()
-    res_t, w_ref, div_ref = oracle_check.certify(lam_np)
+    res_t, w_ref, div_ref = oracle_check.certify(lam_t.cpu().numpy())
     w_ref = [torch.from_numpy(a).to(div.device) for a in w_ref]
 
     def rel(a, b):
         return float((a.double() - b.double()).norm() / b.double().norm())
+
+    def errors(lam, w_a, dn):
+        return {"lambda_rel_l2": rel(lam, lam_t), "u_rel_l2": rel(w_a[0], w_ref[0]), "v_rel_l2": rel(w_a[1], w_ref[1]),
+                "w_rel_l2": rel(w_a[2], w_ref[2]), "final_div_rel": dn / d0}
+
+    def compare():
+        return errors(*state())
 
     out = {"reference_solve": "FP64 FGMRES(30) + V-cycle to 1e-11 on the GPU, certified by the CPU oracle's FP64 "
                               "residual; winds from the oracle's calc_updated_winds of that lambda",
@@ -528,16 +542,54 @@ def accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, opts, to
            "final_div_rel_reference": div_ref}
     for tol in tols:
         opt = wi.WindOptions(**{**dataclasses_asdict(opts), "tol_rel": tol})
-        st, lam, w_a, div_a = solve_with(opt)
-        out[f"{tol:g}"] = {"iterations": st["iterations"], "lambda_rel_l2": rel(lam, lam_t),
-                           "u_rel_l2": rel(w_a[0], w_ref[0]), "v_rel_l2": rel(w_a[1], w_ref[1]),
-                           "w_rel_l2": rel(w_a[2], w_ref[2]), "final_div_rel": div_a}
-    return out
+        st, lam, w_a, dn = solve_with(opt)
+        out[f"{tol:g}"] = {"iterations": st["iterations"], **errors(lam, w_a, dn)}
+    return out, compare
 
 
 def dataclasses_asdict(opt) -> dict:
     import dataclasses
     return {f.name: getattr(opt, f.name) for f in dataclasses.fields(opt)}
+
+
+def learned_report(lib, wi, dom, h, step, stream, tols, plain_ms, accuracy_solve=None):
+    """The learned+mixed solver on the workload: FGMRES(30) with the composite
+    preconditioner z = M(r) + U(r - A M(r)) (the benchmark's V-cycle, then the
+    U-Net trained on solver-logged pairs of 128x128x32 terrains, BF16 tensor-core
+    convolutions), against the same outer loop with the V-cycle alone (the
+    method without the network).  For each tolerance: solves/s of 3 timed
+    solves (after one untimed), iterations, and the speed-up over the plain GPU
+    BiCGStab.  None when no trained parameters are shipped."""
+    import torch
+    from hicar_b200 import _capi, learned as L
+    from hicar_b200.train_unet import COMPOSITE_WEIGHTS, load_params
+    if not os.path.exists(COMPOSITE_WEIGHTS):
+        return None
+    net = L.UNet(dom.nx, dom.ny, dom.nz)
+    net.set_params(torch.from_numpy(load_params(COMPOSITE_WEIGHTS)))
+    net.attach(h)
+    out = {"weights": os.path.relpath(COMPOSITE_WEIGHTS, ROOT)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for tol in tols:
+        for tag, pre in (("learned", _capi.PRECOND_MG_LEARNED), ("fgmres_mg", _capi.PRECOND_MG)):
+            wi.set_options(wi.WindOptions(tol_rel=tol, wind_solver_iterations=3000, solver=_capi.SOLVER_FGMRES,
+                                          precond=pre, fgmres_restart=30, stall_iters=200, **L.MG_CYCLE))
+            step()
+            torch.cuda.synchronize()
+            e0.record()
+            sts = [step() for _ in range(3)]
+            e1.record()
+            torch.cuda.synchronize()
+            v = 3.0 / (e0.elapsed_time(e1) / 1000.0)
+            key = f"{tag}_{tol:g}"
+            out[key] = {"solves_per_s": v, "iterations": sts[0]["iterations"], "status": sts[0]["status"],
+                        "precond": sts[0]["precond"], "true_res_rel": sts[0]["true_res"] / sts[0]["b_norm"],
+                        "speedup_vs_plain_gpu": v / (1000.0 / plain_ms)}
+            if accuracy_solve is not None and tag == "learned":
+                out[key].update(accuracy_solve())
+    lib.hicarw_set_learned_precond(h, None)
+    net.close()
+    return out
 
 
 def run_ours(args, wl):
@@ -700,9 +752,17 @@ def run_ours(args, wl):
         coefs = np.empty((15, dom.ny, dom.nz, dom.nx), np.float32)
         lib.hicarw_get_coefs(h, coefs.ctypes.data, _capi.MEM_HOST, stream.cuda_stream)
         ocheck = OracleCheck(case, coefs)
+    compare = None
     if ocheck is not None and not args.no_accuracy:
         tols = [TOL] + ([args.parity_tol] if par else [])
-        accuracy = accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, opt, tols, ocheck)
+        accuracy, compare = accuracy_report(lib, wi, wind, dom, h, div, u0, v0, w0, wl, stream, opt, tols, ocheck)
+        wi.set_options(opt)
+
+    # ---- the learned+mixed solver (FGMRES + V-cycle + U-Net correction) against FGMRES + V-cycle ----
+    learned = None
+    if world == 1 and not args.no_learned and args.solver == "mg":
+        learned = learned_report(lib, wi, dom, h, step, stream, [TOL] + ([args.parity_tol] if par else []), plain_ms,
+                                 compare)
         wi.set_options(opt)
 
     cpu = None
@@ -726,6 +786,16 @@ def run_ours(args, wl):
                     acc_keys[tag + k] = a_[k]
         acc_keys["final_div_rel_converged"] = accuracy["final_div_rel_reference"]
         acc_keys["converged_oracle_true_res_rel"] = accuracy["reference_oracle_true_res_rel"]
+    if learned:
+        for tag, tol in (("", TOL), ("parity_", args.parity_tol)):
+            for name in ("learned", "fgmres_mg"):
+                r_ = learned.get(f"{name}_{tol:g}")
+                if r_:
+                    acc_keys[f"{tag}{name}_solves_per_s"] = r_["solves_per_s"]
+                    acc_keys[f"{tag}{name}_iterations"] = r_["iterations"]
+                    acc_keys[f"{tag}{name}_speedup_vs_plain_gpu"] = r_["speedup_vs_plain_gpu"]
+                    if "lambda_rel_l2" in r_:
+                        acc_keys[f"{tag}{name}_lambda_rel_l2"] = r_["lambda_rel_l2"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if opt.krylov_precision == 0 else "f32+f64", "data": "synthetic",
@@ -741,7 +811,7 @@ def run_ours(args, wl):
                        "parity_tol_iterations": par["iterations"] if par else None,
                        "parity_tol_speedup_vs_plain_gpu": (par["solves_per_s"] / world / (1000.0 / plain_ms)
                                                            if par else None),
-                       "accuracy": accuracy,
+                       "accuracy": accuracy, "learned_fgmres": learned,
                        "l2": "inputs larger than L2 (15 FP32 coefficient arrays, %.2f GB)"
                              % (15 * 4 * (dom.nx + 2) * (dom.ny + 2) * (dom.nz + 2) / 1e9),
                        "parallelism": f"{world} independent subdomains" if world > 1 else "1 GPU"},
@@ -925,6 +995,8 @@ def main():
                     help="iterations of the reference method on the workload (reference arm)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baselines")
     ap.add_argument("--no-cpu-c1", action="store_true", help="skip the full CPU solve of the 64x64x20 case")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned+mixed FGMRES report (run only when trained parameters are shipped)")
     ap.add_argument("--parity-tol", type=float, default=1e-9,
                     help="also time the solve at this tolerance and report its accuracy (0: off)")
     ap.add_argument("--ncu-range", default="none", choices=["none", "step", "profile"],

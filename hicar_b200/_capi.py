@@ -18,7 +18,7 @@ MEM_DEVICE, MEM_HOST = 0, 1
 KRYLOV_F64, KRYLOV_F32, KRYLOV_F32_X64 = 0, 1, 2
 SOLVER_REFERENCE, SOLVER_FUSED, SOLVER_MIXED, SOLVER_FGMRES = 0, 1, 2, 3
 CRIT_RECURRENCE, CRIT_TRUE = 0, 1
-PRECOND_JACOBI, PRECOND_MG, PRECOND_LEARNED = 0, 1, 2
+PRECOND_JACOBI, PRECOND_MG, PRECOND_LEARNED, PRECOND_MG_LEARNED = 0, 1, 2, 3
 
 # Every exported symbol of include/hicarw.h (checked by the CPU test suite).
 EXPORTS = [

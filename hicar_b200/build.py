@@ -20,7 +20,6 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 UNITS = {
     "k_model.cu": ["-fmad=false"],
     "k_krylov.cu": [],
-    "k_fused.cu": [],
     "k_mg.cu": [],
     "k_noalloc.cu": [],
     "k_fgmres.cu": [],

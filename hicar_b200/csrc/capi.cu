@@ -3,7 +3,7 @@
 // wind.F90:1010-1099) and the device-driven BiCGStab loop.
 //
 // The loop: one CUDA graph holds `check_every` BiCGStab iterations (the kernel
-// schedule of k_krylov.cu, or the fused schedule of k_fused.cu).  The host
+// schedule of k_krylov.cu).  The host
 // replays it and, one graph behind, reads the device-side `stop` flag through
 // pinned memory, so the GPU never waits for the host inside a solve.  Kernels
 // of an ended solve return immediately.
@@ -21,7 +21,6 @@
 #include "../../include/hicarw.h"
 #include "common.cuh"
 #include "kernels.h"
-#include "fused.h"
 #include "mg.h"
 #include "fgmres.h"
 #include "unet.h"
@@ -124,7 +123,6 @@ struct hicarw_handle {
     float *swork = nullptr; // cell-sized scratch of balance_uvw (divergence) and smooth_alpha (ping-pong)
     int structure_uploaded = 0, operator_probed = 0, precond_n_sweeps = 2;
     std::map<GraphKey, GraphRec> graphs;
-    FusedBufs fb;
     Mg mg;
     GmresState *gst = nullptr;      // FGMRES device state
     GmresState *fg_host = nullptr;  // pinned copy of its scalar head
@@ -138,6 +136,7 @@ struct hicarw_handle {
     hicarw_unet *unet = nullptr; // learned preconditioner (not owned)
     int unet_dirty = 1;   // coefficients changed since the network's operator features were computed
     int use_learned = 0;  // the current solve applies the learned preconditioner
+    int use_mglearned = 0; // ... the V-cycle followed by the learned correction of its residual
     int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
     long long launches_at_call = 0;
@@ -249,12 +248,11 @@ static T *V(hicarw_handle *h, int q) { return (T *)h->vec[q]; }
 static bool x64(const hicarw_handle *h) { return h->vprec != HICARW_KRYLOV_F32; }
 
 // Krylov vector precision of the configured solve: the reference schedule takes
-// the option, FGMRES is FP64, the FP32 schedules are FP32.
+// the option, FGMRES is FP64.
 static int solve_precision(const hicarw_handle *h)
 {
     if (h->opt.solver == HICARW_SOLVER_REFERENCE) return h->opt.krylov_precision;
-    if (h->opt.solver == HICARW_SOLVER_FGMRES) return HICARW_KRYLOV_F64;
-    return HICARW_KRYLOV_F32;
+    return HICARW_KRYLOV_F64;
 }
 
 // Stage a caller array to the device when it lives in host memory.
@@ -268,12 +266,33 @@ static int stage_in(hicarw_handle *h, const float *src, float **buf, size_t n, i
     return 0;
 }
 
+// Options as the solve uses them.  HICARW_SOLVER_MIXED names the reference
+// schedule with FP32 Krylov vectors, FP64 reductions and FP64 lambda, periodic
+// FP64 residual replacement and the FP64 true-residual stop; the fused FP32
+// schedule (HICARW_SOLVER_FUSED) no longer exists.
+static int normalize_options(hicarw_options *o)
+{
+    if (o->krylov_precision < HICARW_KRYLOV_F64 || o->krylov_precision > HICARW_KRYLOV_F32_X64) return HICARW_ERR_ARG;
+    if (o->solver == HICARW_SOLVER_FUSED) return HICARW_ERR_ARG;
+    if (o->solver == HICARW_SOLVER_MIXED) {
+        o->solver = HICARW_SOLVER_REFERENCE;
+        o->krylov_precision = HICARW_KRYLOV_F32_X64;
+        o->criterion = HICARW_CRIT_TRUE;
+    }
+    if (o->solver != HICARW_SOLVER_REFERENCE && o->solver != HICARW_SOLVER_FGMRES) return HICARW_ERR_ARG;
+    if (o->check_every <= 0) o->check_every = 8;
+    if (o->replace_every <= 0) o->replace_every = 50;
+    return 0;
+}
+
 extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options *opt, const hicarw_metrics *m,
                                       int mem_kind, void *stream, hicarw_handle **out)
 {
     if (!g || !m || !out || g->nx < 3 || g->ny < 3 || g->nz < 2 || !(g->dx > 0.0f)) return HICARW_ERR_ARG;
-    if (opt && (opt->krylov_precision < HICARW_KRYLOV_F64 || opt->krylov_precision > HICARW_KRYLOV_F32_X64))
-        return HICARW_ERR_ARG;
+    hicarw_options o0;
+    if (opt) o0 = *opt;
+    else hicarw_default_options(&o0);
+    if (normalize_options(&o0) != 0) return HICARW_ERR_ARG;
     hicarw_handle *h = new hicarw_handle();
     Dims &d = h->d;
     d.nx = g->nx; d.ny = g->ny; d.nz = g->nz;
@@ -283,10 +302,7 @@ extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options
     d.npad = d.plane * d.my;
     d.dx = g->dx;
     h->nest = g->nest;
-    if (opt) h->opt = *opt;
-    else hicarw_default_options(&h->opt);
-    if (h->opt.check_every <= 0) h->opt.check_every = 8;
-    if (h->opt.replace_every <= 0) h->opt.replace_every = 50;
+    h->opt = o0;
     cudaStream_t s = (cudaStream_t)stream;
     int rc = 0;
 #define ALLOC(p, n) do { cudaError_t e_ = dalloc((void **)&(p), (n)); if (e_ != cudaSuccess) { set_err(h, "cudaMalloc", e_); hicarw_finalize_iter_winds(h); return HICARW_ERR_CUDA; } } while (0)
@@ -347,7 +363,6 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     cudaDeviceSynchronize();
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
-    fused_free(h->fb);
     mg_free(h->mg);
     if (h->gst) cudaFree(h->gst);
     if (h->fg_host) cudaFreeHost(h->fg_host);
@@ -376,11 +391,10 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
 
 extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
 {
-    if (!h || !opt || opt->krylov_precision < HICARW_KRYLOV_F64 || opt->krylov_precision > HICARW_KRYLOV_F32_X64)
-        return HICARW_ERR_ARG;
-    h->opt = *opt;
-    if (h->opt.check_every <= 0) h->opt.check_every = 8;
-    if (h->opt.replace_every <= 0) h->opt.replace_every = 50;
+    if (!h || !opt) return HICARW_ERR_ARG;
+    hicarw_options o = *opt;
+    if (normalize_options(&o) != 0) return HICARW_ERR_ARG;
+    h->opt = o;
     if (h->opt.max_iters + 2 > h->hist_cap) {
         cudaFree(h->hist);
         h->hist_cap = h->opt.max_iters + 2;
@@ -455,18 +469,38 @@ static void enqueue_iteration_prec(hicarw_handle *h, int prec, int sweeps, cudaS
     else enqueue_iteration<float, float>(h, V<float>(h, V_X), sweeps, s);
 }
 
-// The set-up kernel (r = b - A x, r^ = p = r and the first dots) in the vector precision prec.
-static void enqueue_setup_prec(hicarw_handle *h, int prec, const OpCtx &c, const RedBuf &rb, cudaStream_t s)
+// The set-up kernel (r = b - A x, r^ = p = r and the first dots) in the vector
+// precision prec; restart != 0 keeps the iteration count and the target.
+static void enqueue_setup_prec(hicarw_handle *h, int prec, const OpCtx &c, const RedBuf &rb, cudaStream_t s,
+                               int restart)
 {
     if (prec == HICARW_KRYLOV_F64)
         launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
-                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, restart, s);
     else if (prec == HICARW_KRYLOV_F32_X64)
         launch_setup<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
-                                    V<float>(h, V_P), h->st, h->hist, rb, s);
+                                    V<float>(h, V_P), h->st, h->hist, rb, restart, s);
     else
         launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
-                                   V<float>(h, V_P), h->st, h->hist, rb, s);
+                                   V<float>(h, V_P), h->st, h->hist, rb, restart, s);
+}
+
+// FP64 true residual of the current solution in the vector precision prec:
+// mode 0 the norm only (-> true_res), 1 residual replacement (r = b - A x and
+// rho = <r^, r>; nothing once the solve has stopped).
+static void enqueue_true_residual_prec(hicarw_handle *h, int prec, int mode, cudaStream_t s)
+{
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    if (prec == HICARW_KRYLOV_F64)
+        launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), mode ? V<double>(h, V_R) : nullptr,
+                                             mode ? V<double>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
+    else if (prec == HICARW_KRYLOV_F32_X64)
+        launch_true_residual<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), mode ? V<float>(h, V_R) : nullptr,
+                                            mode ? V<float>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
+    else
+        launch_true_residual<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), mode ? V<float>(h, V_R) : nullptr,
+                                           mode ? V<float>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
 }
 
 static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec **out)
@@ -478,14 +512,7 @@ static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec
     g_capturing = 1;
     g_capture_nodes = 0;
     CK(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-    for (int q = 0; q < chunk; q++) {
-        if (h->opt.solver == HICARW_SOLVER_REFERENCE) {
-            enqueue_iteration_prec(h, prec, sweeps, h->cap);
-        } else {
-            FusedCtx fc = fused_ctx(h);
-            fused_enqueue_iteration(fc, sweeps, h->opt.solver == HICARW_SOLVER_MIXED, h->cap);
-        }
-    }
+    for (int q = 0; q < chunk; q++) enqueue_iteration_prec(h, prec, sweeps, h->cap);
     cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
     g_capturing = 0;
     if (e != cudaSuccess) { set_err(h, "cudaStreamEndCapture", e); return HICARW_ERR_CUDA; }
@@ -508,10 +535,14 @@ static int run_loop(hicarw_handle *h, int prec, int sweeps, cudaStream_t s)
     int rc = get_graph(h, prec, sweeps, chunk, &g);
     if (rc) return rc;
     const int max_chunks = (h->opt.max_iters + chunk - 1) / chunk + 2;
+    // FP32 Krylov vectors: the recurrence residual is replaced by the FP64 true
+    // residual of the FP64 solution every replace_every iterations (rounded to graphs)
+    const int rep = prec != HICARW_KRYLOV_F64 && h->opt.replace_every > 0 ? std::max(1, h->opt.replace_every / chunk) : 0;
     h->hflag[0] = h->hflag[1] = 0;
     for (int n = 0; n < max_chunks; n++) {
         CK(cudaGraphLaunch(g->exec, s));
         g_launches += g->nodes;
+        if (rep && (n + 1) % rep == 0) enqueue_true_residual_prec(h, prec, 1, s);
         CK(cudaMemcpyAsync(&h->hflag[n & 1], &h->st->stop, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaEventRecord(h->ev[n & 1], s));
         if (n >= 1) {
@@ -537,13 +568,30 @@ static int fetch_state(hicarw_handle *h, cudaStream_t s)
 // bicgstab_solve (:555-791) on the current x / rhs.  Fills st (pinned mirror).
 static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s);
 
+// Preconditioner of a solve: the V-cycle (HICARW_PRECOND_MG, and the first
+// stage of HICARW_PRECOND_MG_LEARNED), the U-Net alone (HICARW_PRECOND_LEARNED),
+// or the V-cycle followed by the U-Net's correction of the residual it leaves
+// (HICARW_PRECOND_MG_LEARNED); the forms with the U-Net run inside FGMRES only,
+// and all but Jacobi need the probed operator.
+static void select_precond(hicarw_handle *h, int allow)
+{
+    const int p = h->opt.precond;
+    const bool fg = h->opt.solver == HICARW_SOLVER_FGMRES, ok = allow && h->operator_probed;
+    h->use_mglearned = ok && fg && p == HICARW_PRECOND_MG_LEARNED && h->unet != nullptr;
+    h->use_mg = ok && (p == HICARW_PRECOND_MG || h->use_mglearned);
+    h->use_learned = ok && fg && p == HICARW_PRECOND_LEARNED && h->unet != nullptr;
+}
+static int precond_kind(const hicarw_handle *h)
+{
+    return h->use_mglearned ? HICARW_PRECOND_MG_LEARNED
+                            : h->use_learned ? HICARW_PRECOND_LEARNED
+                                             : h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI;
+}
+
 static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allow_mg = 1)
 {
     int rc;
-    h->use_mg = allow_mg && h->opt.precond == HICARW_PRECOND_MG && h->operator_probed &&
-                (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES);
-    h->use_learned = allow_mg && h->opt.precond == HICARW_PRECOND_LEARNED && h->operator_probed &&
-                     h->opt.solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
+    select_precond(h, allow_mg);
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         mg_params(h);
         if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
@@ -559,44 +607,28 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters,
                        h->use_mg ? h->opt.stall_iters : 0, s);
     CK(cudaEventRecord(h->t0, s));
-    if (solver == HICARW_SOLVER_REFERENCE) {
-        enqueue_setup_prec(h, prec, c, rb, s);
-        rc = run_loop(h, prec, sweeps, s);
-        if (rc) return rc;
-    } else {
-        if ((rc = fused_prepare(h->fb, h->d, s)) != 0) { h->err = "fused buffers"; return HICARW_ERR_CUDA; }
-        FusedCtx fc = fused_ctx(h);
-        fused_setup(fc, solver == HICARW_SOLVER_MIXED, s);
-        rc = run_loop(h, prec, sweeps, s);
-        if (rc) return rc;
-        // true-residual stopping rule: restart from the FP64 solution while the
-        // FP64 residual is above target (MIXED only; the iterate is in x64)
-        if (solver == HICARW_SOLVER_MIXED && h->opt.criterion == HICARW_CRIT_TRUE) {
-            for (int rs = 0; rs < 20; rs++) {
-                if ((rc = fetch_state(h, s)) != 0) return rc;
-                if (h->hst->status != 0) break;
-                fused_true_residual(fc, 0, s);
-                if ((rc = fetch_state(h, s)) != 0) return rc;
-                if (h->hst->true_res <= h->hst->target || h->hst->it >= h->opt.max_iters) break;
-                fused_restart(fc, s);
-                rc = run_loop(h, prec, sweeps, s);
-                if (rc) return rc;
-            }
+    (void)solver;
+    enqueue_setup_prec(h, prec, c, rb, s, 0);
+    rc = run_loop(h, prec, sweeps, s);
+    if (rc) return rc;
+    // true-residual stopping rule (iterative refinement of lambda): while the
+    // FP64 residual of the FP64 solution is above the target, restart the
+    // recurrences from it (r = r^ = p = b - A x) and continue
+    if (h->opt.criterion == HICARW_CRIT_TRUE) {
+        for (int rs = 0; rs < 20; rs++) {
+            if ((rc = fetch_state(h, s)) != 0) return rc;
+            if (h->hst->status != 0) break;
+            enqueue_true_residual_prec(h, prec, 0, s);
+            if ((rc = fetch_state(h, s)) != 0) return rc;
+            if (h->hst->true_res <= h->hst->target || h->hst->it >= h->opt.max_iters) break;
+            enqueue_setup_prec(h, prec, c, rb, s, 1);
+            rc = run_loop(h, prec, sweeps, s);
+            if (rc) return rc;
         }
     }
     CK(cudaEventRecord(h->t1, s));
     // final FP64 true residual of the solution (diagnostic; reference has none)
-    if (solver == HICARW_SOLVER_REFERENCE) {
-        if (prec == HICARW_KRYLOV_F64)
-            launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
-        else if (prec == HICARW_KRYLOV_F32_X64)
-            launch_true_residual<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
-        else
-            launch_true_residual<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), nullptr, nullptr, h->st, 0, rb, s);
-    } else {
-        FusedCtx fc = fused_ctx(h);
-        fused_true_residual(fc, 0, s);
-    }
+    enqueue_true_residual_prec(h, prec, 0, s);
     return fetch_state(h, s);
 }
 
@@ -607,11 +639,51 @@ int unet_precond(hicarw_unet *n, const OpCtx &c, const double *in, double *out, 
 bool unet_matches(const hicarw_unet *n, const Dims &d);
 }  // namespace hw
 
+// z = M(r) + U(r - A M(r)): the V-cycle, then the U-Net's estimate of the error
+// left in its residual (V_T and V_PRES are free during FGMRES: they hold A M(r)
+// and the residual left by the V-cycle).
+__global__ void mgl_residual_kernel(long long n, const double *__restrict__ r, double *__restrict__ az,
+                                    double *__restrict__ res, const SolveState *gate)
+{
+    if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        res[q] = r[q] - az[q];
+        az[q] = 0.0; // the U-Net writes the interior of its output only
+    }
+}
+
+__global__ void mgl_add_kernel(long long n, const double *__restrict__ u, double *__restrict__ z, const SolveState *gate)
+{
+    if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        z[q] += u[q];
+}
+
+static void mg_learned_apply(hicarw_handle *h, const double *in, double *out, const SolveState *gate, cudaStream_t s)
+{
+    const OpCtx c = opctx(h);
+    const long long n = h->d.npad;
+    const int g = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    double *az = V<double>(h, V_T), *res = V<double>(h, V_PRES);
+    mg_apply<double>(h->mg, in, out, gate, s);
+    launch_spmv<double>(c, out, az, gate, s);
+    {
+        ProfScope ps_("mgl_residual", (double)n * 32.0, s);
+        mgl_residual_kernel<<<g, 256, 0, s>>>(n, in, az, res, gate);
+        count_launch(1);
+    }
+    unet_precond(h->unet, c, res, az, gate, s);
+    ProfScope ps_("mgl_add", (double)n * 24.0, s);
+    mgl_add_kernel<<<g, 256, 0, s>>>(n, az, out, gate);
+    count_launch(1);
+}
+
 static void fgmres_precond_cb(void *ctx, const double *in, double *out, cudaStream_t s)
 {
     auto *pc = (decltype(hicarw_handle::fg_pc) *)ctx;
     hicarw_handle *h = pc->h;
-    if (h->use_learned) unet_precond(h->unet, opctx(h), in, out, h->st, s);
+    if (h->use_mglearned) mg_learned_apply(h, in, out, h->st, s);
+    else if (h->use_learned) unet_precond(h->unet, opctx(h), in, out, h->st, s);
     else if (h->use_mg) mg_apply<double>(h->mg, in, out, h->st, s);
     else enqueue_precond<double>(h, in, out, pc->sweeps, h->st, 0, s);
 }
@@ -672,7 +744,7 @@ static int fgmres_ready(hicarw_handle *h, int sweeps, cudaStream_t s, FgmresCtx 
 {
     int rc = fgmres_prepare(h, sweeps, f);
     if (rc) return rc;
-    if (h->use_learned && h->unet_dirty) {
+    if ((h->use_learned || h->use_mglearned) && h->unet_dirty) {
         if (unet_prepare_operator(h->unet, opctx(h), s) != 0) {
             h->err = "learned preconditioner grid mismatch";
             return HICARW_ERR_ARG;
@@ -712,7 +784,7 @@ static int fgmres_solve(hicarw_handle *h, int sweeps, cudaStream_t s)
     fgmres_reset(h->gst, m, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, h->hist, h->st, s);
     CK(cudaEventRecord(h->t0, s));
     // one restart cycle = one graph
-    const int pkind = h->use_learned ? HICARW_PRECOND_LEARNED : (h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI);
+    const int pkind = precond_kind(h);
     GraphKey key{HICARW_KRYLOV_F64, sweeps, m, HICARW_SOLVER_FGMRES, 0, pkind};
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
@@ -769,7 +841,7 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
     o->target = st->target;
     o->true_res = st->true_res;
     o->replacements = st->replacements;
-    o->precond = h->use_learned ? HICARW_PRECOND_LEARNED : (h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI);
+    o->precond = precond_kind(h);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, h->t0, h->t1);
     o->solve_ms = ms;
@@ -780,14 +852,8 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
 static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float *u, float *v, float *w, cudaStream_t s)
 {
     Metrics m = metrics_of(h);
-    if (h->opt.solver == HICARW_SOLVER_REFERENCE || h->opt.solver == HICARW_SOLVER_FGMRES) {
-        if (x64(h)) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
-        else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
-    } else {
-        FusedCtx fc = fused_ctx(h);
-        if (h->opt.solver == HICARW_SOLVER_MIXED) launch_winds<double>(h->d, m, fc.x64, h->alpha, rho, u, v, w, adv_den, s);
-        else launch_winds<float>(h->d, m, fc.x, h->alpha, rho, u, v, w, adv_den, s);
-    }
+    if (x64(h)) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
+    else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
     return 0;
 }
 
@@ -795,7 +861,6 @@ static int zero_solution(hicarw_handle *h, cudaStream_t s)
 {
     size_t es = x64(h) ? 8 : 4;
     CK(cudaMemsetAsync(h->vec[V_X], 0, (size_t)h->d.npad * es, s));
-    if (h->fb.ready) CK(cudaMemsetAsync(h->fb.x64, 0, (size_t)h->d.npad * 8, s));
     return 0;
 }
 
@@ -1086,8 +1151,7 @@ extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind,
     CK(cudaMalloc((void **)&conv, (size_t)d.npad * 8));
     CK(cudaMalloc((void **)&gath, n * 8));
     const double *src64 = nullptr;
-    if (h->opt.solver == HICARW_SOLVER_MIXED && h->fb.ready) src64 = h->fb.x64;
-    else if (x64(h)) src64 = V<double>(h, V_X);
+    if (x64(h)) src64 = V<double>(h, V_X);
     else {
         launch_convert<float, double>(d.npad, V<float>(h, V_X), conv, s);
         src64 = conv;
@@ -1185,20 +1249,31 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
     if (sweeps <= 0 && !h->operator_probed) return HICARW_ERR_STATE; // the V-cycle needs the probed operator
+    const bool learned = sweeps < 0 && (h->opt.precond == HICARW_PRECOND_LEARNED ||
+                                        h->opt.precond == HICARW_PRECOND_MG_LEARNED);
+    if (learned && !h->unet) return HICARW_ERR_STATE;
     double *bx, *by, *bd, *bp;
     CK(dalloc((void **)&bx, (size_t)d.npad * 8));
     CK(dalloc((void **)&by, (size_t)d.npad * 8));
     CK(dalloc((void **)&bd, (size_t)d.npad * 8));
     CK(dalloc((void **)&bp, (size_t)d.npad * 8));
     int rc = put_padded(h, x, bx, mem_kind, s);
+    if (!rc && learned) rc = ensure_vectors(h, HICARW_KRYLOV_F64); // scratch of the composite
+    if (!rc && learned && h->unet_dirty) {
+        if (unet_prepare_operator(h->unet, opctx(h), s) != 0) rc = HICARW_ERR_ARG;
+        else h->unet_dirty = 0;
+    }
     if (!rc && sweeps <= 0) {
-        if (h->mg_dirty || !h->mg.ready) {
+        if ((h->mg_dirty || !h->mg.ready) && !(learned && h->opt.precond == HICARW_PRECOND_LEARNED)) {
             mg_params(h);
             if (mg_build(h->mg, d, h->coef, s) != 0) rc = HICARW_ERR_CUDA;
             else h->mg_dirty = 0;
         }
         if (!rc) {
-            mg_apply<double>(h->mg, bx, by, nullptr, s);
+            CK(cudaMemsetAsync(by, 0, (size_t)d.npad * 8, s));
+            if (learned && h->opt.precond == HICARW_PRECOND_LEARNED) unet_precond(h->unet, opctx(h), bx, by, nullptr, s);
+            else if (learned) mg_learned_apply(h, bx, by, nullptr, s);
+            else mg_apply<double>(h->mg, bx, by, nullptr, s);
             rc = get_padded(h, by, y, mem_kind, s);
         }
         int herr = 0;
@@ -1285,12 +1360,8 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     const int prec = solve_precision(h);
     int rc = ensure_vectors(h, prec);
     if (rc) return rc;
-    const int fused = solver == HICARW_SOLVER_FUSED || solver == HICARW_SOLVER_MIXED;
-    if (fused && (rc = fused_prepare(h->fb, h->d, s)) != 0) return HICARW_ERR_CUDA;
-    h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed && !fused;
-    h->use_learned = h->opt.precond == HICARW_PRECOND_LEARNED && h->operator_probed &&
-                     solver == HICARW_SOLVER_FGMRES && h->unet != nullptr;
-    if (h->use_learned && h->unet_dirty) {
+    select_precond(h, 1);
+    if ((h->use_learned || h->use_mglearned) && h->unet_dirty) {
         if (unet_prepare_operator(h->unet, opctx(h), s) != 0) return HICARW_ERR_ARG;
         h->unet_dirty = 0;
     }
@@ -1311,7 +1382,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         RedBuf rb{h->partials, h->red_blocks};
         if ((rc = zero_solution(h, s)) != 0) return rc;
         launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, 0, s);
-        enqueue_setup_prec(h, prec, c, rb, s);
+        enqueue_setup_prec(h, prec, c, rb, s, 0);
     }
     prof_state_kernel<<<1, 1, 0, s>>>(h->st, 1);
     CK(cudaStreamSynchronize(s));
@@ -1321,11 +1392,8 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
     for (int q = 0; q < reps; q++) {
         if (solver == HICARW_SOLVER_FGMRES) {
             fgmres_enqueue_cycle(fg, s);
-        } else if (solver == HICARW_SOLVER_REFERENCE) {
-            enqueue_iteration_prec(h, prec, h->precond_n_sweeps, s);
         } else {
-            FusedCtx fc = fused_ctx(h);
-            fused_enqueue_iteration(fc, h->precond_n_sweeps, solver == HICARW_SOLVER_MIXED, s);
+            enqueue_iteration_prec(h, prec, h->precond_n_sweeps, s);
         }
     }
     g_prof_on = 0;
@@ -1553,7 +1621,7 @@ static void batch_enqueue_setup(hicarw_batch *b, int i, const hicarw_batch_item 
         OpCtx c = opctx(h);
         RedBuf rb{h->partials, h->red_blocks};
         launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
-                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, s);
+                                     V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, 0, s);
     }
     batch_count_reset_kernel<<<1, 1, 0, s>>>(b->counters + i);
     count_launch(1);
@@ -1658,9 +1726,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
     for (int i = 0; i < n; i++) {
         hicarw_handle *h = b->hs[i];
         h->launches_at_call = g_launches.load();
-        h->use_mg = h->opt.precond == HICARW_PRECOND_MG && h->operator_probed;
-        h->use_learned = h->opt.solver == HICARW_SOLVER_FGMRES && h->opt.precond == HICARW_PRECOND_LEARNED &&
-                         h->operator_probed && h->unet != nullptr;
+        select_precond(h, 1);
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
             mg_params(h);
             if (mg_build(h->mg, h->d, h->coef, s) != 0) {
@@ -1671,7 +1737,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
             rebuild = true;
         }
         if (h->opt.solver == HICARW_SOLVER_FGMRES) {
-            const bool dirty = h->use_learned && h->unet_dirty;
+            const bool dirty = (h->use_learned || h->use_mglearned) && h->unet_dirty;
             FgmresCtx f;
             if ((rc = fgmres_ready(h, h->precond_n_sweeps, s, &f)) != 0) return rc;
             if (dirty || b->fg[i].V != f.V || b->fg[i].m != f.m) rebuild = true;
@@ -1856,19 +1922,3 @@ void handle_operator(const hicarw_handle *h, OpCtx *c) { *c = opctx(h); }
 void handle_set_error(hicarw_handle *h, const char *msg) { h->err = msg; }
 }  // namespace hw
 
-// ---- pieces shared with the fused schedule ----
-FusedCtx fused_ctx(hicarw_handle *h)
-{
-    FusedCtx c;
-    c.op = opctx(h);
-    c.rb = RedBuf{h->partials, h->red_blocks};
-    c.st = h->st;
-    c.hist = h->hist;
-    c.div = h->div;
-    c.fb = &h->fb;
-    c.x64 = (h->opt.solver == HICARW_SOLVER_MIXED && h->fb.ready) ? h->fb.x64 : nullptr;
-    c.replace_every = h->opt.replace_every;
-    float **slots[] = {&c.x, &c.r, &c.rhat, &c.p, &c.phat, &c.v, &c.s, &c.shat, &c.t, &c.rhs, &c.Dinv, &c.pres};
-    for (int q = 0; q < NVEC; q++) *slots[q] = h->vprec == HICARW_KRYLOV_F32 ? (float *)h->vec[q] : nullptr;
-    return c;
-}

@@ -16,6 +16,9 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -50,47 +53,107 @@ __global__ void __launch_bounds__(ROWT) spmv_march_kernel(OpCtx c, const V *__re
     march_rows<V>(c, x, [&](long long o, double v) { y[o] = (V)v; });
 }
 
-// Column-marching operator kernels for the probed operator when the
-// environment sets HICARW_SPMV_MARCH=1 (read at every launch, so at graph
-// capture for the captured ones).
-static bool use_march(const OpCtx &c)
+// Operator kernel of a launch (read at every launch, so at graph capture for
+// the captured ones): the float4 column-marching kernels for the probed
+// operator when nx is a multiple of 4 (the default), the scalar column-marching
+// ones when the environment sets HICARW_SPMV_MARCH=1, the row kernels when it
+// sets HICARW_SPMV_MARCH=0 (and for the analytic operator).
+enum { SPMV_ROW = 0, SPMV_MARCH = 1, SPMV_MARCH4 = 2 };
+static int spmv_kind(const OpCtx &c)
 {
+    if (!c.probed) return SPMV_ROW;
     const char *e = getenv("HICARW_SPMV_MARCH");
-    return c.probed && e && e[0] == '1';
+    if (e && e[0] == '0') return SPMV_ROW;
+    if (e && e[0] == '1') return SPMV_MARCH;
+    return march4_ok(c.d) ? SPMV_MARCH4 : SPMV_ROW;
+}
+// Resident CTAs of a kernel on the whole device (its occupancy at ROWT threads),
+// looked up once per kernel.
+static int resident_ctas(const void *kernel)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, int>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto &e : cache)
+        if (e.first == kernel) return e.second;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, ROWT, 0);
+    const int n = std::max(1, sms * std::max(1, per_sm));
+    cache.emplace_back(kernel, n);
+    return n;
 }
 
-// One wave of resident CTAs (the kernel's occupancy, cached), at most `cap`.
+// One wave of resident CTAs, at most `cap` and at most one warp per work item.
+template <typename K>
+static int wave_grid(K *kernel, long long warps_needed, int cap)
+{
+    const int resident = resident_ctas((const void *)kernel);
+    const long long n = (warps_needed + MARCH_WARPS - 1) / MARCH_WARPS;
+    return (int)std::max<long long>(1, std::min<long long>(n, std::min(cap, resident)));
+}
+
 template <typename K>
 static int march_grid(K *kernel, const Dims &d, int cap)
 {
-    static int resident = 0;
-    if (!resident) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, ROWT, 0);
-        resident = std::max(1, sms * std::max(1, per_sm));
-    }
-    const long long n = (march_strips(d) + MARCH_WARPS - 1) / MARCH_WARPS;
-    return (int)std::min<long long>(n, std::min(cap, resident));
+    return wave_grid(kernel, march_strips(d), cap);
 }
+
+template <typename K>
+static int march4_grid(K *kernel, const Dims &d, int cap)
+{
+    return wave_grid(kernel, march4_items(d), cap);
+}
+
+// ---- the float4 column-marching kernels ----
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_m4_kernel(OpCtx c, const V *__restrict__ x, V *__restrict__ y,
+                                                       const SolveState *gate)
+{
+    if (gated(gate)) return;
+    march4_rows<V>(
+        c, x,
+        [&](long long o, const double (&v)[4]) {
+            V t[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) t[e] = (V)v[e];
+            st4v(y + o, t);
+        },
+        [&](long long o, double v) { y[o] = (V)v; });
+}
+
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
+                                                             const V *__restrict__ rhat, SolveState *stt,
+                                                             double *partials);
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
+                                                            const V *__restrict__ sv, const V *__restrict__ rhat,
+                                                            SolveState *stt, double *hist, double *partials);
 
 template <typename V>
 void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaStream_t st)
 {
     ProfScope ps_("spmv", coef_bytes(c.d) + rows(c.d) * 2.0 * sizeof(V), st);
-    if (use_march(c))
+    const int kind = spmv_kind(c);
+    if (kind == SPMV_MARCH4)
+        spmv_m4_kernel<V><<<march4_grid(spmv_m4_kernel<V>, c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
+    else if (kind == SPMV_MARCH)
         spmv_march_kernel<V><<<march_grid(spmv_march_kernel<V>, c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     else spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     count_launch(1);
 }
 
 // ---- setup: r = b - A x0, r^ = r, p = r, <r^,r>, <r,r>, <b,b> (:585-645) ----
-// X is the type of the solution (FP64 accumulator in the MIXED schedule).
+// X is the type of the solution (FP64 with FP32 vectors and FP64 lambda).
+// restart != 0: a restart of the recurrences from the current solution (the
+// true-residual stopping rule): the iteration count, the initial norm and the
+// target are kept, the stop flags cleared.
 template <typename V, typename X>
 __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restrict__ x, const V *__restrict__ rhs,
                                                      V *__restrict__ r, V *__restrict__ rhat, V *__restrict__ p,
-                                                     SolveState *stt, double *hist, double *partials)
+                                                     SolveState *stt, double *hist, double *partials, int restart)
 {
     double acc[3] = {0.0, 0.0, 0.0};
     const long long n = nsegs(c.d);
@@ -109,6 +172,22 @@ __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restric
     }
     double tot[3];
     if (!grid_reduce<3>(acc, partials, &stt->ticket[0], tot)) return;
+    if (threadIdx.x == 0 && restart) {
+        const double rn = sqrt(tot[1]);
+        stt->rho = tot[0];
+        stt->rnorm = rn;
+        stt->omega = 1.0;
+        stt->alpha = 1.0;
+        stt->best_rn = rn;
+        stt->best_it = stt->it;
+        stt->status = 1;
+        stt->stop = 0;
+        stt->halt = 0;
+        stt->upd_r = stt->upd_p = 0;
+        if (rn <= stt->target) { stt->status = 0; stt->stop = 1; stt->halt = 1; }
+        else if (stt->it >= stt->max_iters) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
+        return;
+    }
     if (threadIdx.x == 0) {
         stt->rho = tot[0];
         double rn = sqrt(tot[1]);
@@ -129,10 +208,10 @@ __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restric
 
 template <typename V, typename X>
 void launch_setup(const OpCtx &c, const X *x, const V *rhs, V *r, V *rhat, V *p, SolveState *stt, double *hist,
-                  const RedBuf &rb, cudaStream_t st)
+                  const RedBuf &rb, int restart, cudaStream_t st)
 {
     ProfScope ps_("setup", coef_bytes(c.d) + rows(c.d) * (sizeof(X) + 4.0 * sizeof(V)), st);
-    setup_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r, rhat, p, stt, hist, rb.partials);
+    setup_kernel<V, X><<<rb.blocks, ROWT, 0, st>>>(c, x, rhs, r, rhat, p, stt, hist, rb.partials, restart);
     count_launch(1);
 }
 
@@ -214,12 +293,45 @@ __global__ void __launch_bounds__(ROWT) spmv_sigma_march_kernel(OpCtx c, const V
     if (threadIdx.x == 0) sigma_step(stt, tot[0]);
 }
 
+// The same with float4 column-marching rows.
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
+                                                             const V *__restrict__ rhat, SolveState *stt,
+                                                             double *partials)
+{
+    if (gated(stt)) return;
+    double acc[1] = {0.0};
+    march4_rows<V>(
+        c, phat,
+        [&](long long o, const double (&y)[4]) {
+            V vv[4], rh[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) vv[e] = (V)y[e];
+            st4v(v + o, vv);
+            ld4v(rhat + o, rh);
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[0] += (double)rh[e] * (double)vv[e];
+        },
+        [&](long long o, double y) {
+            const V vv = (V)y;
+            v[o] = vv;
+            acc[0] += (double)rhat[o] * (double)vv;
+        });
+    double tot[1];
+    if (!grid_reduce<1>(acc, partials, &stt->ticket[1], tot)) return;
+    if (threadIdx.x == 0) sigma_step(stt, tot[0]);
+}
+
 template <typename V>
 void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, SolveState *stt, const RedBuf &rb,
                        cudaStream_t st)
 {
     ProfScope ps_("spmv_sigma", coef_bytes(c.d) + rows(c.d) * 3.0 * sizeof(V), st);
-    if (use_march(c))
+    const int kind = spmv_kind(c);
+    if (kind == SPMV_MARCH4)
+        spmv_sigma_m4_kernel<V><<<march4_grid(spmv_sigma_m4_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+            c, phat, v, rhat, stt, rb.partials);
+    else if (kind == SPMV_MARCH)
         spmv_sigma_march_kernel<V><<<march_grid(spmv_sigma_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
             c, phat, v, rhat, stt, rb.partials);
     else spmv_sigma_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, phat, v, rhat, stt, rb.partials);
@@ -277,12 +389,53 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_march_kernel(OpCtx c, const V 
     if (threadIdx.x == 0) dot5_step(stt, hist, tot);
 }
 
+// The same with float4 column-marching rows.
+template <typename V>
+__global__ void __launch_bounds__(ROWT) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
+                                                            const V *__restrict__ sv, const V *__restrict__ rhat,
+                                                            SolveState *stt, double *hist, double *partials)
+{
+    if (gated(stt)) return;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    auto add = [&](double td, double sd, double rd) {
+        acc[0] += td * sd;
+        acc[1] += td * td;
+        acc[2] += rd * sd;
+        acc[3] += rd * td;
+        acc[4] += sd * sd;
+    };
+    march4_rows<V>(
+        c, shat,
+        [&](long long o, const double (&y)[4]) {
+            V tv[4], s4[4], r4[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) tv[e] = (V)y[e];
+            st4v(t + o, tv);
+            ld4v(sv + o, s4);
+            ld4v(rhat + o, r4);
+#pragma unroll
+            for (int e = 0; e < 4; e++) add((double)tv[e], (double)s4[e], (double)r4[e]);
+        },
+        [&](long long o, double y) {
+            const V tv = (V)y;
+            t[o] = tv;
+            add((double)tv, (double)sv[o], (double)rhat[o]);
+        });
+    double tot[5];
+    if (!grid_reduce<5>(acc, partials, &stt->ticket[2], tot)) return;
+    if (threadIdx.x == 0) dot5_step(stt, hist, tot);
+}
+
 template <typename V>
 void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *rhat, SolveState *stt, double *hist,
                       const RedBuf &rb, cudaStream_t st)
 {
     ProfScope ps_("spmv_dot5", coef_bytes(c.d) + rows(c.d) * 4.0 * sizeof(V), st);
-    if (use_march(c))
+    const int kind = spmv_kind(c);
+    if (kind == SPMV_MARCH4)
+        spmv_dot5_m4_kernel<V><<<march4_grid(spmv_dot5_m4_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+            c, shat, t, s, rhat, stt, hist, rb.partials);
+    else if (kind == SPMV_MARCH)
         spmv_dot5_march_kernel<V><<<march_grid(spmv_dot5_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
             c, shat, t, s, rhat, stt, hist, rb.partials);
     else spmv_dot5_kernel<V><<<rb.blocks, ROWT, 0, st>>>(c, shat, t, s, rhat, stt, hist, rb.partials);
@@ -439,6 +592,7 @@ __global__ void __launch_bounds__(ROWT) true_residual_kernel(OpCtx c, const X *_
                                                              V *__restrict__ r_out, V *__restrict__ rhat,
                                                              SolveState *stt, int mode, double *partials)
 {
+    if (mode == 1 && gated(stt)) return; // a replacement after the solve has stopped changes nothing
     double acc[2] = {0.0, 0.0};
     const long long n = nsegs(c.d);
     for (long long s = blockIdx.x; s < n; s += gridDim.x) {
@@ -514,11 +668,11 @@ template void launch_update_xrp<float, double>(const Dims &, double *, const flo
                                                const float *, const float *, float *, const float *, const SolveState *,
                                                cudaStream_t);
 template void launch_setup<double, double>(const OpCtx &, const double *, const double *, double *, double *,
-                                           double *, SolveState *, double *, const RedBuf &, cudaStream_t);
+                                           double *, SolveState *, double *, const RedBuf &, int, cudaStream_t);
 template void launch_setup<float, float>(const OpCtx &, const float *, const float *, float *, float *, float *,
-                                         SolveState *, double *, const RedBuf &, cudaStream_t);
+                                         SolveState *, double *, const RedBuf &, int, cudaStream_t);
 template void launch_setup<float, double>(const OpCtx &, const double *, const float *, float *, float *, float *,
-                                          SolveState *, double *, const RedBuf &, cudaStream_t);
+                                          SolveState *, double *, const RedBuf &, int, cudaStream_t);
 template void launch_true_residual<double, double>(const OpCtx &, const double *, const double *, double *,
                                                    const double *, SolveState *, int, const RedBuf &, cudaStream_t);
 template void launch_true_residual<float, float>(const OpCtx &, const float *, const float *, float *, const float *,

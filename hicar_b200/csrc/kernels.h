@@ -70,7 +70,7 @@ void launch_rich(const Dims &d, const V *in, V *out, const V *pres, const V *Din
                  cudaStream_t st);
 template <typename V, typename X>
 void launch_setup(const OpCtx &c, const X *x, const V *rhs, V *r, V *rhat, V *p, SolveState *stt, double *hist,
-                  const RedBuf &rb, cudaStream_t st);
+                  const RedBuf &rb, int restart, cudaStream_t st);
 template <typename V>
 void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, SolveState *stt, const RedBuf &rb,
                        cudaStream_t st);

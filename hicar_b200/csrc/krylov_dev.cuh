@@ -262,3 +262,175 @@ __device__ __forceinline__ void march_rows(const OpCtx &c, const V *__restrict__
 
 
 }  // namespace hw
+
+namespace hw {
+
+// ---- float4 column-marching rows of y = A x (probed operator, nx % 4 == 0) ----
+// A lane owns four consecutive interior columns i0 .. i0+3 (i0 = 1 + 4g: a
+// 16-byte aligned group in the padded layout), a warp a strip of 128 columns
+// of one j row, and it marches k upwards over a chunk of at most M4_KC levels.
+// Every coefficient and vector row is read with one 16-byte load per lane (a
+// 512-byte segment per warp); x at k-1, k, k+1 of the own row and of the rows
+// j-1 and j+1 stays in registers (three new loads per level); the columns
+// i0-1 and i0+4 come from the neighbouring lanes by shuffles, and the lanes at
+// the ends of a strip load their outer column themselves.  Each interior row
+// sums its 15 terms in spmv_row's order, in FP64 (the same values bit for
+// bit).  Identity rows: the lateral j rows, the ghost planes, and the lateral
+// columns i = 0 and i = mx - 1 (a scalar row, done by the strip's first lane
+// and by the lane of the last group).  Work items (j, strip, level chunk) are
+// ordered j fastest, so that warps running at the same time share the x rows
+// j +- 1 through L2.  f4(o, y[4]) receives a group's four values at the
+// offset of its first element, f1(o, y) a scalar row.
+constexpr int M4_KC = 16;
+
+__device__ __forceinline__ void ld4v(const float *__restrict__ p, float (&o)[4])
+{
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+}
+__device__ __forceinline__ void ld4v(const double *__restrict__ p, double (&o)[4])
+{
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void st4v(float *__restrict__ p, const float (&v)[4])
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4v(double *__restrict__ p, const double (&v)[4])
+{
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
+}
+
+__host__ __device__ __forceinline__ bool march4_ok(const Dims &d) { return d.nx % 4 == 0 && d.nx >= 4; }
+__host__ __device__ __forceinline__ long long march4_items(const Dims &d)
+{
+    const int G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + M4_KC - 1) / M4_KC;
+    return (long long)d.my * nsx * nkc;
+}
+
+template <typename V, typename F4, typename F1>
+__device__ __forceinline__ void march4_rows(const OpCtx &c, const V *__restrict__ x, F4 &&f4, F1 &&f1)
+{
+    const Dims &d = c.d;
+    const int G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + M4_KC - 1) / M4_KC;
+    const long long items = (long long)d.my * nsx * nkc;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const long long P = d.P, PL = d.plane, N = d.npad;
+    for (long long w = (long long)blockIdx.x * wpb + wib; w < items; w += (long long)gridDim.x * wpb) {
+        const int j = (int)(w % d.my);
+        const long long rest = w / d.my;
+        const int bx = (int)(rest % nsx), kc = (int)(rest / nsx);
+        const int g = bx * 32 + lane;
+        const bool live = g < G;
+        const int k0 = kc * M4_KC, k1 = min(k0 + M4_KC, d.mz) - 1;
+        const long long ob = (long long)j * PL + 1 + XO + 4LL * g; // group start at k = 0
+        const long long oc = (long long)j * PL + XO;                // column i = 0 at k = 0
+        const bool first = live && g == 0, lastg = live && g == G - 1;
+        // lateral columns i = 0 and i = mx - 1: identity rows
+        if (first)
+            for (int k = k0; k <= k1; k++) f1(oc + k * P, (double)x[oc + k * P]);
+        if (lastg)
+            for (int k = k0; k <= k1; k++) f1(oc + (d.mx - 1) + k * P, (double)x[oc + (d.mx - 1) + k * P]);
+        if (j == 0 || j == d.my - 1) { // lateral j rows: identity (warp-uniform)
+            if (live)
+                for (int k = k0; k <= k1; k++) {
+                    V xv[4];
+                    ld4v(x + ob + k * P, xv);
+                    const double y[4] = {(double)xv[0], (double)xv[1], (double)xv[2], (double)xv[3]};
+                    f4(ob + k * P, y);
+                }
+            continue;
+        }
+        const bool west = live && lane == 0, east = live && (lane == 31 || g == G - 1);
+        // windows at k-1 (m), k (0) of the own row (c), the rows j-1 (s) and j+1 (n); the outer columns
+        V c_m[4] = {}, c_0[4] = {}, s_m[4] = {}, s_0[4] = {}, n_m[4] = {}, n_0[4] = {};
+        V w_m = 0, w_0 = 0, e_m = 0, e_0 = 0;
+        if (live) {
+            ld4v(x + ob + k0 * P, c_0);
+            ld4v(x + ob - PL + k0 * P, s_0);
+            ld4v(x + ob + PL + k0 * P, n_0);
+            if (k0 > 0) {
+                ld4v(x + ob + (k0 - 1) * P, c_m);
+                ld4v(x + ob - PL + (k0 - 1) * P, s_m);
+                ld4v(x + ob + PL + (k0 - 1) * P, n_m);
+            }
+        }
+        if (west) { w_0 = x[ob - 1 + k0 * P]; if (k0 > 0) w_m = x[ob - 1 + (k0 - 1) * P]; }
+        if (east) { e_0 = x[ob + 4 + k0 * P]; if (k0 > 0) e_m = x[ob + 4 + (k0 - 1) * P]; }
+        for (int k = k0; k <= k1; k++) {
+            const long long o = ob + k * P;
+            const bool interior = k >= 1 && k <= d.nz;
+            V c_p[4] = {}, s_p[4] = {}, n_p[4] = {};
+            V w_p = 0, e_p = 0;
+            float cf[15][4];
+            if (live && k + 1 < d.mz) {
+                ld4v(x + o + P, c_p);
+                ld4v(x + o - PL + P, s_p);
+                ld4v(x + o + PL + P, n_p);
+                if (west) w_p = x[o - 1 + P];
+                if (east) e_p = x[o + 4 + P];
+            }
+            if (live && interior) {
+#pragma unroll
+                for (int q = 0; q < 15; q++) {
+                    const float4 t = __ldg(reinterpret_cast<const float4 *>(c.coef + q * N + o));
+                    cf[q][0] = t.x; cf[q][1] = t.y; cf[q][2] = t.z; cf[q][3] = t.w;
+                }
+            }
+            // the columns i0-1 (element 0's west) and i0+4 (element 3's east) from the neighbouring lanes
+            const V lm = __shfl_up_sync(0xffffffffu, c_m[3], 1), l0 = __shfl_up_sync(0xffffffffu, c_0[3], 1),
+                    lp = __shfl_up_sync(0xffffffffu, c_p[3], 1);
+            const V rm = __shfl_down_sync(0xffffffffu, c_m[0], 1), r0 = __shfl_down_sync(0xffffffffu, c_0[0], 1),
+                    rp = __shfl_down_sync(0xffffffffu, c_p[0], 1);
+            if (live) {
+                double y[4];
+                if (!interior) {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) y[e] = (double)c_0[e];
+                } else {
+                    const V wm = west ? w_m : lm, w0 = west ? w_0 : l0, wp = west ? w_p : lp;
+                    const V em = east ? e_m : rm, e0 = east ? e_0 : r0, ep = east ? e_p : rp;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const double xwm = e > 0 ? (double)c_m[e - 1] : (double)wm;
+                        const double xw0 = e > 0 ? (double)c_0[e - 1] : (double)w0;
+                        const double xwp = e > 0 ? (double)c_p[e - 1] : (double)wp;
+                        const double xem = e < 3 ? (double)c_m[e + 1] : (double)em;
+                        const double xe0 = e < 3 ? (double)c_0[e + 1] : (double)e0;
+                        const double xep = e < 3 ? (double)c_p[e + 1] : (double)ep;
+                        // probed 15-point interior (:883-907), reference term order
+                        double v = (double)cf[CO][e] * (double)s_m[e];
+                        v += (double)cf[CG][e] * (double)s_0[e];
+                        v += (double)cf[CM][e] * (double)s_p[e];
+                        v += (double)cf[CK][e] * xwm;
+                        v += (double)cf[CC][e] * (double)c_m[e];
+                        v += (double)cf[CJ][e] * xem;
+                        v += (double)cf[CE][e] * xw0;
+                        v += (double)cf[CA][e] * (double)c_0[e];
+                        v += (double)cf[CD][e] * xe0;
+                        v += (double)cf[CI][e] * xwp;
+                        v += (double)cf[CB][e] * (double)c_p[e];
+                        v += (double)cf[CH][e] * xep;
+                        v += (double)cf[CN][e] * (double)n_m[e];
+                        v += (double)cf[CF][e] * (double)n_0[e];
+                        v += (double)cf[CL][e] * (double)n_p[e];
+                        y[e] = v;
+                    }
+                }
+                f4(o, y);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                c_m[e] = c_0[e]; c_0[e] = c_p[e];
+                s_m[e] = s_0[e]; s_0[e] = s_p[e];
+                n_m[e] = n_0[e]; n_0[e] = n_p[e];
+            }
+            w_m = w_0; w_0 = w_p;
+            e_m = e_0; e_0 = e_p;
+        }
+    }
+}
+
+}  // namespace hw

@@ -279,6 +279,114 @@ def training_pairs(case, net: UNet, n_samples: int, seed: int = 0, solve: bool =
     return out
 
 
+# The V-cycle of the composite preconditioner (V(0,1) on the finest level, omega 1,
+# W-cycles on levels 2-4): the cycle the benchmark's multigrid solves use.
+MG_CYCLE = dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4))
+
+
+def composite_pairs(case, net: UNet, ks=SOLVER_ITERS, tight_tol: float = 1e-10, cycle=None):
+    """Training samples of the composite preconditioner z = M(r) + U(r - A M(r))
+    (HICARW_PRECOND_MG_LEARNED), logged from the plain solver on one terrain:
+    the case's right-hand side b = -2 div(u, v, w) is solved once tightly
+    (FGMRES + V-cycle, x*), then the reference BiCGStab (Jacobi-Richardson) is
+    run from x = 0, its iterate x_k logged after k = ks[0], ks[1], ...
+    iterations (each leg continuing from the last iterate).  For each logged
+    iterate: r = b - A x_k and e = x* - x_k, the V-cycle's z1 = M(r), and the
+    pair the network learns, r' = r - A z1 and e' = e - z1 (A e' = r').  Returns
+    [(x0, target)]: the network's input features of r' (act layout) and its
+    supervised target e' coef_A / rms(r') (FP32 (ny, nz, nx))."""
+    torch = _torch()
+    from . import wind, wind_iterative as wi
+    cycle = MG_CYCLE if cycle is None else cycle
+    dom, h = calibrated_handle(case)
+    lib = _capi.load()
+    shape = (dom.ny + 2, dom.nz + 2, dom.nx + 2)
+    coefs = torch.empty((15, dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    _capi.check(lib.hicarw_get_coefs(h, _ptr(coefs), _capi.MEM_DEVICE, None), h)
+    diag = coefs[0].double()
+    div = torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
+    dom.set_winds(case.u, case.v, case.w)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    b = torch.zeros(shape, dtype=torch.float64, device="cuda")
+    b[1:-1, 1:-1, 1:-1] = -2.0 * div.double()  # compute_rhs_3d (wind_iterative.F90:1513-1530)
+    st = _capi.Stats()
+
+    def lam():
+        x = torch.empty(shape, dtype=torch.float64, device="cuda")
+        _capi.check(lib.hicarw_get_lambda(h, _ptr(x), _capi.MEM_DEVICE, None), h)
+        return x
+
+    def op(x):
+        y = torch.empty_like(x)
+        _capi.check(lib.hicarw_apply_operator(h, _ptr(x), _ptr(y), _capi.MEM_DEVICE, None), h)
+        return y
+
+    def interior_only(a):
+        a[0], a[-1], a[:, 0], a[:, -1], a[:, :, 0], a[:, :, -1] = 0, 0, 0, 0, 0, 0
+        return a
+
+    wi.set_options(wi.WindOptions(tol_rel=tight_tol, tol_abs=0.0, wind_solver_iterations=3000,
+                                  solver=_capi.SOLVER_FGMRES, precond=_capi.PRECOND_MG, **cycle))
+    lib.hicarw_reset_solution(h, None)
+    _capi.check(lib.hicarw_solve_rhs(h, _ptr(b), _capi.MEM_DEVICE, None, C.byref(st)), h)
+    xstar = lam()
+    lib.hicarw_reset_solution(h, None)
+    out, done = [], 0
+    for k in ks:
+        wi.set_options(wi.WindOptions(tol_rel=1e-30, tol_abs=0.0, wind_solver_iterations=k - done))
+        _capi.check(lib.hicarw_solve_rhs(h, _ptr(b), _capi.MEM_DEVICE, None, C.byref(st)), h)
+        done = k
+        xk = lam()
+        r = interior_only(b - op(xk))
+        e = interior_only(xstar - xk)
+        wi.set_options(wi.WindOptions(precond=_capi.PRECOND_MG, **cycle))
+        z1 = torch.empty_like(r)
+        _capi.check(lib.hicarw_apply_precond(h, _ptr(r), _ptr(z1), 0, _capi.MEM_DEVICE, None), h)
+        rp = interior_only(r - op(z1))
+        ep = e - z1
+        x0, rms = net.features(h, rp)
+        if not rms > 0.0:
+            continue
+        out.append((x0, (ep[1:-1, 1:-1, 1:-1] * diag / rms).float().contiguous()))
+    wi.finalize_iter_winds()
+    wind.reset()
+    return out
+
+
+def train_online(net: UNet, terrain_cases, steps_per_terrain: int = 2, batch: int = 4, lr: float = 1e-3,
+                 lr_decay_every: int = 0, buffer: int = 64, seed: int = 0, log_every: int = 0):
+    """Adam on the composite's supervised loss |O_0 - T|^2 / |T|^2 (a
+    relative error of the learned correction), with the samples of each
+    terrain (composite_pairs) added to a replay buffer of the latest `buffer`
+    samples as the terrains stream past; `steps_per_terrain` steps of `batch`
+    samples drawn from the buffer follow each terrain.  `terrain_cases` yields
+    seeded cases (never stored all at once).  Returns the loss history."""
+    import collections
+    torch = _torch()
+    gen = torch.Generator().manual_seed(seed)
+    pool = collections.deque(maxlen=buffer)
+    hist = []
+    n_terrains = 0
+    for case in terrain_cases:
+        pool.extend(composite_pairs(case, net))
+        n_terrains += 1
+        if lr_decay_every and n_terrains % lr_decay_every == 0:
+            lr *= 0.5
+        for _ in range(steps_per_terrain):
+            net.zero_grads()
+            tot = 0.0
+            for _ in range(batch):
+                x0, target = pool[int(torch.randint(0, len(pool), (1,), generator=gen))]
+                net.forward(x0)
+                tot += net.backward(target, 1.0 / max(float((target.double() ** 2).mean()), 1e-30))
+            net.adam_step(lr)
+            hist.append(tot / batch)
+        if log_every and n_terrains % log_every == 0:
+            print(f"terrain {n_terrains}: loss {sum(hist[-log_every:]) / max(1, len(hist[-log_every:])):.4f}",
+                  flush=True)
+    return hist
+
+
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, batch: int = 4, seed: int = 0, loss: str = "residual"):
     """Adam on the mean of the per-sample losses; returns the loss history.
     loss="residual": mean((A z - rhat)^2) with z = O_0 / coef_A, the preconditioned

@@ -4,6 +4,15 @@ parameters (FP32 .npy), e.g.
     python -m hicar_b200.train_unet --nx 128 --ny 128 --nz 32 --terrains 16 \\
         --samples 8 --steps 2000 --out hicar_b200/weights/unet_128x128x32.npy
 
+    python -m hicar_b200.train_unet --source composite --terrains 4096 \\
+        --out hicar_b200/weights/unet_mg_128x128x32.npy
+
+The composite source trains the second stage of HICARW_PRECOND_MG_LEARNED
+(z = M(r) + U(r - A M(r))) online: each seeded terrain's plain-solver iterates
+give (residual, error) pairs after the V-cycle (learned.composite_pairs), the
+pairs enter a replay buffer, and a few Adam steps follow each terrain, so that
+thousands of terrains stream through without being stored.
+
 Terrains are the seeded generator's cases (hicar_b200.cases, seeds
 --seed0 .. --seed0 + terrains - 1); the samples of a terrain are random
 residuals and/or the residuals of the plain solver's iterates on the terrain's
@@ -22,6 +31,7 @@ import numpy as np
 
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_128x128x32.npy")
+COMPOSITE_WEIGHTS = os.path.join(WEIGHTS_DIR, "unet_mg_128x128x32.npy")
 
 
 def load_params(path: str = DEFAULT_WEIGHTS):
@@ -43,15 +53,42 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed0", type=int, default=1000)
     ap.add_argument("--hills", type=int, default=20)
-    ap.add_argument("--source", default="random", choices=["random", "solver", "mixed"],
-                    help="residuals: random fields, the plain solver's iterates, or half of each")
-    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--source", default="random", choices=["random", "solver", "mixed", "composite"],
+                    help="residuals: random fields, the plain solver's iterates, half of each, or the "
+                         "composite preconditioner's residuals after the V-cycle (online)")
+    ap.add_argument("--steps-per-terrain", type=int, default=2, help="composite: Adam steps after each terrain")
+    ap.add_argument("--buffer", type=int, default=64, help="composite: replay buffer of samples")
+    ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
+    if args.out is None:
+        args.out = COMPOSITE_WEIGHTS if args.source == "composite" else DEFAULT_WEIGHTS
 
     import torch
 
     from . import cases, learned as L
     net = L.UNet(args.nx, args.ny, args.nz, seed=args.seed0)
+    if args.source == "composite":
+        t0 = time.time()
+        stream = (cases.build_case(args.nx, args.ny, args.nz, seed=args.seed0 + t, adv_den=True,
+                                   n_hills=args.hills) for t in range(args.terrains))
+        hist = L.train_online(net, stream, steps_per_terrain=args.steps_per_terrain, batch=args.batch, lr=args.lr,
+                              lr_decay_every=max(1, args.terrains // 4), buffer=args.buffer, seed=args.seed0,
+                              log_every=max(1, args.terrains // 16))
+        torch.cuda.synchronize()
+        p = net.params().cpu().numpy()
+        os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+        np.save(args.out, p)
+        info = {"grid": [args.nx, args.ny, args.nz], "terrains": args.terrains, "source": "composite",
+                "pairs_per_terrain": len(L.SOLVER_ITERS), "solver_iterations_logged": list(L.SOLVER_ITERS),
+                "steps": len(hist), "steps_per_terrain": args.steps_per_terrain, "batch": args.batch,
+                "buffer": args.buffer, "lr": args.lr, "seed0": args.seed0, "hills": args.hills,
+                "cycle": {k: (list(v) if isinstance(v, tuple) else v) for k, v in L.MG_CYCLE.items()},
+                "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-50:])),
+                "train_s": time.time() - t0, "params": int(p.size)}
+        with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+            json.dump(info, f, indent=1)
+        print(json.dumps(info))
+        return
     t0 = time.time()
     pairs = []
     for t in range(args.terrains):

@@ -71,10 +71,11 @@ enum {
 /* Solve schedule. */
 enum {
     HICARW_SOLVER_REFERENCE = 0, /* right-preconditioned BiCGStab, reference kernel schedule */
-    HICARW_SOLVER_FUSED = 1,     /* same method, fused FP32 kernels (temporal blocking of the
-                                    Jacobi-Richardson sweeps with the outer matvec) */
-    HICARW_SOLVER_MIXED = 2,     /* FUSED + FP64 solution accumulation and periodic FP64
-                                    true-residual replacement (iterative refinement of lambda) */
+    HICARW_SOLVER_FUSED = 1,     /* withdrawn (the fused FP32 schedule): rejected with HICARW_ERR_ARG */
+    HICARW_SOLVER_MIXED = 2,     /* shorthand: the reference schedule with HICARW_KRYLOV_F32_X64 and
+                                    HICARW_CRIT_TRUE (FP32 vectors, FP64 reductions and lambda, periodic
+                                    FP64 residual replacement, restarts until the FP64 true residual
+                                    meets the target: iterative refinement of lambda) */
     HICARW_SOLVER_FGMRES = 3     /* flexible GMRES(m), FP64 Krylov, right-preconditioned with any
                                     (also variable) preconditioner; the outer loop of the learned one */
 };
@@ -84,14 +85,17 @@ enum {
     HICARW_PRECOND_JACOBI = 0, /* the reference's Block-Jacobi / Jacobi-Richardson sweeps (:1268-1315) */
     HICARW_PRECOND_MG = 1,     /* multigrid V-cycle: z-line Jacobi smoother, 2x2 x-y aggregation,
                                   Galerkin coarse operators down to one column (probed operator only) */
-    HICARW_PRECOND_LEARNED = 2 /* the U-Net attached by hicarw_set_learned_precond (FGMRES only,
-                                  probed operator only) */
+    HICARW_PRECOND_LEARNED = 2, /* the U-Net attached by hicarw_set_learned_precond (FGMRES only,
+                                   probed operator only) */
+    HICARW_PRECOND_MG_LEARNED = 3 /* the V-cycle, then the attached U-Net's correction of the residual it
+                                     leaves: z = M(r) + U(r - A M(r)) (FGMRES only, probed operator only) */
 };
 
 /* Stopping rule. */
 enum {
     HICARW_CRIT_RECURRENCE = 0, /* ||s - w t|| <= max(tol_abs, tol_rel ||b||) (wind_iterative.F90:633,758) */
-    HICARW_CRIT_TRUE = 1        /* additionally ||b - A x|| (FP64) <= max(tol_abs, tol_rel ||b||) */
+    HICARW_CRIT_TRUE = 1        /* additionally ||b - A x|| (FP64) <= max(tol_abs, tol_rel ||b||): while it is
+                                   not, the BiCGStab recurrences restart from the current solution */
 };
 
 typedef struct hicarw_grid {
@@ -108,7 +112,9 @@ typedef struct hicarw_options {
     int krylov_precision; /* HICARW_KRYLOV_* */
     int solver;           /* HICARW_SOLVER_* */
     int criterion;        /* HICARW_CRIT_* */
-    int replace_every;    /* MIXED: FP64 true-residual replacement period (iterations) */
+    int replace_every;    /* FP32 Krylov vectors: the recurrence residual is replaced by the FP64 true
+                             residual b - A x every replace_every iterations (rounded down to a multiple
+                             of check_every; default 50) */
     int check_every;      /* iterations between host reads of the device-side stop flag */
     int precond;          /* HICARW_PRECOND_* */
     int stall_iters;      /* stop a preconditioned solve whose residual has not dropped by 1% for
@@ -144,7 +150,7 @@ typedef struct hicarw_stats {
     double b_norm;     /* ||b|| */
     double target;     /* max(tol_abs, tol_rel ||b||) */
     double true_res;   /* ||b - A x|| in FP64 at exit (negative when not computed) */
-    int replacements;  /* FP64 residual replacements (MIXED) */
+    int replacements;  /* FP64 residual replacements and restarts (FP32 Krylov vectors) */
     int launches;      /* kernels launched by this call (incl. graph nodes) */
     int precond;       /* preconditioner of the accepted solve */
     double solve_ms;   /* device time of the Krylov solve (CUDA events) */
@@ -218,8 +224,10 @@ int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed, int mem_k
 int hicarw_apply_operator(hicarw_handle *h, const double *x, double *y, int mem_kind, void *stream);
 
 /* y = M^-1 x: sweeps >= 1 applies the reference preconditioner (apply_precond,
- * wind_iterative.F90:1268-1315) with that many sweeps; sweeps <= 0 applies one
- * multigrid V-cycle (probed operator only). */
+ * wind_iterative.F90:1268-1315) with that many sweeps; sweeps == 0 applies one
+ * multigrid V-cycle (probed operator only); sweeps < 0 applies the learned
+ * preconditioner the options name (HICARW_PRECOND_LEARNED or _MG_LEARNED, with
+ * the attached U-Net), else the V-cycle. */
 int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream);
 
 /* Solve A lambda = rhs for a caller-given right-hand side ((nx+2, nz+2, ny+2), FP64),

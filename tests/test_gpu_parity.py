@@ -197,9 +197,11 @@ def test_same_input_solve_matches_in_method(oracle_mod, case64):
 
 
 def test_fp32_and_mixed_solves(oracle_mod, case64):
-    """FP32 Krylov vectors (reference schedule) and the MIXED schedule (FP32
-    vectors, FP64 solution + residual replacement, true-residual stop) against
-    the oracle's reference-precision solve driven to 1e-10."""
+    """FP32 Krylov vectors (reference schedule) and the MIXED shorthand (FP32
+    vectors, FP64 lambda, periodic FP64 residual replacement, restarts until
+    the FP64 true residual meets the target) against the oracle's
+    reference-precision solve driven to 1e-10; the withdrawn fused schedule is
+    rejected."""
     s, u, v, w, st1, st2, leak = oracle_mod.update_winds_first(case64, tol_rel=1e-10)
     lam_ref = s.vec("x")
     dom, stats = _gpu_first_update(case64, krylov_precision=_capi.KRYLOV_F32, tol_rel=1e-6)
@@ -211,10 +213,13 @@ def test_fp32_and_mixed_solves(oracle_mod, case64):
     dom, stats = _gpu_first_update(case64, solver=_capi.SOLVER_MIXED, criterion=_capi.CRIT_TRUE,
                                    tol_rel=1e-8, replace_every=20)
     assert stats[1]["status"] == 0
+    assert stats[1]["replacements"] >= 1
     assert stats[1]["true_res"] <= stats[1]["target"] * 1.0000001
     assert _rel(_lambda(dom), lam_ref) < 1e-5
     for g, r in ((dom.u_dqdt, u), (dom.v_dqdt, v), (dom.w_dqdt, w)):
         assert _rel(_np(g), r) < 1e-5
+    h = wi.handle(dom.nest_indx)
+    assert _capi.load().hicarw_set_options(h, C.byref(wi.WindOptions(solver=_capi.SOLVER_FUSED).to_c())) == -1
 
 
 def test_host_pointers_match_device_pointers(case64):

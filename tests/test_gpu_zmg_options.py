@@ -162,16 +162,14 @@ def test_mg_solve_w_levels(oracle_mod, case):
     assert _rel(lam, s.vec("x")) < 1e-5
 
 
-_MARCH = pytest.mark.skipif(os.environ.get("HICARW_TEST_SPMV_MARCH") != "1",
-                            reason="opt-in column-marching operator kernels: run with HICARW_TEST_SPMV_MARCH=1")
-
-
-@_MARCH
-@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13)])
+@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13), (132, 37, 9), (8, 6, 5)])
 def test_column_marching_operator_matches_row_kernels(shape, monkeypatch):
-    """The column-marching operator apply (HICARW_SPMV_MARCH=1) gives the row
-    kernels' FP64 values bit for bit, identity rows included, on a grid
-    narrower than one strip of 32 columns in places and on a ragged one."""
+    """The column-marching operator applies (HICARW_SPMV_MARCH=1: scalar, one
+    column per lane; unset: four columns per lane with 16-byte loads where nx
+    is a multiple of 4) give the row kernels' FP64 values bit for bit, identity
+    rows included: on a grid narrower than one strip in places, a ragged one
+    (nx odd: the row kernels serve the float4 setting), one whose last strip
+    holds a single lane, and one of two float4 groups."""
     from hicar_b200 import wind_iterative as wi
     nx, ny, nz = shape
     case = cases.build_case(nx, ny, nz, seed=19, adv_den=True, n_hills=10)
@@ -180,29 +178,37 @@ def test_column_marching_operator_matches_row_kernels(shape, monkeypatch):
     lib = _capi.load()
     x = np.random.default_rng(23).standard_normal((ny + 2, nz + 2, nx + 2))
     out = {}
-    for march in ("0", "1"):
-        monkeypatch.setenv("HICARW_SPMV_MARCH", march)
+    for march in ("0", "1", "4"):
+        if march == "4":
+            monkeypatch.delenv("HICARW_SPMV_MARCH", raising=False)
+        else:
+            monkeypatch.setenv("HICARW_SPMV_MARCH", march)
         y = np.empty_like(x)
         _capi.check(lib.hicarw_apply_operator(h, x.ctypes.data, y.ctypes.data, _capi.MEM_HOST, None), h)
         out[march] = y
     np.testing.assert_array_equal(out["1"], out["0"])
+    np.testing.assert_array_equal(out["4"], out["0"])
 
 
-@_MARCH
-def test_column_marching_solve(case, monkeypatch):
+@pytest.mark.parametrize("prec", [_capi.KRYLOV_F64, _capi.KRYLOV_F32_X64])
+def test_column_marching_solve(case, monkeypatch, prec):
     """The multigrid-preconditioned solve with the column-marching sigma and
-    five-dot kernels: the same lambda as with the row kernels (the reductions
-    sum in another order, so to the solve tolerance), iterations within one."""
+    five-dot kernels (scalar and float4), FP64 and FP32 Krylov vectors: the
+    same lambda as with the row kernels (the reductions sum in another order,
+    so to the solve tolerance), iterations within one."""
     from hicar_b200 import wind, wind_iterative as wi
     res = {}
-    for march in ("0", "1"):
-        monkeypatch.setenv("HICARW_SPMV_MARCH", march)
+    for march in ("0", "1", "4"):
+        if march == "4":
+            monkeypatch.delenv("HICARW_SPMV_MARCH", raising=False)
+        else:
+            monkeypatch.setenv("HICARW_SPMV_MARCH", march)
         wi.finalize_iter_winds()
         wind.reset()
         dom, _, div, _ = _calibrated(case)
         h = wi.handle(dom.nest_indx)
         wi.set_options(wi.WindOptions(tol_rel=1e-9, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
-                                      stall_iters=50))
+                                      stall_iters=50, krylov_precision=prec))
         dom.set_winds(case.u, case.v, case.w)
         _capi.load().hicarw_reset_solution(h, None)
         wind.calc_divergence(div, dom, use_dqdt=True)
@@ -210,9 +216,10 @@ def test_column_marching_solve(case, monkeypatch):
         lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
         _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
         res[march] = (st, lam)
-    assert res["1"][0]["status"] == 0
-    assert abs(res["1"][0]["iterations"] - res["0"][0]["iterations"]) <= 1
-    assert _rel(res["1"][1], res["0"][1]) < 1e-6
+    for march in ("1", "4"):
+        assert res[march][0]["status"] == 0
+        assert abs(res[march][0]["iterations"] - res["0"][0]["iterations"]) <= 1
+        assert _rel(res[march][1], res["0"][1]) < 1e-6
 
 
 @pytest.mark.parametrize("wlev", [(), (1, 2)])
