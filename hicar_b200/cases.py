@@ -228,6 +228,22 @@ def build_case(nx: int, ny: int, nz: int, dx: float = 250.0, n_hills: int = 20, 
     return Case(domain=d, u=u, v=v, w=w, alpha=a, adv_den=adv_den, name=name)
 
 
+def stability_inputs(case: Case, seed: int = 0, nsect: int = 72):
+    """Inputs of update_stability beside the winds: the potential temperature
+    (ny, nz, nx), a stable profile 288 K + 4 K/km with N(0, 0.2) K noise, and the
+    blocking heights per wind-direction sector (nsect, ny, nz, nx): U[0, 3000] m,
+    the range that HICAR's terrain search (compute_terrain_blocking_heights,
+    wind.F90:1571-1729) produces on these terrains, kept at least the level's
+    thickness."""
+    d = case.domain
+    rng = np.random.default_rng(seed + 4243)
+    theta = (288.0 + 0.004 * d.z.astype(np.float64) + rng.normal(0.0, 0.2, d.z.shape)).astype(F32)
+    ft = rng.uniform(0.0, 3000.0, (nsect, d.ny, d.nz, d.nx))
+    dz = (d.dz_levels[None, None, :, None] * d.jacobian[None]).astype(np.float64)
+    ft = np.maximum(ft, dz).astype(F32)
+    return theta, ft
+
+
 # Workloads named by what they are (sizes from the reference's benchmark plan).
 WORKLOADS = {
     "cpu64": dict(nx=64, ny=64, nz=20, n_hills=20, alpha="const"),

@@ -1496,6 +1496,19 @@ extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *a
     return HICARW_OK;
 }
 
+extern "C" int hicarw_update_stability(hicarw_handle *h, const float *u, const float *v, const float *z,
+                                       const float *theta, const float *froude_terrain, int nsect, int froude_mode,
+                                       float *froude, float *blk_ri, int mem_kind, void *stream)
+{
+    if (!h || !u || !v || !z || !theta || !froude || !blk_ri || h->d.nz < 5 || device_only(mem_kind) ||
+        (froude_mode && (!froude_terrain || nsect < 1)))
+        return HICARW_ERR_ARG;
+    launch_update_stability(h->d, u, v, z, theta, froude_terrain, nsect, froude_mode, froude, blk_ri,
+                            (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
 extern "C" int hicarw_smooth_alpha(hicarw_handle *h, float *alpha, int window, int nsmooths, int mem_kind,
                                    void *stream)
 {

@@ -590,6 +590,77 @@ __global__ void calc_w_kernel(Dims d, Metrics m, const float *__restrict__ div, 
     }
 }
 
+// update_stability (wind.F90:1421-1565) with calc_dry_stability, calc_Ri and
+// calc_froude (atm_utilities.F90:466-546): one thread per column (i, j), all
+// levels; FP32 in Fortran's order of operations.  The wind-direction sector
+// comes from atan2f, which is not correctly rounded on either side: a cell
+// whose direction lies within an ulp of a 5-degree sector edge can pick the
+// neighbouring sector's blocking height.
+constexpr float STAB_GRAVITY = 9.81f;          // mod_wrf_constants gravity
+constexpr float STAB_RAD2DEG = 57.2957779371f; // wind.F90:39
+
+__device__ __forceinline__ float dry_stability(float th_top, float th_bot, float z_top, float z_bot, bool has_surf,
+                                               float th_surf)
+{
+    if (has_surf) return STAB_GRAVITY * (th_top - th_bot) / ((z_top - z_bot) * th_surf);
+    return STAB_GRAVITY * (th_top - th_bot) / ((z_top - z_bot) * (th_top + th_bot) / 2.0f);
+}
+
+__global__ void update_stability_kernel(Dims d, const float *__restrict__ u, const float *__restrict__ v,
+                                        const float *__restrict__ z, const float *__restrict__ theta,
+                                        const float *__restrict__ fterr, int nsect, int froude_mode,
+                                        float *__restrict__ froude, float *__restrict__ blk_ri)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1;
+    if (i > d.nx) return;
+    const long long ncell = (long long)d.nx * d.ny * d.nz;
+    int rk = d.nz; // Ri_k_max (:1444-1454)
+    for (int k = 2; k <= d.nz; k++)
+        if (z[cidx(d, i, k, j)] - z[cidx(d, i, 1, j)] > 100.0f) {
+            rk = max(2, k - 1);
+            break;
+        }
+    const float us = (u[uidx(d, i, 5, j)] + u[uidx(d, i + 1, 5, j)]) / 2.0f; // u_shear(:, kms, :) (:1462-1465)
+    const float vs = (v[cidx(d, i, 5, j)] + v[cidx(d, i, 5, j + 1)]) / 2.0f;
+    const float th_b = theta[cidx(d, i, 1, j)], th_t = theta[cidx(d, i, rk, j)];
+    const float z_b = z[cidx(d, i, 1, j)], z_t = z[cidx(d, i, rk, j)];
+    // calc_Ri of the column's bulk stability (:1482-1495)
+    const float stab = dry_stability(th_t, th_b, z_t, z_b, false, 0.0f);
+    const float dz = z_t - z_b, a = us / dz, b = vs / dz;
+    const float den = a * a + b * b;
+    const float ri = den == 0.0f ? 10.0f : stab / den;
+    for (int k = 1; k <= d.nz; k++) {
+        const long long o = cidx(d, i, k, j);
+        blk_ri[o] = k < d.nz ? ri : 10.0f;
+        float fr = 0.1f;
+        if (froude_mode && k < d.nz) { // (:1503-1560)
+            const float um = (u[uidx(d, i, k, j)] + u[uidx(d, i + 1, k, j)]) / 2.0f;
+            const float vm = (v[cidx(d, i, k, j)] + v[cidx(d, i, k, j + 1)]) / 2.0f;
+            const float ws = sqrtf(um * um + vm * vm);
+            float wd = atan2f(-um, -vm) * STAB_RAD2DEG;
+            if (wd <= 0.0f) wd = wd + 360.0f;
+            if (wd == 360.0f) wd = 0.0f;
+            const int dir = max(min((int)(wd / 5.0f) + 1, nsect), 1);
+            const float tf = fterr[o + (long long)(dir - 1) * ncell];
+            const float st = dry_stability(theta[cidx(d, i, k + 1, j)], theta[o], z[cidx(d, i, k + 1, j)], z[o], true,
+                                           th_b);
+            const float bv = sqrtf(fmaxf(st, 0.0f));
+            const float fden = tf * bv;
+            fr = fden == 0.0f ? 100.0f : ws / fden;
+        }
+        froude[o] = fr;
+    }
+}
+
+void launch_update_stability(const Dims &d, const float *u, const float *v, const float *z, const float *theta,
+                             const float *fterr, int nsect, int froude_mode, float *froude, float *blk_ri,
+                             cudaStream_t st)
+{
+    dim3 b(128), g((d.nx + 127) / 128, d.ny);
+    update_stability_kernel<<<g, b, 0, st>>>(d, u, v, z, theta, fterr, nsect, froude_mode, froude, blk_ri);
+    count_launch(1);
+}
+
 // calc_alpha (wind.F90:1102-1173), elementwise part; (1/Fr)**4 as (t*t)*(t*t)
 __global__ void calc_alpha_kernel(Dims d, const float *__restrict__ froude, float *__restrict__ alpha)
 {

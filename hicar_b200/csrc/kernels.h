@@ -33,6 +33,9 @@ void launch_idealized_wgrid(const Dims &d, const Metrics &m, const float *u, con
 void launch_calc_w(const Dims &d, const Metrics &m, const float *div, const float *rho, float *w, int adv_den,
                    cudaStream_t st);
 void launch_calc_alpha(const Dims &d, const float *froude, float *alpha, int halo, cudaStream_t st);
+void launch_update_stability(const Dims &d, const float *u, const float *v, const float *z, const float *theta,
+                             const float *fterr, int nsect, int froude_mode, float *froude, float *blk_ri,
+                             cudaStream_t st);
 void launch_smooth_xy(const Dims &d, const float *in, float *out, int w, cudaStream_t st);
 void launch_module_vars(const Dims &d, const float *adz, const float *dzdx, const float *dzdy, const float *nterr,
                         float *dz_if, float *dzdx_surf, float *dzdy_surf, float *adz_col, cudaStream_t st);

@@ -108,6 +108,20 @@ def balance_uvw(domain: DeviceDomain, adv_den: bool, update: bool = False) -> No
                                                 int(bool(update)), _capi.MEM_DEVICE, _s()), h)
 
 
+def update_stability(domain: DeviceDomain, z, theta, froude, blk_ri, froude_terrain=None,
+                     froude_mode: bool = True) -> None:
+    """update_stability (wind.F90:1421-1565): blk_ri and (froude_mode: alpha_const < 0
+    with iterative winds) the Froude number from the dqdt winds, the mass-level
+    heights z, the potential temperature theta and the sector blocking heights
+    froude_terrain (nsect, ny, nz, nx)."""
+    h = wi.handle(domain.nest_indx)
+    nsect = int(froude_terrain.shape[0]) if froude_terrain is not None else 0
+    _capi.check(_capi.load().hicarw_update_stability(
+        h, ptr(domain.u_dqdt), ptr(domain.v_dqdt), ptr(z), ptr(theta),
+        ptr(froude_terrain) if froude_terrain is not None else None, nsect, int(bool(froude_mode)), ptr(froude),
+        ptr(blk_ri), _capi.MEM_DEVICE, _s()), h)
+
+
 def calc_alpha(domain: DeviceDomain, froude, halo: int = 1, window: int = 2, nsmooths: int = 3) -> None:
     """calc_alpha (wind.F90:1102-1173) into domain.wind_alpha, then the smoothing of
     update_winds (:784: windowsize 2, clamped to the halo width, 3 passes)."""

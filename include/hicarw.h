@@ -316,6 +316,19 @@ int hicarw_calc_idealized_wgrid(hicarw_handle *h, const float *u, const float *v
  * (use_dqdt selects the divergence form of the dqdt winds, as calc_divergence). */
 int hicarw_balance_uvw(hicarw_handle *h, const float *u, const float *v, const float *density, float *w, int adv_den,
                        int use_dqdt, int mem_kind, void *stream);
+/* update_stability (wind.F90:1421-1565): the bulk Richardson number blk_ri of each
+ * column (its stability between the surface and the level ~100 m above it, and
+ * the shear of the mean wind at level 5 over that depth) and, when froude_mode !=
+ * 0 (alpha_const < 0 with iterative winds), the Froude number of every cell: the
+ * mean wind speed over the local stability (surface potential temperature as the
+ * reference) times the blocking height of the cell's wind-direction sector,
+ * froude_terrain (nx, nz, ny, nsect) with 5-degree sectors (nsect = 72 in HICAR;
+ * domain%vars_4d froude_terrain).  froude is 0.1 and blk_ri 10 on the top level,
+ * froude 0.1 everywhere when froude_mode == 0.  u, v are the dqdt winds, z the
+ * mass-level heights, theta the potential temperature (nx, nz, ny); nz >= 5. */
+int hicarw_update_stability(hicarw_handle *h, const float *u, const float *v, const float *z, const float *theta,
+                            const float *froude_terrain, int nsect, int froude_mode, float *froude, float *blk_ri,
+                            int mem_kind, void *stream);
 /* calc_alpha (wind.F90:1102-1173): alpha(Froude) in [0.2, 2], 0.2 on the top level,
  * the `halo` outermost rows / columns copied from the first tile row / column. */
 int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *alpha, int halo, int mem_kind, void *stream);

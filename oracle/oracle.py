@@ -63,6 +63,7 @@ def _lib(precision: str):
     lib.orc_balance_uvw.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int]
     lib.orc_calc_alpha.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, C.c_int]
     lib.orc_smooth_array.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int]
+    lib.orc_update_stability.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int, C.c_int, vp, vp]
     lib.orc_spmv.argtypes = [vp, vp, vp]
     lib.orc_apply_precond.argtypes = [vp, vp, vp]
     lib.orc_bicgstab.argtypes = [vp, C.c_int, vp]
@@ -193,6 +194,18 @@ class OracleSolver:
         out = np.empty((self.ny, self.nz, self.nx), self.dt)
         self.lib.orc_calc_alpha(self.nx, self.ny, self.nz, _ptr(self._a(froude)), _ptr(out), int(halo))
         return out
+
+    def update_stability(self, u, v, z, theta, froude_terrain=None, froude_mode=True):
+        """update_stability (wind.F90:1421-1565): (froude, blk_ri), each (ny, nz, nx);
+        froude_terrain has shape (nsect, ny, nz, nx) (Fortran (nx, nz, ny, nsect))."""
+        froude = np.empty((self.ny, self.nz, self.nx), self.dt)
+        blk_ri = np.empty_like(froude)
+        ft = self._a(froude_terrain) if froude_terrain is not None else None
+        nsect = int(ft.shape[0]) if ft is not None else 0
+        self.lib.orc_update_stability(self.nx, self.ny, self.nz, _ptr(self._a(u)), _ptr(self._a(v)), _ptr(self._a(z)),
+                                      _ptr(self._a(theta)), _ptr(ft) if ft is not None else None, nsect,
+                                      int(bool(froude_mode)), _ptr(froude), _ptr(blk_ri))
+        return froude, blk_ri
 
     def smooth_array(self, a, window, nsmooths):
         """smooth_array_3d, ydim = 3 (array_utilities.F90:322-397), nsmooths passes."""

@@ -1135,3 +1135,95 @@ void orc_smooth_array(int nx, int ny, int nz, fld *a, int window, int nsmooths)
     }
     free(in);
 }
+
+/* ------------------------------------------------------------------------ */
+/* update_stability (wind.F90:1421-1565) with its helpers calc_dry_stability,  */
+/* calc_Ri and calc_froude (atm_utilities.F90:466-546)                       */
+/* ------------------------------------------------------------------------ */
+#define ORC_GRAVITY ((fld)9.81)          /* mod_wrf_constants gravity */
+#define ORC_RAD2DEG ((fld)57.2957779371) /* wind.F90:39 */
+#if defined(ORC_FLD_DOUBLE)
+#define FLD_ATAN2 atan2
+#else
+#define FLD_ATAN2 atan2f
+#endif
+
+/* calc_dry_stability (atm_utilities.F90:466-479); has_surf selects the th_surf form */
+static fld orc_dry_stability(fld th_top, fld th_bot, fld z_top, fld z_bot, int has_surf, fld th_surf)
+{
+    if (has_surf) return ORC_GRAVITY * (th_top - th_bot) / ((z_top - z_bot) * th_surf);
+    return ORC_GRAVITY * (th_top - th_bot) / ((z_top - z_bot) * (th_top + th_bot) / (fld)2);
+}
+
+/* calc_Ri (atm_utilities.F90:528-546) */
+static fld orc_calc_ri(fld bv2, fld u_shear, fld v_shear, fld dz)
+{
+    fld a = u_shear / dz, b = v_shear / dz;
+    fld denom = a * a + b * b;
+    return denom == (fld)0 ? (fld)10 : bv2 / denom;
+}
+
+/* calc_froude (atm_utilities.F90:504-525) */
+static fld orc_calc_froude(fld bv2, fld barrier_height, fld wind_speed)
+{
+    fld n = FLD_SQRT(bv2 > (fld)0 ? bv2 : (fld)0);
+    fld denom = barrier_height * n;
+    return denom == (fld)0 ? (fld)100 : wind_speed / denom;
+}
+
+/* update_stability at one rank: u (nx+1, nz, ny), v (nx, nz, ny+1) are the dqdt
+ * winds, z and theta (nx, nz, ny) the mass-level heights and potential
+ * temperature, froude_terrain (nx, nz, ny, nsect) the blocking heights per
+ * 5-degree wind-direction sector.  Writes froude and blk_ri (nx, nz, ny);
+ * froude_mode != 0 is the branch of alpha_const < 0 with iterative winds
+ * (otherwise froude stays 0.1). */
+void orc_update_stability(int nx, int ny, int nz, const fld *u, const fld *v, const fld *z, const fld *theta,
+                          const fld *froude_terrain, int nsect, int froude_mode, fld *froude, fld *blk_ri)
+{
+    const fld RI_Z_MAX = (fld)100.0;
+#define SC(i, k, j) ((size_t)((i) - 1) + (size_t)nx * ((size_t)((k) - 1) + (size_t)nz * (size_t)((j) - 1)))
+#define SU(i, k, j) ((size_t)((i) - 1) + (size_t)(nx + 1) * ((size_t)((k) - 1) + (size_t)nz * (size_t)((j) - 1)))
+#define SV(i, k, j) ((size_t)((i) - 1) + (size_t)nx * ((size_t)((k) - 1) + (size_t)nz * (size_t)((j) - 1)))
+#pragma omp parallel for
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            int rk = nz; /* Ri_k_max (:1444-1454) */
+            for (int k = 2; k <= nz; k++)
+                if (z[SC(i, k, j)] - z[SC(i, 1, j)] > RI_Z_MAX) {
+                    rk = k - 1 > 2 ? k - 1 : 2;
+                    break;
+                }
+            /* u_m, v_m (:1457-1460) and the surface shear u_m(:, kms+4, :) (:1462-1465) */
+            fld us = (u[SU(i, 5, j)] + u[SU(i + 1, 5, j)]) / (fld)2;
+            fld vs = (v[SV(i, 5, j)] + v[SV(i, 5, j + 1)]) / (fld)2;
+            for (int k = 1; k <= nz; k++) { /* (:1472-1480) */
+                froude[SC(i, k, j)] = (fld)0.1;
+                blk_ri[SC(i, k, j)] = (fld)10.0;
+            }
+            for (int k = 1; k <= nz - 1; k++) { /* (:1482-1495) */
+                fld th_bot = theta[SC(i, 1, j)], th_top = theta[SC(i, rk, j)];
+                fld z_bot = z[SC(i, 1, j)], z_top = z[SC(i, rk, j)];
+                fld stab = orc_dry_stability(th_top, th_bot, z_top, z_bot, 0, (fld)0);
+                blk_ri[SC(i, k, j)] = orc_calc_ri(stab, us, vs, z_top - z_bot);
+            }
+            if (!froude_mode) continue;
+            for (int k = 1; k <= nz - 1; k++) { /* (:1503-1560) */
+                fld um = (u[SU(i, k, j)] + u[SU(i + 1, k, j)]) / (fld)2;
+                fld vm = (v[SV(i, k, j)] + v[SV(i, k, j + 1)]) / (fld)2;
+                fld ws = FLD_SQRT(um * um + vm * vm);
+                fld wd = FLD_ATAN2(-um, -vm) * ORC_RAD2DEG;
+                if (wd <= (fld)0.0) wd = wd + (fld)360;
+                if (wd == (fld)360.0) wd = (fld)0.0;
+                int dir = (int)(wd / (fld)5) + 1;
+                dir = dir < nsect ? dir : nsect;
+                dir = dir > 1 ? dir : 1;
+                fld tf = froude_terrain[SC(i, k, j) + (size_t)(dir - 1) * (size_t)nx * nz * ny];
+                fld stab = orc_dry_stability(theta[SC(i, k + 1, j)], theta[SC(i, k, j)], z[SC(i, k + 1, j)],
+                                             z[SC(i, k, j)], 1, theta[SC(i, 1, j)]);
+                froude[SC(i, k, j)] = orc_calc_froude(stab, tf, ws);
+            }
+        }
+#undef SC
+#undef SU
+#undef SV
+}

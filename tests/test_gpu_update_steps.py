@@ -104,3 +104,32 @@ def test_calc_alpha_and_smoothing(setup):
     _capi.check(lib.hicarw_smooth_alpha(h, _p(a), 2, 3, _capi.MEM_DEVICE, None), h)
     torch.cuda.synchronize()
     _eq(a, s.smooth_array(ref, 2, 3))
+
+
+def test_update_stability(setup):
+    """update_stability on the device against the oracle: the bulk Richardson
+    number bit-exact; the Froude number bit-exact in every cell whose wind
+    direction is not within 1e-4 degree of a 5-degree sector edge (atan2f is not
+    correctly rounded, so such a cell may take the neighbouring sector), and
+    the Froude branch switched off leaves 0.1 everywhere."""
+    case, s = setup
+    if case.domain.nz < 5:
+        pytest.skip("update_stability reads the wind at level 5")
+    dom, h = _handle(case)
+    theta, ft = cases.stability_inputs(case, seed=5)
+    ref_fr, ref_ri = s.update_stability(case.u, case.v, case.domain.z, theta, ft)
+    fr = torch.empty(case.w.shape, dtype=torch.float32, device="cuda")
+    ri = torch.empty_like(fr)
+    from hicar_b200 import wind
+    wind.update_stability(dom, _t(case.domain.z), _t(theta), fr, ri, froude_terrain=_t(ft))
+    torch.cuda.synchronize()
+    _eq(ri, ref_ri)
+    um = 0.5 * (case.u[:, :, :-1].astype(np.float64) + case.u[:, :, 1:])
+    vm = 0.5 * (case.v[:-1].astype(np.float64) + case.v[1:])
+    wd = np.degrees(np.arctan2(-um, -vm)) % 360.0
+    edge = np.abs(wd / 5.0 - np.round(wd / 5.0)) * 5.0 < 1e-4
+    diff = fr.cpu().numpy() != ref_fr
+    assert not (diff & ~edge).any(), int((diff & ~edge).sum())
+    wind.update_stability(dom, _t(case.domain.z), _t(theta), fr, ri, froude_terrain=None, froude_mode=False)
+    torch.cuda.synchronize()
+    assert bool((fr == 0.1).all())

@@ -207,3 +207,41 @@ def test_calc_alpha_and_smoothing(oracle_mod, c1):
     sm = s.smooth_array(spike, 2, 1)
     assert sm[8:13, 3, 10:15] == pytest.approx(np.ones((5, 5)))
     assert sm.sum() == pytest.approx(25.0)
+
+
+def test_update_stability_known_answers(oracle_mod, c1):
+    """update_stability (wind.F90:1421-1565) on a uniform wind and a linear
+    potential-temperature profile: the wind blows from 92.5 degrees, so every
+    cell takes the blocking height of sector int(92.5/5) + 1 = 19 (a wind from
+    exactly 90 degrees lands in sector 18: the reference's rad2deg,
+    57.2957779371, is below 180/pi, so 90 degrees reads 89.9999975); the local
+    Brunt-Vaisala frequency is g dtheta/dz / theta_surf; the bulk Richardson
+    number uses the column between the surface and the level ~100 m up and the
+    wind at level 5; the top level keeps Fr = 0.1 and Ri = 10; with the Froude
+    branch off every Froude number is 0.1."""
+    d = c1.domain
+    s = oracle_mod.OracleSolver(d, "f64")
+    U0 = 7.5
+    ang = np.radians(92.5)
+    u = np.full(c1.u.shape, -U0 * np.sin(ang))
+    v = np.full(c1.v.shape, -U0 * np.cos(ang))
+    z = d.z.astype(np.float64)
+    theta = 290.0 + 0.005 * z
+    ft = np.full((72, d.ny, d.nz, d.nx), 1.0e6)
+    ft[18] = 800.0
+    fr, ri = s.update_stability(u, v, z, theta, ft)
+    g = 9.81
+    n2 = g * (theta[:, 1:, :] - theta[:, :-1, :]) / ((z[:, 1:, :] - z[:, :-1, :]) * theta[:, :1, :])
+    np.testing.assert_allclose(fr[:, :-1, :], U0 / (800.0 * np.sqrt(n2)), rtol=1e-10)
+    np.testing.assert_array_equal(fr[:, -1, :], 0.1)
+    # bulk Ri: Ri_k_max = the last level within 100 m of the surface (at least 2)
+    rk = np.argmax(z - z[:, :1, :] > 100.0, axis=1)  # first level above 100 m (0-based)
+    rk = np.maximum(rk - 1, 1)
+    zt = np.take_along_axis(z, rk[:, None, :], axis=1)[:, 0, :]
+    tt = np.take_along_axis(theta, rk[:, None, :], axis=1)[:, 0, :]
+    nb = g * (tt - theta[:, 0, :]) / ((zt - z[:, 0, :]) * (tt + theta[:, 0, :]) / 2.0)
+    ri_ref = nb / (U0 / (zt - z[:, 0, :])) ** 2
+    np.testing.assert_allclose(ri[:, :-1, :], np.broadcast_to(ri_ref[:, None, :], ri[:, :-1, :].shape), rtol=1e-10)
+    np.testing.assert_array_equal(ri[:, -1, :], 10.0)
+    fr0, _ = s.update_stability(u, v, z, theta, ft, froude_mode=False)
+    np.testing.assert_array_equal(fr0, 0.1)
