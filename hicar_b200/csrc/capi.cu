@@ -1496,6 +1496,20 @@ extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *a
     return HICARW_OK;
 }
 
+extern "C" int hicarw_debug_wait_timeout(hicarw_handle *h, double limit_us, void *stream)
+{
+    if (!h || !(limit_us >= 1.0 && limit_us <= 100000.0)) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(&h->st->err, 0, sizeof(int), s));
+    mg_wait_probe(&h->st->err, (uint64_t)(limit_us * 1000.0), s);
+    CK(cudaGetLastError());
+    const int rc = fetch_state(h, s); // HICARW_ERR_TIMEOUT when the wait gave up
+    CK(cudaMemsetAsync(&h->st->err, 0, sizeof(int), s));
+    CK(cudaStreamSynchronize(s));
+    if (rc == HICARW_ERR_TIMEOUT) h->err = "a bounded device-side wait timed out (wait probe)";
+    return rc;
+}
+
 extern "C" int hicarw_update_stability(hicarw_handle *h, const float *u, const float *v, const float *z,
                                        const float *theta, const float *froude_terrain, int nsect, int froude_mode,
                                        float *froude, float *blk_ri, int mem_kind, void *stream)

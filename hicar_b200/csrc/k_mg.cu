@@ -1338,6 +1338,29 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
 template void mg_apply<double>(const Mg &, const double *, double *, const SolveState *, cudaStream_t);
 template void mg_apply<float>(const Mg &, const float *, float *, const SolveState *, cudaStream_t);
 
+// ---- the bounded wait of the tensor-copy kernels, made to run out ----
+// An mbarrier that expects one arrival that never comes (no copy is issued to
+// it), waited on with tc::mbar_wait and a limit of limit_ns: on time-out the
+// kernel records the error flag as the smoother and convolution kernels do and
+// returns, leaving nothing in flight.
+__global__ void wait_probe_kernel(uint64_t limit_ns, int *err)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    const bool ok = tc::mbar_wait(&bar, 0, limit_ns);
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+}
+
+void mg_wait_probe(int *err, uint64_t limit_ns, cudaStream_t s)
+{
+    wait_probe_kernel<<<1, 32, 0, s>>>(limit_ns, err);
+    count_launch(1);
+}
+
 // ---- s = r - alpha v (the MG schedule applies M^-1 to s separately) ----
 template <typename V>
 __global__ void s_update_kernel(long long n, const V *__restrict__ r, const V *__restrict__ v, V *__restrict__ sv,

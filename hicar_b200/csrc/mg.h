@@ -36,6 +36,8 @@ void mg_free(Mg &mg);
 long long mg_tma_posts(); // post-smoother launches enqueued through the tensor-copy kernel
 template <typename V>
 void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStream_t s);
+// one bounded mbarrier wait that nothing completes, limit_ns long; sets *err on time-out
+void mg_wait_probe(int *err, uint64_t limit_ns, cudaStream_t s);
 template <typename V>
 void launch_s_update(const Dims &d, const V *r, const V *v, V *s, const SolveState *stt, cudaStream_t st);
 

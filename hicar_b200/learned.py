@@ -354,15 +354,20 @@ def composite_pairs(case, net: UNet, ks=SOLVER_ITERS, tight_tol: float = 1e-10, 
 
 
 def train_online(net: UNet, terrain_cases, steps_per_terrain: int = 2, batch: int = 4, lr: float = 1e-3,
-                 lr_decay_every: int = 0, buffer: int = 64, seed: int = 0, log_every: int = 0):
+                 lr_decay_every: int = 0, buffer: int = 64, seed: int = 0, log_every: int = 0,
+                 time_limit_s: float = 0.0):
     """Adam on the composite's supervised loss |O_0 - T|^2 / |T|^2 (a
     relative error of the learned correction), with the samples of each
     terrain (composite_pairs) added to a replay buffer of the latest `buffer`
     samples as the terrains stream past; `steps_per_terrain` steps of `batch`
     samples drawn from the buffer follow each terrain.  `terrain_cases` yields
-    seeded cases (never stored all at once).  Returns the loss history."""
+    seeded cases (never stored all at once).  time_limit_s > 0 stops after the
+    terrain during which that much wall time has passed.  Returns the loss
+    history and the number of terrains used."""
     import collections
+    import time
     torch = _torch()
+    t_start = time.time()
     gen = torch.Generator().manual_seed(seed)
     pool = collections.deque(maxlen=buffer)
     hist = []
@@ -382,9 +387,11 @@ def train_online(net: UNet, terrain_cases, steps_per_terrain: int = 2, batch: in
             net.adam_step(lr)
             hist.append(tot / batch)
         if log_every and n_terrains % log_every == 0:
-            print(f"terrain {n_terrains}: loss {sum(hist[-log_every:]) / max(1, len(hist[-log_every:])):.4f}",
-                  flush=True)
-    return hist
+            print(f"terrain {n_terrains}: loss {sum(hist[-log_every:]) / max(1, len(hist[-log_every:])):.4f} "
+                  f"({time.time() - t_start:.0f} s)", flush=True)
+        if time_limit_s > 0 and time.time() - t_start > time_limit_s:
+            break
+    return hist, n_terrains
 
 
 def train(net: UNet, pairs, steps: int, lr: float = 1e-3, batch: int = 4, seed: int = 0, loss: str = "residual"):

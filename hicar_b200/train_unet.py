@@ -58,6 +58,8 @@ def main(argv=None):
                          "composite preconditioner's residuals after the V-cycle (online)")
     ap.add_argument("--steps-per-terrain", type=int, default=2, help="composite: Adam steps after each terrain")
     ap.add_argument("--buffer", type=int, default=64, help="composite: replay buffer of samples")
+    ap.add_argument("--max-minutes", type=float, default=0.0,
+                    help="composite: stop streaming terrains after this much wall time (0: all terrains)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     if args.out is None:
@@ -71,14 +73,16 @@ def main(argv=None):
         t0 = time.time()
         stream = (cases.build_case(args.nx, args.ny, args.nz, seed=args.seed0 + t, adv_den=True,
                                    n_hills=args.hills) for t in range(args.terrains))
-        hist = L.train_online(net, stream, steps_per_terrain=args.steps_per_terrain, batch=args.batch, lr=args.lr,
-                              lr_decay_every=max(1, args.terrains // 4), buffer=args.buffer, seed=args.seed0,
-                              log_every=max(1, args.terrains // 16))
+        hist, used = L.train_online(net, stream, steps_per_terrain=args.steps_per_terrain, batch=args.batch,
+                                    lr=args.lr, lr_decay_every=max(1, args.terrains // 4), buffer=args.buffer,
+                                    seed=args.seed0, log_every=max(1, args.terrains // 16),
+                                    time_limit_s=60.0 * args.max_minutes)
         torch.cuda.synchronize()
         p = net.params().cpu().numpy()
         os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
         np.save(args.out, p)
-        info = {"grid": [args.nx, args.ny, args.nz], "terrains": args.terrains, "source": "composite",
+        info = {"grid": [args.nx, args.ny, args.nz], "terrains": used, "terrains_requested": args.terrains,
+                "source": "composite",
                 "pairs_per_terrain": len(L.SOLVER_ITERS), "solver_iterations_logged": list(L.SOLVER_ITERS),
                 "steps": len(hist), "steps_per_terrain": args.steps_per_terrain, "batch": args.batch,
                 "buffer": args.buffer, "lr": args.lr, "seed0": args.seed0, "hills": args.hills,

@@ -261,6 +261,15 @@ int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms
  * that overlap on the GPU race on the shared array. */
 int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm, void *stream);
 
+/* Test hook of the bounded device-side waits (no counterpart in the reference):
+ * one kernel waits, through the same bounded mbarrier wait as the tensor-copy
+ * smoother and the tensor-core convolutions, on a barrier that nothing completes,
+ * with a limit of limit_us (1 .. 100000) microseconds.  It gives up, records the
+ * error flag and returns, with nothing in flight; this call then returns
+ * HICARW_ERR_TIMEOUT as a timed-out solve does, and clears the flag, so that
+ * the handle and the GPU stay usable. */
+int hicarw_debug_wait_timeout(hicarw_handle *h, double limit_us, void *stream);
+
 /* Last CUDA error string of this handle (static storage). */
 const char *hicarw_last_error(hicarw_handle *h);
 
