@@ -818,17 +818,34 @@ def run_ours(args, wl):
             "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_c1": c1,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "clocks": clocks, "gpu_launches": int(launches)}
+    wi.finalize_iter_winds()
+    if world == 1 and not args.no_batch and args.workload == "mixed1024":
+        torch.cuda.synchronize()
+        b = batch_measure(args, WORKLOADS["batch96"], rank, world, dist, local, quick=True)
+        c = b["config"]
+        line["config"].update({"batch96_solves_per_s": b["value"], "batch96_e2e_solves_per_s": b["e2e"]["value"],
+                               "batch96_sequential_solves_per_s": c["sequential_solves_per_s"],
+                               "batch96_p50_ms": c["batched_p50_ms"], "batch96_p99_ms": c["batched_p99_ms"],
+                               "batch96_learned_subdomains": c["learned_subdomains"],
+                               "batch96_iterations_max": c["iterations_max"]})
+        line["batch96"] = {k: b[k] for k in ("value", "ms_per_step", "steps", "warmup", "config", "e2e", "clocks",
+                                             "gpu_launches")}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    wi.finalize_iter_winds()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_batch(args, wl):
-    """The batch workload: every step solves all subdomains (divergence, batched
-    MG-preconditioned BiCGStab in one graph launch, wind correction)."""
+def batch_measure(args, wl, rank, world, dist, local, quick=False):
+    """The batch workload: every step solves all subdomains (divergence, the
+    batched solve in one graph launch, wind correction).  Three of every four
+    subdomains use BiCGStab with the V-cycle, every fourth FGMRES with the
+    composite learned preconditioner when trained parameters are shipped.  The
+    kernel autotuner picks the operator kernels' z-march depth and the
+    smoother's feed per subdomain-size bucket (quick: a reduced search), the
+    batch autotuner the concurrent chains and iterations per loop body.
+    Returns the JSON line."""
     import ctypes as C
 
     import numpy as np
@@ -836,8 +853,137 @@ def run_batch(args, wl):
     from hicar_b200 import _capi
     from hicar_b200.batch import BatchSolver, subdomain_cases
     from hicar_b200.domain import ptr
+    from hicar_b200.train_unet import COMPOSITE_WEIGHTS, load_params
     from hicar_b200.wind_iterative import WindOptions
 
+    lib = _capi.load()
+    stream = torch.cuda.current_stream()
+    cyc = MG_CYCLE if MG_CYCLE != "auto" else "V01-W24"  # batches: the cycle named on the command line
+    opts = WindOptions(tol_rel=TOL, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50,
+                       advect_density=wl["adv_den"], **MG_CYCLES[cyc])
+    params = None
+    if args.batch_learned_every > 0 and os.path.exists(COMPOSITE_WEIGHTS):
+        params = torch.from_numpy(load_params(COMPOSITE_WEIGHTS))
+    bs = BatchSolver(subdomain_cases(wl["batch"], seed=subdomain_seed(rank), nxy=wl["nxy"], nz=wl["nz"],
+                                     n_hills=wl["n_hills"], dx=wl["dx"]), options=opts, stream=stream.cuda_stream,
+                     learned_every=args.batch_learned_every if params is not None else 0, learned_params=params)
+    try:
+        kt = bs.autotune_kernels(levels=(16, 32) if quick else (8, 16, 32, 64), feeds=(1,) if quick else (1, 0))
+        tuned_ms = bs.autotune()
+        lanes, chunk = bs.config()
+        # the same subdomains one after another through hicarw_calc_iter_winds (untimed by the contract; reported)
+        bs.restore_winds()
+        bs.divergence()
+        torch.cuda.synchronize()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record()
+        st = _capi.Stats()
+        seq_each = []
+        for i, (h, dom) in enumerate(zip(bs.handles, bs.domains)):
+            lib.hicarw_reset_solution(h, C.c_void_p(bs.stream))
+            _capi.check(lib.hicarw_calc_iter_winds(h, ptr(dom.wind_alpha), ptr(bs.divs[i]), ptr(dom.density), 1,
+                                                   ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt),
+                                                   _capi.MEM_DEVICE, C.c_void_p(bs.stream), C.byref(st)), h)
+            seq_each.append(st.solve_ms)
+        q1.record()
+        torch.cuda.synchronize()
+        seq_ms = q0.elapsed_time(q1)
+        steps, warmup = (3, 1) if quick else (args.steps, args.warmup)
+        for _ in range(warmup):
+            bs.step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(local)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = lib.hicarw_kernel_launches()
+        torch.cuda.synchronize()
+        e0.record()
+        stats = []
+        for _ in range(steps):
+            stats = bs.step()
+        e1.record()
+        torch.cuda.synchronize()
+        launches = lib.hicarw_kernel_launches() - l0
+        clocks = sampler.stop()
+        t_ms = reduce_max(e0.elapsed_time(e1), dist, f"cuda:{local}")
+        value = world * steps * bs.n / (t_ms / 1000.0)
+        # e2e: every subdomain's winds from pinned host memory in, corrected winds out
+        host = [[torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in sv] for sv in bs.saved]
+        for hs, sv in zip(host, bs.saved):
+            for dst, src in zip(hs, sv):
+                dst.copy_(src.cpu())
+        outs = [[torch.empty_like(a) for a in hs] for hs in host]
+        h2d = sum(a.numel() * 4 for hs in host for a in hs)
+
+        def e2e_step():
+            for dom, hs in zip(bs.domains, host):
+                dom.u_dqdt.copy_(hs[0], non_blocking=True)
+                dom.v_dqdt.copy_(hs[1], non_blocking=True)
+                dom.w_dqdt.copy_(hs[2], non_blocking=True)
+            bs.divergence()
+            bs.solve(cold=True)
+            for dom, os_ in zip(bs.domains, outs):
+                os_[0].copy_(dom.u_dqdt, non_blocking=True)
+                os_[1].copy_(dom.v_dqdt, non_blocking=True)
+                os_[2].copy_(dom.w_dqdt, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0.record()
+        e2e_steps = max(1, min(steps, 3))
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        te = reduce_max(e0.elapsed_time(e1), dist, f"cuda:{local}")
+        e2e_value = world * e2e_steps * bs.n / (te / 1000.0)
+        big = max(range(bs.n), key=lambda i: bs.domains[i].nx * bs.domains[i].ny * bs.domains[i].nz)
+        d_big = bs.domains[big]
+        roofline = None if quick else profile_roofline(lib, bs.handles[big], stream, False,
+                                                       d_big.nx * d_big.ny * d_big.nz)
+        if roofline:
+            roofline["profiled_subdomain"] = [d_big.nx, d_big.ny, d_big.nz]
+        iters = [s_["iterations"] for s_ in stats]
+        bs.step()
+        lat = bs.latencies()
+        seq_lat = np.asarray(seq_each)
+        n_learned = sum(bs.learned)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+                "warmup": warmup, "ms_per_step": t_ms / steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"batch{bs.n}: {bs.n} subdomains, nx,ny in {wl['nxy'][0]}..{wl['nxy'][1]} "
+                                       f"step {wl['nxy'][2]}, nz in {wl['nz'][0]}..{wl['nz'][1]} step {wl['nz'][2]}, "
+                                       f"{bs.cells} cells, {wl['n_hills']} hills each, adv_den={wl['adv_den']}",
+                           "solver": f"batched: BiCGStab + V-cycle ({bs.n - n_learned}), FGMRES(30) + V-cycle + "
+                                     f"U-Net correction ({n_learned}); one graph launch per step",
+                           "mg_cycle": cyc, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
+                           "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms, "kernel_autotune": kt,
+                           "learned_subdomains": n_learned,
+                           "sequential_solves_per_s": bs.n / (seq_ms / 1000.0), "iterations_min": min(iters),
+                           "iterations_max": max(iters), "statuses": sorted(set(s_["status"] for s_ in stats)),
+                           "batched_p50_ms": float(np.percentile(lat, 50)),
+                           "batched_p99_ms": float(np.percentile(lat, 99)), "batched_max_ms": float(lat.max()),
+                           "sequential_p50_ms": float(np.percentile(seq_lat, 50)),
+                           "sequential_p99_ms": float(np.percentile(seq_lat, 99)),
+                           "latency_note": "batched: completion time of each solve from the start of the batch graph; "
+                                           "sequential: each subdomain's own calc_iter_winds",
+                           "l2": "inputs larger than L2 (coefficients of all subdomains)",
+                           "parallelism": f"{world} ranks x {bs.n} subdomains" if world > 1 else "1 GPU"},
+                "roofline": roofline, "cpu_baseline": None,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+                "clocks": clocks, "gpu_launches": int(launches)}
+    finally:
+        bs.close()
+    return line
+
+
+def run_batch(args, wl):
+    """The batch workload as its own bench line."""
+    import torch
     rank, world, local = dist_setup()
     torch.cuda.set_device(local)
     dist = None
@@ -846,122 +992,9 @@ def run_batch(args, wl):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    lib = _capi.load()
-    stream = torch.cuda.current_stream()
-    cyc = MG_CYCLE if MG_CYCLE != "auto" else "V11"  # batches: the cycle named on the command line, else V(1,1)
-    opts = WindOptions(tol_rel=TOL, wind_solver_iterations=3000, precond=_capi.PRECOND_MG, stall_iters=50,
-                       advect_density=wl["adv_den"], **MG_CYCLES[cyc])
-    bs = BatchSolver(subdomain_cases(wl["batch"], seed=subdomain_seed(rank), nxy=wl["nxy"], nz=wl["nz"],
-                                     n_hills=wl["n_hills"],
-                                     dx=wl["dx"]), options=opts, stream=stream.cuda_stream)
-    tuned_ms = bs.autotune()
-    lanes, chunk = bs.config()
-    # the same subdomains one after another through hicarw_calc_iter_winds (untimed by the contract; reported)
-    bs.restore_winds()
-    bs.divergence()
-    torch.cuda.synchronize()
-    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    q0.record()
-    st = _capi.Stats()
-    seq_each = []
-    for i, (h, dom) in enumerate(zip(bs.handles, bs.domains)):
-        lib.hicarw_reset_solution(h, C.c_void_p(bs.stream))
-        _capi.check(lib.hicarw_calc_iter_winds(h, ptr(dom.wind_alpha), ptr(bs.divs[i]), ptr(dom.density), 1,
-                                               ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt), _capi.MEM_DEVICE,
-                                               C.c_void_p(bs.stream), C.byref(st)), h)
-        seq_each.append(st.solve_ms)
-    q1.record()
-    torch.cuda.synchronize()
-    seq_ms = q0.elapsed_time(q1)
-    for _ in range(args.warmup):
-        bs.step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = lib.hicarw_kernel_launches()
-    torch.cuda.synchronize()
-    e0.record()
-    stats = []
-    for _ in range(args.steps):
-        stats = bs.step()
-    e1.record()
-    torch.cuda.synchronize()
-    launches = lib.hicarw_kernel_launches() - l0
-    clocks = sampler.stop()
-    t_ms = e0.elapsed_time(e1)
-    t_ms = reduce_max(t_ms, dist, f"cuda:{local}")
-    value = world * args.steps * bs.n / (t_ms / 1000.0)
-    # e2e: every subdomain's winds from pinned host memory in, corrected winds out
-    host = [[torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in sv] for sv in bs.saved]
-    for hs, sv in zip(host, bs.saved):
-        for dst, src in zip(hs, sv):
-            dst.copy_(src.cpu())
-    outs = [[torch.empty_like(a) for a in hs] for hs in host]
-    h2d = sum(a.numel() * 4 for hs in host for a in hs)
-
-    def e2e_step():
-        for dom, hs in zip(bs.domains, host):
-            dom.u_dqdt.copy_(hs[0], non_blocking=True)
-            dom.v_dqdt.copy_(hs[1], non_blocking=True)
-            dom.w_dqdt.copy_(hs[2], non_blocking=True)
-        bs.divergence()
-        bs.solve(cold=True)
-        for dom, os_ in zip(bs.domains, outs):
-            os_[0].copy_(dom.u_dqdt, non_blocking=True)
-            os_[1].copy_(dom.v_dqdt, non_blocking=True)
-            os_[2].copy_(dom.w_dqdt, non_blocking=True)
-
-    e2e_step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0.record()
-    e2e_steps = max(1, min(args.steps, 3))
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record()
-    torch.cuda.synchronize()
-    te = e0.elapsed_time(e1)
-    te = reduce_max(te, dist, f"cuda:{local}")
-    e2e_value = world * e2e_steps * bs.n / (te / 1000.0)
-    big = max(range(bs.n), key=lambda i: bs.domains[i].nx * bs.domains[i].ny * bs.domains[i].nz)
-    d_big = bs.domains[big]
-    roofline = profile_roofline(lib, bs.handles[big], stream, False, d_big.nx * d_big.ny * d_big.nz)
-    if roofline:
-        d = bs.domains[big]
-        roofline["profiled_subdomain"] = [d.nx, d.ny, d.nz]
-    iters = [s["iterations"] for s in stats]
-    bs.step()
-    lat = bs.latencies()
-    seq_lat = np.asarray(seq_each)
-    latency = {"batched_p50_ms": float(np.percentile(lat, 50)), "batched_p99_ms": float(np.percentile(lat, 99)),
-               "batched_max_ms": float(lat.max()), "sequential_p50_ms": float(np.percentile(seq_lat, 50)),
-               "sequential_p99_ms": float(np.percentile(seq_lat, 99)),
-               "note": "batched: completion time of each solve from the start of the batch graph; sequential: "
-                       "each subdomain's own calc_iter_winds"}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {bs.n} subdomains, nx,ny in {wl['nxy'][0]}..{wl['nxy'][1]} "
-                                   f"step {wl['nxy'][2]}, nz in {wl['nz'][0]}..{wl['nz'][1]} step {wl['nz'][2]}, "
-                                   f"{bs.cells} cells, {wl['n_hills']} hills each, adv_den={wl['adv_den']}",
-                       "solver": "batched mg (one graph launch per step)", "mg_cycle": cyc, "tol_rel": TOL,
-                       "fields": "f32",
-                       "krylov": "f64", "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms,
-                       "sequential_solves_per_s": bs.n / (seq_ms / 1000.0), "iterations_min": min(iters),
-                       "iterations_max": max(iters), "statuses": sorted(set(s["status"] for s in stats)),
-                       "latency": latency,
-                       "l2": "inputs larger than L2 (coefficients of all subdomains)",
-                       "parallelism": f"{world} ranks x {bs.n} subdomains" if world > 1 else "1 GPU"},
-            "roofline": roofline, "cpu_baseline": None,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-            "clocks": clocks, "gpu_launches": int(launches)}
+    line = batch_measure(args, wl, rank, world, dist, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    bs.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -995,6 +1028,10 @@ def main():
                     help="iterations of the reference method on the workload (reference arm)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baselines")
     ap.add_argument("--no-cpu-c1", action="store_true", help="skip the full CPU solve of the 64x64x20 case")
+    ap.add_argument("--batch-learned-every", type=int, default=4,
+                    help="batch workloads: every m-th subdomain uses the learned preconditioner (0: none)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 96-subdomain batch measurement that the default run adds to its line")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned+mixed FGMRES report (run only when trained parameters are shipped)")
     ap.add_argument("--parity-tol", type=float, default=1e-9,

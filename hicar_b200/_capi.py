@@ -38,6 +38,7 @@ EXPORTS = [
     "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune", "hicarw_batch_latencies",
     "hicarw_calc_w_real", "hicarw_calc_idealized_wgrid", "hicarw_balance_uvw", "hicarw_calc_alpha",
     "hicarw_smooth_alpha", "hicarw_update_stability", "hicarw_debug_wait_timeout",
+    "hicarw_set_kernel_tuning",
 ]
 
 
@@ -155,6 +156,7 @@ def load(path: str = LIB_PATH):
         "hicarw_smooth_alpha": (ci, [vp, vp, ci, ci, ci, vp]),
         "hicarw_update_stability": (ci, [vp, vp, vp, vp, vp, vp, ci, ci, vp, vp, ci, vp]),
         "hicarw_debug_wait_timeout": (ci, [vp, C.c_double, vp]),
+        "hicarw_set_kernel_tuning": (ci, [vp, ci, ci]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -33,9 +33,13 @@ def subdomain_cases(n: int, seed: int = 0, nxy=(96, 512, 32), nz=(20, 48, 4), n_
 
 class BatchSolver:
     """Handles for every case (created, calibrated with the 27-colour probe on the
-    device) and the batch that solves them together."""
+    device) and the batch that solves them together.  learned_every = m > 0
+    solves every m-th subdomain with FGMRES(30) and the composite learned
+    preconditioner (V-cycle + U-Net correction, parameters `learned_params`),
+    the others with `options`."""
 
-    def __init__(self, cases, options: WindOptions | None = None, device="cuda", stream=None):
+    def __init__(self, cases, options: WindOptions | None = None, device="cuda", stream=None,
+                 learned_every: int = 0, learned_params=None):
         torch = _torch()
         self.lib = _capi.load()
         self.options = options or WindOptions(tol_rel=1e-6, wind_solver_iterations=3000,
@@ -43,6 +47,7 @@ class BatchSolver:
         self.adv = bool(self.options.advect_density)
         self.stream = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         self.domains, self.handles, self.divs, self.saved = [], [], [], []
+        self.nets, self.learned = [], []
         self.batch = None
         try:
             for i, case in enumerate(cases):
@@ -60,6 +65,18 @@ class BatchSolver:
                 self.domains.append(dom)
                 self.divs.append(torch.empty((dom.ny, dom.nz, dom.nx), dtype=torch.float32, device=device))
                 self.saved.append((dom.u_dqdt.clone(), dom.v_dqdt.clone(), dom.w_dqdt.clone()))
+                is_learned = learned_every > 0 and learned_params is not None and i % learned_every == learned_every - 1
+                self.learned.append(is_learned)
+                if is_learned:
+                    from . import learned as L
+                    net = L.UNet(dom.nx, dom.ny, dom.nz)
+                    net.set_params(learned_params)
+                    net.attach(h)
+                    self.nets.append(net)
+                    lo = WindOptions(**{**self.options.__dict__, "solver": _capi.SOLVER_FGMRES,
+                                        "precond": _capi.PRECOND_MG_LEARNED, "fgmres_restart": 30,
+                                        "stall_iters": 200, **L.MG_CYCLE})
+                    _capi.check(self.lib.hicarw_set_options(h, C.byref(lo.to_c())), h)
             n = len(self.handles)
             arr = (C.c_void_p * n)(*[h.value for h in self.handles])
             b = C.c_void_p()
@@ -123,6 +140,51 @@ class BatchSolver:
                                                    C.byref(best)))
         return best.value
 
+    def autotune_kernels(self, levels=(8, 16, 32, 64), feeds=(1, 0), reps: int = 2):
+        """Kernel tuning per subdomain-size bucket (nz, and the column count
+        nx * ny in classes of 128 x 128 columns): for the largest subdomain of
+        each bucket, time `reps` solves (device solve time) with every z-march
+        depth of the float4 operator kernels in `levels` and every multigrid
+        post-smoother feed in `feeds` (1 tensor copies, 0 register-fed), and apply
+        the fastest to the whole bucket.  Returns the table
+        [{bucket, subdomains, shape, levels, feed, ms, tried}]."""
+        st = _capi.Stats()
+        buckets = {}
+        for i, d in enumerate(self.domains):
+            buckets.setdefault((d.nz, (d.nx * d.ny) // (128 * 128)), []).append(i)
+        table = []
+        for key in sorted(buckets):
+            idx = buckets[key]
+            rep = max(idx, key=lambda i: self.domains[i].nx * self.domains[i].ny)
+            h, dom = self.handles[rep], self.domains[rep]
+            tried = {}
+            for kc in levels:
+                for feed in feeds:
+                    _capi.check(self.lib.hicarw_set_kernel_tuning(h, kc, feed), h)
+                    ms = []
+                    for _ in range(reps + 1):
+                        dom.set_winds(*self.saved[rep])
+                        self.lib.hicarw_reset_solution(h, C.c_void_p(self.stream))
+                        _capi.check(self.lib.hicarw_calc_divergence(
+                            h, ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt),
+                            ptr(dom.density) if self.adv else None, ptr(self.divs[rep]), int(self.adv), 0, 1,
+                            _capi.MEM_DEVICE, C.c_void_p(self.stream)), h)
+                        _capi.check(self.lib.hicarw_calc_iter_winds(
+                            h, ptr(dom.wind_alpha), ptr(self.divs[rep]), ptr(dom.density) if self.adv else None,
+                            int(self.adv), ptr(dom.u_dqdt), ptr(dom.v_dqdt), ptr(dom.w_dqdt), _capi.MEM_DEVICE,
+                            C.c_void_p(self.stream), C.byref(st)), h)
+                        ms.append(st.solve_ms)
+                    tried[f"{kc}/{feed}"] = min(ms[1:])  # the first solve captures the graphs
+            best = min(tried, key=tried.get)
+            kc, feed = (int(x) for x in best.split("/"))
+            for i in idx:
+                _capi.check(self.lib.hicarw_set_kernel_tuning(self.handles[i], kc, feed), self.handles[i])
+            table.append({"bucket": {"nz": key[0], "columns_over_16384": key[1]}, "subdomains": len(idx),
+                          "shape": [dom.nx, dom.ny, dom.nz], "levels": kc, "feed": feed, "ms": tried[best],
+                          "tried": tried})
+        self.restore_winds()
+        return table
+
     def latencies(self):
         """Per-subdomain solve latency (ms from the batch start) of the last solve."""
         import numpy as np
@@ -145,6 +207,9 @@ class BatchSolver:
         for h in self.handles:
             self.lib.hicarw_finalize_iter_winds(h)
         self.handles = []
+        for net in self.nets:
+            net.close()
+        self.nets = []
 
     def __del__(self):
         try:

@@ -137,6 +137,8 @@ struct hicarw_handle {
     int unet_dirty = 1;   // coefficients changed since the network's operator features were computed
     int use_learned = 0;  // the current solve applies the learned preconditioner
     int use_mglearned = 0; // ... the V-cycle followed by the learned correction of its residual
+    int tune_kc = 0;       // levels per work item of the float4 marching operator kernels (0: default)
+    int tune_mg_feed = -1; // multigrid post-smoother feed: 1 tensor copies, 0 register-fed, -1 the build's choice
     int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
     long long launches_at_call = 0;
@@ -183,6 +185,14 @@ static void mg_params(hicarw_handle *h)
     h->mg.wmask = h->opt.mg_w_levels & ~1;
 }
 
+// The V-cycle of the handle's probed operator, with the tuned post-smoother feed.
+static int mg_build_tuned(hicarw_handle *h, cudaStream_t s)
+{
+    if (mg_build(h->mg, h->d, h->coef, s) != 0) return -1;
+    if (h->tune_mg_feed >= 0) h->mg.use_tma = h->tune_mg_feed;
+    return 0;
+}
+
 static Metrics metrics_of(const hicarw_handle *h)
 {
     Metrics m;
@@ -200,6 +210,7 @@ static OpCtx opctx(const hicarw_handle *h)
     c.coef = h->coef;
     c.bc = h->bc;
     c.probed = h->operator_probed;
+    c.kc = h->tune_kc;
     return c;
 }
 
@@ -594,7 +605,7 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     select_precond(h, allow_mg);
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
         mg_params(h);
-        if (mg_build(h->mg, h->d, h->coef, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
+        if (mg_build_tuned(h, s) != 0) { h->err = "multigrid build failed"; return HICARW_ERR_CUDA; }
         h->mg_dirty = 0;
     }
     if (h->opt.solver == HICARW_SOLVER_FGMRES) return fgmres_solve(h, sweeps, s);
@@ -1266,7 +1277,7 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
     if (!rc && sweeps <= 0) {
         if ((h->mg_dirty || !h->mg.ready) && !(learned && h->opt.precond == HICARW_PRECOND_LEARNED)) {
             mg_params(h);
-            if (mg_build(h->mg, d, h->coef, s) != 0) rc = HICARW_ERR_CUDA;
+            if (mg_build_tuned(h, s) != 0) rc = HICARW_ERR_CUDA;
             else h->mg_dirty = 0;
         }
         if (!rc) {
@@ -1366,7 +1377,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
         h->unet_dirty = 0;
     }
     if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
-        if (mg_build(h->mg, h->d, h->coef, s) != 0) return HICARW_ERR_CUDA;
+        if (mg_build_tuned(h, s) != 0) return HICARW_ERR_CUDA;
         h->mg_dirty = 0;
     }
     FgmresCtx fg;
@@ -1493,6 +1504,19 @@ extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *a
         return HICARW_ERR_ARG;
     launch_calc_alpha(h->d, froude, alpha, halo, (cudaStream_t)stream);
     CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_set_kernel_tuning(hicarw_handle *h, int spmv_levels, int mg_post_feed)
+{
+    if (!h || spmv_levels < 0 || spmv_levels > 1024 || mg_post_feed < -1 || mg_post_feed > 1) return HICARW_ERR_ARG;
+    cudaDeviceSynchronize();
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    h->tune_kc = spmv_levels;
+    h->tune_mg_feed = mg_post_feed;
+    if (mg_post_feed >= 0) h->mg.use_tma = mg_post_feed;
+    else h->mg_dirty = 1; // the build decides again
     return HICARW_OK;
 }
 
@@ -1756,7 +1780,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         select_precond(h, 1);
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
             mg_params(h);
-            if (mg_build(h->mg, h->d, h->coef, s) != 0) {
+            if (mg_build_tuned(h, s) != 0) {
                 fprintf(stderr, "hicarw batch: multigrid build of subdomain %d failed\n", i);
                 return HICARW_ERR_CUDA;
             }

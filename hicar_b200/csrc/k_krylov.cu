@@ -101,9 +101,9 @@ static int march_grid(K *kernel, const Dims &d, int cap)
 }
 
 template <typename K>
-static int march4_grid(K *kernel, const Dims &d, int cap)
+static int march4_grid(K *kernel, const OpCtx &c, int cap)
 {
-    return wave_grid(kernel, march4_items(d), cap);
+    return wave_grid(kernel, march4_items(c), cap);
 }
 
 // ---- the float4 column-marching kernels ----
@@ -138,7 +138,7 @@ void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaS
     ProfScope ps_("spmv", coef_bytes(c.d) + rows(c.d) * 2.0 * sizeof(V), st);
     const int kind = spmv_kind(c);
     if (kind == SPMV_MARCH4)
-        spmv_m4_kernel<V><<<march4_grid(spmv_m4_kernel<V>, c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
+        spmv_m4_kernel<V><<<march4_grid(spmv_m4_kernel<V>, c, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     else if (kind == SPMV_MARCH)
         spmv_march_kernel<V><<<march_grid(spmv_march_kernel<V>, c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
     else spmv_kernel<V><<<row_grid(c.d, 148 * 16), ROWT, 0, st>>>(c, x, y, gate);
@@ -329,7 +329,7 @@ void launch_spmv_sigma(const OpCtx &c, const V *phat, V *v, const V *rhat, Solve
     ProfScope ps_("spmv_sigma", coef_bytes(c.d) + rows(c.d) * 3.0 * sizeof(V), st);
     const int kind = spmv_kind(c);
     if (kind == SPMV_MARCH4)
-        spmv_sigma_m4_kernel<V><<<march4_grid(spmv_sigma_m4_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+        spmv_sigma_m4_kernel<V><<<march4_grid(spmv_sigma_m4_kernel<V>, c, rb.blocks), ROWT, 0, st>>>(
             c, phat, v, rhat, stt, rb.partials);
     else if (kind == SPMV_MARCH)
         spmv_sigma_march_kernel<V><<<march_grid(spmv_sigma_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
@@ -433,7 +433,7 @@ void launch_spmv_dot5(const OpCtx &c, const V *shat, V *t, const V *s, const V *
     ProfScope ps_("spmv_dot5", coef_bytes(c.d) + rows(c.d) * 4.0 * sizeof(V), st);
     const int kind = spmv_kind(c);
     if (kind == SPMV_MARCH4)
-        spmv_dot5_m4_kernel<V><<<march4_grid(spmv_dot5_m4_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(
+        spmv_dot5_m4_kernel<V><<<march4_grid(spmv_dot5_m4_kernel<V>, c, rb.blocks), ROWT, 0, st>>>(
             c, shat, t, s, rhat, stt, hist, rb.partials);
     else if (kind == SPMV_MARCH)
         spmv_dot5_march_kernel<V><<<march_grid(spmv_dot5_march_kernel<V>, c.d, rb.blocks), ROWT, 0, st>>>(

@@ -53,6 +53,7 @@ struct OpCtx {
     const float *coef; // 15 * d.npad
     const BcCol *bc;   // mx * my
     int probed;
+    int kc = 0;        // levels per work item of the float4 column-marching kernels (0: the default)
 };
 
 struct RedBuf {

@@ -268,7 +268,8 @@ namespace hw {
 // ---- float4 column-marching rows of y = A x (probed operator, nx % 4 == 0) ----
 // A lane owns four consecutive interior columns i0 .. i0+3 (i0 = 1 + 4g: a
 // 16-byte aligned group in the padded layout), a warp a strip of 128 columns
-// of one j row, and it marches k upwards over a chunk of at most M4_KC levels.
+// of one j row, and it marches k upwards over a chunk of at most M4_KC levels
+// (OpCtx::kc when set: a tuning knob).
 // Every coefficient and vector row is read with one 16-byte load per lane (a
 // 512-byte segment per warp); x at k-1, k, k+1 of the own row and of the rows
 // j-1 and j+1 stays in registers (three new loads per level); the columns
@@ -304,9 +305,11 @@ __device__ __forceinline__ void st4v(double *__restrict__ p, const double (&v)[4
 }
 
 __host__ __device__ __forceinline__ bool march4_ok(const Dims &d) { return d.nx % 4 == 0 && d.nx >= 4; }
-__host__ __device__ __forceinline__ long long march4_items(const Dims &d)
+__host__ __device__ __forceinline__ int march4_kc(const OpCtx &c) { return c.kc > 0 ? c.kc : M4_KC; }
+__host__ __device__ __forceinline__ long long march4_items(const OpCtx &c)
 {
-    const int G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + M4_KC - 1) / M4_KC;
+    const Dims &d = c.d;
+    const int KC = march4_kc(c), G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + KC - 1) / KC;
     return (long long)d.my * nsx * nkc;
 }
 
@@ -314,7 +317,7 @@ template <typename V, typename F4, typename F1>
 __device__ __forceinline__ void march4_rows(const OpCtx &c, const V *__restrict__ x, F4 &&f4, F1 &&f1)
 {
     const Dims &d = c.d;
-    const int G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + M4_KC - 1) / M4_KC;
+    const int KC = march4_kc(c), G = d.nx / 4, nsx = (G + 31) / 32, nkc = (d.mz + KC - 1) / KC;
     const long long items = (long long)d.my * nsx * nkc;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     const long long P = d.P, PL = d.plane, N = d.npad;
@@ -324,7 +327,7 @@ __device__ __forceinline__ void march4_rows(const OpCtx &c, const V *__restrict_
         const int bx = (int)(rest % nsx), kc = (int)(rest / nsx);
         const int g = bx * 32 + lane;
         const bool live = g < G;
-        const int k0 = kc * M4_KC, k1 = min(k0 + M4_KC, d.mz) - 1;
+        const int k0 = kc * KC, k1 = min(k0 + KC, d.mz) - 1;
         const long long ob = (long long)j * PL + 1 + XO + 4LL * g; // group start at k = 0
         const long long oc = (long long)j * PL + XO;                // column i = 0 at k = 0
         const bool first = live && g == 0, lastg = live && g == G - 1;

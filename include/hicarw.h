@@ -261,6 +261,14 @@ int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms
  * that overlap on the GPU race on the shared array. */
 int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm, void *stream);
 
+/* Kernel tuning of one handle (no counterpart in the reference; the batched
+ * solver's autotuner sets it per subdomain size): spmv_levels = levels per work
+ * item of the float4 column-marching operator kernels (the z-march depth; 0 =
+ * the default 16), mg_post_feed = 1 tensor-copy-fed / 0 register-fed multigrid
+ * post-smoother on the wide levels (-1 = the default choice).  Results do not
+ * depend on either. */
+int hicarw_set_kernel_tuning(hicarw_handle *h, int spmv_levels, int mg_post_feed);
+
 /* Test hook of the bounded device-side waits (no counterpart in the reference):
  * one kernel waits, through the same bounded mbarrier wait as the tensor-copy
  * smoother and the tensor-core convolutions, on a barrier that nothing completes,
