@@ -38,7 +38,8 @@ EXPORTS = [
     "hicarw_batch_calc_iter_winds", "hicarw_batch_autotune", "hicarw_batch_latencies",
     "hicarw_calc_w_real", "hicarw_calc_idealized_wgrid", "hicarw_balance_uvw", "hicarw_calc_alpha",
     "hicarw_smooth_alpha", "hicarw_update_stability", "hicarw_debug_wait_timeout",
-    "hicarw_set_kernel_tuning",
+    "hicarw_set_kernel_tuning", "hicarw_dist_configure", "hicarw_dist_setup", "hicarw_dist_apply",
+    "hicarw_dist_precond", "hicarw_dist_face", "hicarw_dist_spmv", "hicarw_dist_update", "hicarw_dist_state",
 ]
 
 
@@ -157,6 +158,14 @@ def load(path: str = LIB_PATH):
         "hicarw_update_stability": (ci, [vp, vp, vp, vp, vp, vp, ci, ci, vp, vp, ci, vp]),
         "hicarw_debug_wait_timeout": (ci, [vp, C.c_double, vp]),
         "hicarw_set_kernel_tuning": (ci, [vp, ci, ci]),
+        "hicarw_dist_configure": (ci, [vp, ci]),
+        "hicarw_dist_setup": (ci, [vp, vp, vp, ci, vp]),
+        "hicarw_dist_apply": (ci, [vp, ci, vp, ci, vp]),
+        "hicarw_dist_precond": (ci, [vp, ci, vp]),
+        "hicarw_dist_face": (ci, [vp, ci, ci, vp, ci, vp]),
+        "hicarw_dist_spmv": (ci, [vp, ci, vp, ci, vp]),
+        "hicarw_dist_update": (ci, [vp, vp]),
+        "hicarw_dist_state": (ci, [vp, P(ci), P(Stats), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

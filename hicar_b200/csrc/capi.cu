@@ -138,6 +138,8 @@ struct hicarw_handle {
     int use_learned = 0;  // the current solve applies the learned preconditioner
     int use_mglearned = 0; // ... the V-cycle followed by the learned correction of its residual
     int tune_kc = 0;       // levels per work item of the float4 marching operator kernels (0: default)
+    int edges = 0;         // decomposed solve: rank-edge sides of this subdomain (EDGE_* bits)
+    double *dist_buf = nullptr; // decomposed solve: device staging of host-side totals (5 values)
     int tune_mg_feed = -1; // multigrid post-smoother feed: 1 tensor copies, 0 register-fed, -1 the build's choice
     int use_mg = 0;       // preconditioner of the solve being enqueued
     std::string err;
@@ -211,6 +213,7 @@ static OpCtx opctx(const hicarw_handle *h)
     c.bc = h->bc;
     c.probed = h->operator_probed;
     c.kc = h->tune_kc;
+    c.edges = h->edges;
     return c;
 }
 
@@ -393,6 +396,7 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
     if (h->hscan) cudaFreeHost(h->hscan);
     for (int q = 0; q < 2; q++)
         if (h->ev[q]) cudaEventDestroy(h->ev[q]);
+    if (h->dist_buf) cudaFree(h->dist_buf);
     if (h->t0) cudaEventDestroy(h->t0);
     if (h->t1) cudaEventDestroy(h->t1);
     if (h->cap) cudaStreamDestroy(h->cap);
@@ -1504,6 +1508,156 @@ extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *a
         return HICARW_ERR_ARG;
     launch_calc_alpha(h->d, froude, alpha, halo, (cudaStream_t)stream);
     CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+// ---- decomposed solves (the reference's multi-rank BiCGStab, wind_iterative.F90:555-791 with
+// exchange_krylov_halos :1552-1733 and the allreduces :604-729): the library computes, the
+// caller communicates (NCCL, MPI or copies) between the steps ----
+extern "C" int hicarw_dist_configure(hicarw_handle *h, int edges)
+{
+    if (!h || edges < 0 || edges > 15) return HICARW_ERR_ARG;
+    cudaDeviceSynchronize();
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
+    h->graphs.clear();
+    h->edges = edges;
+    if (!h->dist_buf) CK(dalloc((void **)&h->dist_buf, 8 * sizeof(double)));
+    return HICARW_OK;
+}
+
+static int dist_ready(hicarw_handle *h)
+{
+    if (!h || !h->dist_buf || h->opt.solver != HICARW_SOLVER_REFERENCE || h->opt.krylov_precision != HICARW_KRYLOV_F64)
+        return HICARW_ERR_STATE;
+    return 0;
+}
+
+// totals (device dist_tot) -> caller buffer
+static int dist_out(hicarw_handle *h, double *tot, int n, int mem_kind, cudaStream_t s)
+{
+    CK(cudaMemcpyAsync(tot, h->st->dist_tot, n * sizeof(double),
+                       mem_kind == HICARW_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (mem_kind == HICARW_MEM_HOST) CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
+extern "C" int hicarw_dist_setup(hicarw_handle *h, const double *rhs, double *tot3, int mem_kind, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0 || !rhs || !tot3) return rc ? rc : HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    select_precond(h, 1);
+    if (h->use_learned || h->use_mglearned) return HICARW_ERR_STATE;
+    if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
+        mg_params(h);
+        if (mg_build_tuned(h, s) != 0) return HICARW_ERR_CUDA;
+        h->mg_dirty = 0;
+    }
+    if ((rc = ensure_vectors(h, HICARW_KRYLOV_F64)) != 0) return rc;
+    if ((rc = put_padded(h, rhs, V<double>(h, V_RHS), mem_kind, s)) != 0) return rc;
+    launch_diag<double>(h->d, h->coef, h->dz_if, V<double>(h, V_DINV), h->operator_probed, s);
+    launch_zero_rank_edges<double>(h->d, h->edges, V<double>(h, V_DINV), s);
+    launch_state_reset(h->st, h->opt.tol_rel, h->opt.tol_abs, h->opt.max_iters, 0, s);
+    static const int one = 1;
+    CK(cudaMemcpyAsync(&h->st->dist, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    enqueue_setup_prec(h, HICARW_KRYLOV_F64, c, rb, s, 0);
+    return dist_out(h, tot3, 3, mem_kind, s);
+}
+
+extern "C" int hicarw_dist_apply(hicarw_handle *h, int kind, const double *tot, int mem_kind, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    if (kind < 0 || kind > 2 || !tot) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = kind == 0 ? 3 : kind == 1 ? 1 : 5;
+    const double *t = tot;
+    if (mem_kind == HICARW_MEM_HOST) {
+        CK(cudaMemcpyAsync(h->dist_buf, tot, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        t = h->dist_buf;
+    }
+    launch_dist_apply(h->st, h->hist, kind, t, s);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_dist_precond(hicarw_handle *h, int which, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    if (which < 0 || which > 1) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    SolveState *st = h->st;
+    double *r = V<double>(h, V_R), *p = V<double>(h, V_P), *phat = V<double>(h, V_PHAT), *v = V<double>(h, V_V),
+           *sv = V<double>(h, V_S), *shat = V<double>(h, V_SHAT), *Dinv = V<double>(h, V_DINV);
+    if (which == 0) {
+        launch_iteration_begin(st, s);
+        if (h->use_mg) mg_apply<double>(h->mg, p, phat, st, s);
+        else enqueue_precond<double>(h, p, phat, h->precond_n_sweeps, st, 0, s);
+    } else if (h->use_mg) {
+        launch_s_update<double>(h->d, r, v, sv, st, s);
+        mg_apply<double>(h->mg, sv, shat, st, s);
+    } else {
+        OpCtx c = opctx(h);
+        double *pres = V<double>(h, V_PRES);
+        launch_s_precond<double>(h->d, r, v, sv, shat, Dinv, st, s);
+        for (int sw = 2; sw <= h->precond_n_sweeps; sw++) {
+            launch_spmv<double>(c, shat, pres, st, s);
+            launch_rich<double>(h->d, sv, shat, pres, Dinv, st, s);
+        }
+    }
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_dist_face(hicarw_handle *h, int vec, int side, double *buf, int unpack, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    if (vec < 0 || vec > 2 || side < 0 || side > 3 || !buf) return HICARW_ERR_ARG;
+    const int q = vec == 0 ? V_PHAT : vec == 1 ? V_SHAT : V_X;
+    launch_face(h->d, V<double>(h, q), side, buf, unpack != 0, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_dist_spmv(hicarw_handle *h, int which, double *tot, int mem_kind, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    if (which < 0 || which > 1 || !tot) return HICARW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    OpCtx c = opctx(h);
+    RedBuf rb{h->partials, h->red_blocks};
+    SolveState *st = h->st;
+    double *rhat = V<double>(h, V_RHAT), *phat = V<double>(h, V_PHAT), *v = V<double>(h, V_V),
+           *sv = V<double>(h, V_S), *shat = V<double>(h, V_SHAT), *t = V<double>(h, V_T);
+    CK(cudaMemsetAsync(st->dist_tot, 0, 5 * sizeof(double), s)); // a solve that has stopped publishes zeros
+    if (which == 0) launch_spmv_sigma<double>(c, phat, v, rhat, st, rb, s);
+    else launch_spmv_dot5<double>(c, shat, t, sv, rhat, st, h->hist, rb, s);
+    return dist_out(h, tot, which == 0 ? 1 : 5, mem_kind, s);
+}
+
+extern "C" int hicarw_dist_update(hicarw_handle *h, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    double *x = V<double>(h, V_X), *r = V<double>(h, V_R), *p = V<double>(h, V_P), *phat = V<double>(h, V_PHAT),
+           *v = V<double>(h, V_V), *sv = V<double>(h, V_S), *shat = V<double>(h, V_SHAT), *t = V<double>(h, V_T);
+    launch_update_xrp<double, double>(h->d, x, phat, shat, r, sv, t, p, v, h->st, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return HICARW_OK;
+}
+
+extern "C" int hicarw_dist_state(hicarw_handle *h, int *stop, hicarw_stats *stats, void *stream)
+{
+    int rc;
+    if ((rc = dist_ready(h)) != 0) return rc;
+    if ((rc = fetch_state(h, (cudaStream_t)stream)) != 0) return rc;
+    if (stop) *stop = h->hst->stop;
+    if (stats) fill_stats(h, stats, h->precond_n_sweeps, 0);
     return HICARW_OK;
 }
 

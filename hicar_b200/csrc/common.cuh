@@ -81,7 +81,19 @@ struct SolveState {
     int stall_k;    // stall detector window (0 = off)
     int best_it;    // iteration of the best recurrence norm so far
     double best_rn; // best recurrence norm so far
+    int dist;       // decomposed solve: reductions publish their local totals in dist_tot and the
+                    // host applies the scalar steps to the totals summed over all ranks
+    double dist_tot[5];
 };
+
+// Rank-edge sides of a decomposed subdomain (bit mask): their ring cells are
+// halo cells filled by the neighbouring rank, not rows of this rank's system.
+enum { EDGE_W = 1, EDGE_E = 2, EDGE_S = 4, EDGE_N = 8 };
+__host__ __device__ __forceinline__ bool owned_row(const Dims &d, int edges, int i, int j)
+{
+    return !((i == 0 && (edges & EDGE_W)) || (i == d.mx - 1 && (edges & EDGE_E)) || (j == 0 && (edges & EDGE_S)) ||
+             (j == d.my - 1 && (edges & EDGE_N)));
+}
 
 constexpr double BREAKDOWN_EPS = 1.0e-30; // wind_iterative.F90:61
 

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(ROWT) spmv_march_kernel(OpCtx c, const V *__re
 enum { SPMV_ROW = 0, SPMV_MARCH = 1, SPMV_MARCH4 = 2 };
 static int spmv_kind(const OpCtx &c)
 {
-    if (!c.probed) return SPMV_ROW;
+    if (!c.probed || c.edges) return SPMV_ROW; // decomposed subdomains: the row kernels mask the halo rows
     const char *e = getenv("HICARW_SPMV_MARCH");
     if (e && e[0] == '0') return SPMV_ROW;
     if (e && e[0] == '1') return SPMV_MARCH;
@@ -145,6 +145,26 @@ void launch_spmv(const OpCtx &c, const V *x, V *y, const SolveState *gate, cudaS
     count_launch(1);
 }
 
+// rho, the initial norm, the target and the first stopping tests (:602-645) from
+// the set-up dots <r^,r>, <r,r>, <b,b>.
+__device__ __forceinline__ void setup_step(SolveState *stt, double *hist, const double *tot)
+{
+    stt->rho = tot[0];
+    double rn = sqrt(tot[1]);
+    stt->rnorm = rn;
+    stt->res0 = rn;
+    stt->bnorm2 = tot[2];
+    stt->target = fmax(stt->tol_abs, stt->tol_rel * sqrt(tot[2])); // :633
+    stt->omega = 1.0;
+    stt->alpha = 1.0;
+    stt->it = 0;
+    stt->best_rn = rn;
+    stt->best_it = 0;
+    hist[0] = rn;
+    if (rn <= stt->target) { stt->status = 0; stt->stop = 1; stt->halt = 1; }
+    else if (stt->max_iters <= 0) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
+}
+
 // ---- setup: r = b - A x0, r^ = r, p = r, <r^,r>, <r,r>, <b,b> (:585-645) ----
 // X is the type of the solution (FP64 with FP32 vectors and FP64 lambda).
 // restart != 0: a restart of the recurrences from the current solution (the
@@ -166,12 +186,18 @@ __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restric
         r[o] = rv;
         rhat[o] = rv;
         p[o] = rv;
+        if (!owned_row(c.d, c.edges, g.i, g.j)) continue;
         acc[0] += (double)rv * (double)rv; // <r^, r>
         acc[1] += (double)rv * (double)rv; // <r, r>
         acc[2] += bd * bd;                 // <b, b>
     }
     double tot[3];
     if (!grid_reduce<3>(acc, partials, &stt->ticket[0], tot)) return;
+    if (stt->dist) { // decomposed solve: the host sums the ranks' totals and applies setup_step
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 3; q++) stt->dist_tot[q] = tot[q];
+        return;
+    }
     if (threadIdx.x == 0 && restart) {
         const double rn = sqrt(tot[1]);
         stt->rho = tot[0];
@@ -188,22 +214,7 @@ __global__ void __launch_bounds__(ROWT) setup_kernel(OpCtx c, const X *__restric
         else if (stt->it >= stt->max_iters) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
         return;
     }
-    if (threadIdx.x == 0) {
-        stt->rho = tot[0];
-        double rn = sqrt(tot[1]);
-        stt->rnorm = rn;
-        stt->res0 = rn;
-        stt->bnorm2 = tot[2];
-        stt->target = fmax(stt->tol_abs, stt->tol_rel * sqrt(tot[2])); // :633
-        stt->omega = 1.0;
-        stt->alpha = 1.0;
-        stt->it = 0;
-        stt->best_rn = rn;
-        stt->best_it = 0;
-        hist[0] = rn;
-        if (rn <= stt->target) { stt->status = 0; stt->stop = 1; stt->halt = 1; }
-        else if (stt->max_iters <= 0) { stt->status = 1; stt->stop = 1; stt->halt = 1; }
-    }
+    if (threadIdx.x == 0) setup_step(stt, hist, tot);
 }
 
 template <typename V, typename X>
@@ -268,11 +279,14 @@ __global__ void __launch_bounds__(ROWT) spmv_sigma_kernel(OpCtx c, const V *__re
         long long o = kidx(c.d, g.i, g.k, g.j);
         V vv = (V)spmv_row(c, phat, g.i, g.k, g.j);
         v[o] = vv;
-        acc[0] += (double)rhat[o] * (double)vv;
+        if (owned_row(c.d, c.edges, g.i, g.j)) acc[0] += (double)rhat[o] * (double)vv;
     }
     double tot[1];
     if (!grid_reduce<1>(acc, partials, &stt->ticket[1], tot)) return;
-    if (threadIdx.x == 0) sigma_step(stt, tot[0]);
+    if (threadIdx.x == 0) {
+        if (stt->dist) stt->dist_tot[0] = tot[0];
+        else sigma_step(stt, tot[0]);
+    }
 }
 
 // The same with column-marching rows (probed operator).
@@ -353,6 +367,7 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_kernel(OpCtx c, const V *__res
         long long o = kidx(c.d, g.i, g.k, g.j);
         V tv = (V)spmv_row(c, shat, g.i, g.k, g.j);
         t[o] = tv;
+        if (!owned_row(c.d, c.edges, g.i, g.j)) continue;
         double td = (double)tv, sd = (double)sv[o], rd = (double)rhat[o];
         acc[0] += td * sd;
         acc[1] += td * td;
@@ -362,7 +377,11 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_kernel(OpCtx c, const V *__res
     }
     double tot[5];
     if (!grid_reduce<5>(acc, partials, &stt->ticket[2], tot)) return;
-    if (threadIdx.x == 0) dot5_step(stt, hist, tot);
+    if (threadIdx.x == 0) {
+        if (stt->dist)
+            for (int q = 0; q < 5; q++) stt->dist_tot[q] = tot[q];
+        else dot5_step(stt, hist, tot);
+    }
 }
 
 // The same with column-marching rows (probed operator).
@@ -556,6 +575,82 @@ void launch_iteration_begin(SolveState *stt, cudaStream_t st)
     count_launch(1);
 }
 
+// ---- decomposed solve: scalar steps on the totals summed over all ranks ----
+__global__ void dist_apply_kernel(SolveState *stt, double *hist, int kind, const double *__restrict__ tot)
+{
+    double t[5];
+    for (int q = 0; q < 5; q++) t[q] = q < (kind == 0 ? 3 : kind == 1 ? 1 : 5) ? tot[q] : 0.0;
+    if (kind == 0) setup_step(stt, hist, t);
+    else if (kind == 1) {
+        if (!(stt->stop && !stt->profile)) sigma_step(stt, t[0]);
+    } else if (!(stt->stop && !stt->profile)) {
+        double t5[5] = {t[0], t[1], t[2], t[3], t[4]};
+        dot5_step(stt, hist, t5);
+    }
+}
+
+void launch_dist_apply(SolveState *stt, double *hist, int kind, const double *tot, cudaStream_t st)
+{
+    dist_apply_kernel<<<1, 1, 0, st>>>(stt, hist, kind, tot);
+    count_launch(1);
+}
+
+// zero on the halo cells of the rank-edge sides (the preconditioner's zero halo)
+template <typename V>
+__global__ void zero_rank_edges_kernel(Dims d, int edges, V *x)
+{
+    const long long n = (long long)d.mz * d.my;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q % d.mz), j = (int)(q / d.mz);
+        if (edges & EDGE_W) x[kidx(d, 0, k, j)] = (V)0;
+        if (edges & EDGE_E) x[kidx(d, d.mx - 1, k, j)] = (V)0;
+    }
+    const long long m = (long long)d.mz * d.mx;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % d.mx), k = (int)(q / d.mx);
+        if (edges & EDGE_S) x[kidx(d, i, k, 0)] = (V)0;
+        if (edges & EDGE_N) x[kidx(d, i, k, d.my - 1)] = (V)0;
+    }
+}
+
+template <typename V>
+void launch_zero_rank_edges(const Dims &d, int edges, V *x, cudaStream_t st)
+{
+    if (!edges) return;
+    zero_rank_edges_kernel<V><<<64, 256, 0, st>>>(d, edges, x);
+    count_launch(1);
+}
+template void launch_zero_rank_edges<double>(const Dims &, int, double *, cudaStream_t);
+template void launch_zero_rank_edges<float>(const Dims &, int, float *, cudaStream_t);
+
+// faces of a decomposed subdomain: side 0 W / 1 E (column i = 1 / nx owned, i = 0 / nx + 1 halo;
+// (k, j) in Fortran order), 2 S / 3 N (row j = 1 / ny owned, j = 0 / ny + 1 halo; (i, k) order)
+__global__ void face_kernel(Dims d, double *x, int side, double *buf, int unpack)
+{
+    const bool we = side < 2;
+    const long long n = we ? (long long)d.mz * d.my : (long long)d.mx * d.mz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        long long o;
+        if (we) {
+            const int k = (int)(q % d.mz), j = (int)(q / d.mz);
+            const int i = unpack ? (side == 0 ? 0 : d.mx - 1) : (side == 0 ? 1 : d.mx - 2);
+            o = kidx(d, i, k, j);
+        } else {
+            const int i = (int)(q % d.mx), k = (int)(q / d.mx);
+            const int j = unpack ? (side == 2 ? 0 : d.my - 1) : (side == 2 ? 1 : d.my - 2);
+            o = kidx(d, i, k, j);
+        }
+        if (unpack) x[o] = buf[q];
+        else buf[q] = x[o];
+    }
+}
+
+void launch_face(const Dims &d, double *x, int side, double *buf, int unpack, cudaStream_t st)
+{
+    face_kernel<<<64, 256, 0, st>>>(d, x, side, buf, unpack);
+    count_launch(1);
+}
+
 __global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs, int max_iters, int stall_k)
 {
     s->stall_k = stall_k;
@@ -576,6 +671,7 @@ __global__ void state_reset_kernel(SolveState *s, double tol_rel, double tol_abs
     for (int q = 0; q < 8; q++) s->ticket[q] = 0u;
     s->err = 0;
     s->profile = 0;
+    s->dist = 0;
 }
 
 void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, int stall_k, cudaStream_t st)
@@ -599,6 +695,7 @@ __global__ void __launch_bounds__(ROWT) true_residual_kernel(OpCtx c, const X *_
         Seg g = seg_of(c.d, s);
         if (!g.ok) continue;
         long long o = kidx(c.d, g.i, g.k, g.j);
+        if (!owned_row(c.d, c.edges, g.i, g.j)) continue;
         double e = (double)rhs[o] - spmv_row(c, x, g.i, g.k, g.j);
         acc[0] += e * e;
         if (mode >= 1) {
@@ -612,6 +709,10 @@ __global__ void __launch_bounds__(ROWT) true_residual_kernel(OpCtx c, const X *_
     }
     double tot[2];
     if (!grid_reduce<2>(acc, partials, &stt->ticket[3], tot)) return;
+    if (threadIdx.x == 0 && stt->dist && mode == 0) { // decomposed: the local sum of squares, summed by the host
+        stt->dist_tot[0] = tot[0];
+        return;
+    }
     if (threadIdx.x == 0) {
         stt->true_res = sqrt(tot[0]);
         if (mode >= 1) {

@@ -54,6 +54,7 @@ struct OpCtx {
     const BcCol *bc;   // mx * my
     int probed;
     int kc = 0;        // levels per work item of the float4 column-marching kernels (0: the default)
+    int edges = 0;     // rank-edge sides of a decomposed subdomain (EDGE_* bits; 0: one rank)
 };
 
 struct RedBuf {
@@ -86,6 +87,14 @@ void launch_update_xrp(const Dims &d, X *x, const V *phat, const V *shat, V *r, 
                        const V *v, const SolveState *stt, cudaStream_t st);
 void launch_state_reset(SolveState *stt, double tol_rel, double tol_abs, int max_iters, int stall_k, cudaStream_t st);
 void launch_iteration_begin(SolveState *stt, cudaStream_t st);
+// decomposed solve: apply the scalar step of kind 0 (set-up), 1 (sigma) or 2 (five dots) to global totals
+void launch_dist_apply(SolveState *stt, double *hist, int kind, const double *tot, cudaStream_t st);
+// zero a vector on the halo cells of the rank-edge sides (edges bits)
+template <typename V>
+void launch_zero_rank_edges(const Dims &d, int edges, V *x, cudaStream_t st);
+// pack (unpack = 0) the owned boundary face next to `side` (0 W, 1 E, 2 S, 3 N) into buf, or
+// unpack (unpack = 1) buf into the halo face of that side; FP64, (nz+2)(ny+2) or (nz+2)(nx+2) values
+void launch_face(const Dims &d, double *x, int side, double *buf, int unpack, cudaStream_t st);
 template <typename V, typename X>
 void launch_true_residual(const OpCtx &c, const X *x, const V *rhs, V *r_out, const V *rhat, SolveState *stt,
                           int mode, const RedBuf &rb, cudaStream_t st);

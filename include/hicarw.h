@@ -261,6 +261,39 @@ int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms
  * that overlap on the GPU race on the shared array. */
 int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm, void *stream);
 
+/* ---- decomposed solves over several ranks (GPUs) ----
+ * The reference's multi-rank BiCGStab (bicgstab_solve, wind_iterative.F90:555-791,
+ * with exchange_krylov_halos :1552-1733 and the FP64 allreduces of 3, 1 and 5
+ * values :604-729), split at its communication points: the library computes,
+ * the caller communicates (NCCL send/recv and allreduce into its own device
+ * buffers, MPI, or copies), as the reference's own NCCL wrapper does.  One
+ * handle per rank holds the rank's block of the x-y decomposition with a
+ * one-cell ring; hicarw_dist_configure marks the ring sides that border another
+ * rank (bits 1 west, 2 east, 4 south, 8 north): their cells are halo cells,
+ * filled by the caller, excluded from the reductions, and zero inside the
+ * preconditioner (block Jacobi, or a block V-cycle, as :1262-1266).  The
+ * operator comes from hicarw_set_coefs (probed) or calibration; FP64 Krylov
+ * vectors, the reference schedule.  One iteration, with tot the caller's
+ * buffers and "allreduce" the sum over ranks:
+ *   hicarw_dist_setup(rhs) -> allreduce(tot[3]) -> hicarw_dist_apply(0, tot)   (once)
+ *   hicarw_dist_precond(0); exchange faces of p^ (hicarw_dist_face vec 0)
+ *   hicarw_dist_spmv(0) -> allreduce(tot[1]) -> hicarw_dist_apply(1, tot)
+ *   hicarw_dist_precond(1); exchange faces of s^ (vec 1)
+ *   hicarw_dist_spmv(1) -> allreduce(tot[5]) -> hicarw_dist_apply(2, tot)
+ *   hicarw_dist_update(); hicarw_dist_state(&stop) -- until stop.
+ * A face is (nz+2)(ny+2) FP64 values (west/east, side 0/1) or (nx+2)(nz+2)
+ * (south/north, 2/3): pack the owned face next to a side (unpack = 0) into the
+ * buffer sent to that neighbour, unpack (1) what it sent into that side's halo.
+ * tot pointers follow mem_kind; the solution is read with hicarw_get_lambda. */
+int hicarw_dist_configure(hicarw_handle *h, int edges);
+int hicarw_dist_setup(hicarw_handle *h, const double *rhs, double *tot3, int mem_kind, void *stream);
+int hicarw_dist_apply(hicarw_handle *h, int kind, const double *tot, int mem_kind, void *stream);
+int hicarw_dist_precond(hicarw_handle *h, int which, void *stream);
+int hicarw_dist_face(hicarw_handle *h, int vec, int side, double *buf, int unpack, void *stream);
+int hicarw_dist_spmv(hicarw_handle *h, int which, double *tot, int mem_kind, void *stream);
+int hicarw_dist_update(hicarw_handle *h, void *stream);
+int hicarw_dist_state(hicarw_handle *h, int *stop, hicarw_stats *stats, void *stream);
+
 /* Kernel tuning of one handle (no counterpart in the reference; the batched
  * solver's autotuner sets it per subdomain size): spmv_levels = levels per work
  * item of the float4 column-marching operator kernels (the z-march depth; 0 =
