@@ -127,7 +127,9 @@ def _timed_solve(wi, step, kw):
 def pick_cycle(wi, step, base: dict):
     """Two solves of the workload with each cycle of MG_CYCLES (the second one
     timed), then the fastest of them once more with FP32 Krylov vectors and
-    FP64 lambda, and the faster of those with graphs of 4 iterations.  Returns
+    FP64 lambda, the faster of those with the finest level's smoother
+    coefficients in BF16 (cycles without fine pre-smoothing), and the fastest
+    so far with graphs of 4 iterations.  Returns
     the options of the fastest candidate that converged with the multigrid
     preconditioner (no fallback) and, for the FP32-vector one, whose FP64 true
     residual meets the tolerance; its name; and the table of times (ms; None
@@ -143,8 +145,11 @@ def pick_cycle(wi, step, base: dict):
         best_ms = table[best]
         # the same cycle with FP32 Krylov vectors and FP64 lambda, then with
         # graphs of 4 iterations (fewer launched past convergence when few are needed)
-        for tag, extra, accurate in (("f32-vectors", {"krylov_precision": KRYLOV_F32_X64}, True),
-                                     ("chunk4", {"check_every": 4}, False)):
+        trials = [("f32-vectors", {"krylov_precision": KRYLOV_F32_X64}, True)]
+        if kw.get("mg_skip_fine_presmooth"):  # BF16 coefficients of the finest level's post-smoother
+            trials.append(("bf16-smoother", {"mg_precision": 1}, True))
+        trials.append(("chunk4", {"check_every": 4}, False))
+        for tag, extra, accurate in trials:
             trial = {**kw, **extra}
             ms, st = _timed_solve(wi, step, trial)
             ok = st["status"] == 0 and st["precond"] == 1
@@ -798,10 +803,13 @@ def run_ours(args, wl):
                         acc_keys[f"{tag}{name}_lambda_rel_l2"] = r_["lambda_rel_l2"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if opt.krylov_precision == 0 else "f32+f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": ("f64" if opt.krylov_precision == 0 else "f32+f64") + ("+bf16" if opt.mg_precision else ""),
+            "data": "synthetic",
             "config": {"workload": workload_name(args, wl),
                        "solver": args.solver, "mg_cycle_name": (cycle or {}).get("chosen"), "mg_cycle": cycle,
                        "tol_rel": TOL, "fields": "f32", "krylov": krylov_desc(opt),
+                       "preconditioner_precision": ("bf16 coefficients in the finest level's smoother, f32 elsewhere"
+                                                    if opt.mg_precision else "f32"),
                        "iterations": it[0], "ref_method_iterations": ref_iters, "true_res_rel": max(tr),
                        "plain_gpu_solves_per_s": 1000.0 / plain_ms,
                        "speedup_vs_plain_gpu": value / world / (1000.0 / plain_ms),

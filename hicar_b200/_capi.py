@@ -58,7 +58,7 @@ class Options(C.Structure):
                 ("replace_every", C.c_int), ("check_every", C.c_int), ("precond", C.c_int),
                 ("stall_iters", C.c_int), ("mg_omega", C.c_float), ("fgmres_restart", C.c_int),
                 ("mg_coarse_scale", C.c_float), ("mg_skip_fine_presmooth", C.c_int),
-                ("mg_w_levels", C.c_int)]
+                ("mg_w_levels", C.c_int), ("mg_precision", C.c_int)]
 
 
 METRIC_FIELDS = ["jacobian", "jacobian_u", "jacobian_v", "jacobian_w", "dzdx", "dzdy", "dzdx_u", "dzdy_v",

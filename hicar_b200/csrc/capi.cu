@@ -176,6 +176,7 @@ extern "C" void hicarw_default_options(hicarw_options *o)
     o->mg_coarse_scale = 1.35f; // over-correction of the aggregation coarse grid: 35 -> 25 iterations at 512x512x48
     o->mg_skip_fine_presmooth = 0;
     o->mg_w_levels = 0;
+    o->mg_precision = 0;
 }
 
 // V-cycle parameters from the options (read when its launches are enqueued).
@@ -185,6 +186,9 @@ static void mg_params(hicarw_handle *h)
     h->mg.cscale = h->opt.mg_coarse_scale > 0.0f ? h->opt.mg_coarse_scale : 1.35f;
     h->mg.pre0 = h->opt.mg_skip_fine_presmooth ? 0 : 1;
     h->mg.wmask = h->opt.mg_w_levels & ~1;
+    const int bf16 = h->opt.mg_precision == 1;
+    if (bf16 != h->mg.bf16) h->mg_dirty = 1; // the finest level's factors and BF16 copy change
+    h->mg.bf16 = bf16;
 }
 
 // The V-cycle of the handle's probed operator, with the tuned post-smoother feed.
@@ -294,6 +298,7 @@ static int normalize_options(hicarw_options *o)
         o->criterion = HICARW_CRIT_TRUE;
     }
     if (o->solver != HICARW_SOLVER_REFERENCE && o->solver != HICARW_SOLVER_FGMRES) return HICARW_ERR_ARG;
+    if (o->mg_precision < 0 || o->mg_precision > 1) return HICARW_ERR_ARG;
     if (o->check_every <= 0) o->check_every = 8;
     if (o->replace_every <= 0) o->replace_every = 50;
     return 0;

@@ -17,6 +17,7 @@
 // vectors it reads and writes stay FP64.  The V-cycle is a fixed linear map
 // (deterministic kernels, fixed level count), so plain BiCGStab applies.
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 #include <stdlib.h>
 
@@ -78,7 +79,14 @@ __global__ void galerkin_kernel(Dims f, const float *__restrict__ cf, Dims c, fl
 
 // ---- Thomas factors of each column's tridiagonal (C, A, B), couplings to the
 // ghost planes dropped: minv_k = 1/(A_k - C_k cp_{k-1}), cp_k = B_k minv_k ----
-__global__ void factor_kernel(Dims d, const float *__restrict__ coef, float *__restrict__ cp, float *__restrict__ minv)
+__device__ __forceinline__ double fac_operand(float v, int bf16)
+{
+    return bf16 ? (double)__bfloat162float(__float2bfloat16_rn(v)) : (double)v;
+}
+
+// bf16 != 0: the factors of the BF16-rounded tridiagonal (the smoother stores its coefficients in BF16)
+__global__ void factor_kernel(Dims d, const float *__restrict__ coef, float *__restrict__ cp, float *__restrict__ minv,
+                              int bf16)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y + 1;
@@ -86,9 +94,9 @@ __global__ void factor_kernel(Dims d, const float *__restrict__ coef, float *__r
     double cprev = 0.0;
     for (int k = 1; k <= d.nz; k++) {
         long long o = kidx(d, i, k, j);
-        double a = k > 1 ? (double)coef[(long long)CC * d.npad + o] : 0.0;
-        double b = (double)coef[(long long)CA * d.npad + o];
-        double c = k < d.nz ? (double)coef[(long long)CB * d.npad + o] : 0.0;
+        double a = k > 1 ? fac_operand(coef[(long long)CC * d.npad + o], bf16) : 0.0;
+        double b = fac_operand(coef[(long long)CA * d.npad + o], bf16);
+        double c = k < d.nz ? fac_operand(coef[(long long)CB * d.npad + o], bf16) : 0.0;
         double den = b - a * cprev;
         if (fabs(den) < 1e-30) den = copysign(1e-30, den);
         double m = 1.0 / den;
@@ -178,11 +186,21 @@ __device__ __forceinline__ double stencil_smem(const float *__restrict__ coef, l
     return y;
 }
 
-// The 15 coefficients of a row, loaded together (independent loads in flight).
+// The 15 coefficients of a row, loaded together (independent loads in flight);
+// FP32 or BF16 storage (the finest level's smoother coefficients in BF16).
+__device__ __forceinline__ float coef_val(float v) { return v; }
+__device__ __forceinline__ float coef_val(__nv_bfloat16 v) { return __bfloat162float(v); }
+
 __device__ __forceinline__ void load_coefs(const float *__restrict__ coef, long long npad, long long o, float (&cv)[15])
 {
 #pragma unroll
     for (int q = 0; q < 15; q++) cv[q] = __ldg(coef + o + (long long)q * npad);
+}
+__device__ __forceinline__ void load_coefs(const __nv_bfloat16 *__restrict__ coef, long long npad, long long o,
+                                           float (&cv)[15])
+{
+#pragma unroll
+    for (int q = 0; q < 15; q++) cv[q] = __bfloat162float(__ldg(coef + o + (long long)q * npad));
 }
 
 template <int SX, int SP>
@@ -279,8 +297,8 @@ __device__ __forceinline__ void stage_window(const Dims &d, const float *__restr
 // tile and its one-column ring staged in shared memory first.
 constexpr int POST_CELLS = 4; // (column, level) residuals per thread in flight; 3 CTAs per SM by registers
 
-template <typename TR, typename TO, int TX, int TY>
-__global__ void __launch_bounds__(MG_THREADS, 3) post_kernel(Dims d, const float *__restrict__ coef,
+template <typename TR, typename TO, int TX, int TY, typename CT = float>
+__global__ void __launch_bounds__(MG_THREADS, 3) post_kernel(Dims d, const CT *__restrict__ coef,
                                                           const float *__restrict__ cp,
                                                           const float *__restrict__ minv, const TR *__restrict__ r,
                                                           const float *__restrict__ x1, Dims dc,
@@ -362,30 +380,34 @@ constexpr int WX = TX + 2;              // x2 window row: i0-1 .. i0+TX
 constexpr int WK = KC + 2;              // window levels: k0-1 .. k0+KC
 constexpr int X1W = TX + 8;             // staged x1 row: i0-4 .. i0+TX+3 (16-byte aligned start)
 constexpr int XCW = 24;                 // staged coarse row: I0-3 .. I0+20, I0 = i0 >> 1
-constexpr int B_COEF = 15 * KC * TX * 4;
+template <typename CT> constexpr int b_coef() { return 15 * KC * TX * (int)sizeof(CT); }
 constexpr int B_ROW = KC * TX * 4;      // minv / cp
 constexpr int B_X1 = 3 * WK * X1W * 4;
 constexpr int B_XC = 2 * WK * XCW * 4;
 constexpr int up128(int b) { return (b + 127) / 128 * 128; }
-constexpr int O_COEF = 0;
-constexpr int O_MINV = O_COEF + B_COEF;
-constexpr int O_CP = O_MINV + B_ROW;
-constexpr int O_X1 = O_CP + B_ROW;
-constexpr int O_XC = O_X1 + up128(B_X1);
-constexpr int O_R = O_XC + up128(B_XC);
-template <typename TR> constexpr int stage_bytes() { return O_R + up128(KC * TX * (int)sizeof(TR)); }
-template <typename TR> constexpr uint32_t tx_bytes() { return B_COEF + 2 * B_ROW + B_X1 + B_XC + KC * TX * sizeof(TR); }
-static_assert(B_COEF % 128 == 0 && B_ROW % 128 == 0, "stage offsets must stay 128-byte aligned");
+// stage offsets for coefficient type CT
+template <typename CT> constexpr int o_minv() { return b_coef<CT>(); }
+template <typename CT> constexpr int o_cp() { return o_minv<CT>() + B_ROW; }
+template <typename CT> constexpr int o_x1() { return o_cp<CT>() + B_ROW; }
+template <typename CT> constexpr int o_xc() { return o_x1<CT>() + up128(B_X1); }
+template <typename CT> constexpr int o_r() { return o_xc<CT>() + up128(B_XC); }
+template <typename TR, typename CT> constexpr int stage_bytes() { return o_r<CT>() + up128(KC * TX * (int)sizeof(TR)); }
+template <typename TR, typename CT> constexpr uint32_t tx_bytes()
+{
+    return b_coef<CT>() + 2 * B_ROW + B_X1 + B_XC + KC * TX * sizeof(TR);
+}
+static_assert(b_coef<float>() % 128 == 0 && b_coef<__nv_bfloat16>() % 128 == 0 && B_ROW % 128 == 0,
+              "stage offsets must stay 128-byte aligned");
 
 // dynamic shared memory of a launch for nz levels
-template <typename TR> size_t smem_bytes(int nz)
+template <typename TR, typename CT> size_t smem_bytes(int nz)
 {
-    return 128 + (size_t)NS * stage_bytes<TR>() + (size_t)3 * nz * TX * 4 + (size_t)up128(3 * WK * WX * 4) +
+    return 128 + (size_t)NS * stage_bytes<TR, CT>() + (size_t)3 * nz * TX * 4 + (size_t)up128(3 * WK * WX * 4) +
            2 * NS * 8 + 16;
 }
 }  // namespace pt
 
-template <typename TR, typename TO>
+template <typename TR, typename TO, typename CT = float>
 __global__ void __launch_bounds__(pt::THREADS, 2)
     post_tma_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
                     const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
@@ -394,7 +416,9 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
                     int *err)
 {
     using namespace pt;
-    constexpr int SB = stage_bytes<TR>();
+    constexpr int SB = stage_bytes<TR, CT>();
+    constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(), O_XC = o_xc<CT>(),
+                  O_R = o_r<CT>();
     extern __shared__ unsigned char pt_smem[];
     unsigned char *base = (unsigned char *)(((uintptr_t)pt_smem + 127) & ~(uintptr_t)127);
     const int nz = d.nz, nch = (nz + KC - 1) / KC;
@@ -432,7 +456,7 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
                 }
                 unsigned char *st = base + s * SB;
                 const int k0 = 1 + ch * KC, row = j * d.mz + k0;
-                tc::mbar_expect_tx(&full[s], tx_bytes<TR>());
+                tc::mbar_expect_tx(&full[s], tx_bytes<TR, CT>());
                 tc::tma_load_3d(st + O_COEF, &tm_coef, i0 + XO, row, 0, &full[s]);
                 tc::tma_load_2d(st + O_MINV, &tm_minv, i0 + XO, row, &full[s]);
                 tc::tma_load_2d(st + O_CP, &tm_cp, i0 + XO, row, &full[s]);
@@ -481,10 +505,10 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
                 const int t = (k - 1) * TX + lane;
                 float res = 0.0f, x2c = 0.0f, cpv = 0.0f;
                 if (col) {
-                    const float *sco = (const float *)(st + O_COEF);
+                    const CT *sco = (const CT *)(st + O_COEF);
                     float cv[15];
 #pragma unroll
-                    for (int q = 0; q < 15; q++) cv[q] = sco[(q * KC + warp) * TX + lane];
+                    for (int q = 0; q < 15; q++) cv[q] = coef_val(sco[(q * KC + warp) * TX + lane]);
                     const float *xs = s_x2w + (WK + warp + 1) * WX + lane + 1;
                     const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
                     res = (float)(rv - stencil_regs<WK * WX, WX>(cv, xs));
@@ -498,14 +522,15 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
             tc::named_sync(1, CW);
             if (warp == 0) { // forward recurrence over the chunk, then release the stage
                 if (col) {
-                    const float *sco = (const float *)(st + O_COEF), *smv = (const float *)(st + O_MINV);
+                    const CT *sco = (const CT *)(st + O_COEF);
+                    const float *smv = (const float *)(st + O_MINV);
                     float rv[KC], cv[KC], mv[KC];
 #pragma unroll
                     for (int u = 0; u < KC; u++) {
                         const int kq = k0 + u;
                         const bool v = kq <= nz;
                         rv[u] = v ? s_res[(kq - 1) * TX + lane] : 0.0f;
-                        cv[u] = v && kq > 1 ? sco[(CC * KC + u) * TX + lane] : 0.0f;
+                        cv[u] = v && kq > 1 ? coef_val(sco[(CC * KC + u) * TX + lane]) : 0.0f;
                         mv[u] = v ? smv[u * TX + lane] : 0.0f;
                     }
 #pragma unroll
@@ -859,12 +884,20 @@ void mg_free(Mg &mg)
     mg.ready = 0;
     if (mg.err) cudaFree(mg.err);
     mg.err = nullptr;
+    if (mg.coef0h) cudaFree(mg.coef0h);
+    mg.coef0h = nullptr;
 }
 
 static int sm_count();
 static int smem_optin();
 static void fused_setup(Mg &mg);
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+__global__ void bf16_copy_kernel(const float *__restrict__ in, __nv_bfloat16 *__restrict__ out, size_t n)
+{
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        out[q] = __float2bfloat16_rn(in[q]);
+}
 
 int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
 {
@@ -925,8 +958,19 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
             count_launch(1);
         }
         dim3 b(64), g((L.d.nx + 63) / 64, L.d.ny);
-        factor_kernel<<<g, b, 0, s>>>(L.d, L.coef, L.cp, L.minv);
+        factor_kernel<<<g, b, 0, s>>>(L.d, L.coef, L.cp, L.minv, l == 0 && mg.bf16 && !mg.pre0);
         count_launch(1);
+    }
+    // the finest level's smoother coefficients in BF16 (V(0,1) cycles: its post-smoother is the only
+    // kernel that reads them)
+    if (mg.bf16 && !mg.pre0 && mg.nlev > 0) {
+        const size_t n = 15 * (size_t)mg.lev[0].d.npad;
+        if (!mg.coef0h && cudaMalloc((void **)&mg.coef0h, n * sizeof(__nv_bfloat16)) != cudaSuccess) return -1;
+        bf16_copy_kernel<<<(int)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(mg.lev[0].coef, mg.coef0h, n);
+        count_launch(1);
+    } else if (mg.coef0h) {
+        cudaFree(mg.coef0h);
+        mg.coef0h = nullptr;
     }
     const cudaError_t e = cudaGetLastError();
     fused_setup(mg);
@@ -975,15 +1019,15 @@ static void launch_pre(const MgLevel &L, int level, const TR *r, float *out, flo
     count_launch(1);
 }
 
-template <typename TR, typename TO, int TX, int TY>
-static void post_t(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, float omega, float cscale,
-                   const SolveState *gate, cudaStream_t s)
+template <typename TR, typename TO, int TX, int TY, typename CT = float>
+static void post_t(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
+                   float cscale, const SolveState *gate, cudaStream_t s)
 {
     dim3 g((L.d.nx + TX - 1) / TX, (L.d.ny + TY - 1) / TY);
     size_t smem = ((size_t)4 * TX * TY * L.d.nz + (size_t)(TX + 2) * (TY + 2) * (L.d.nz + 2)) * sizeof(float);
-    set_smem(post_kernel<TR, TO, TX, TY>, smem);
-    post_kernel<TR, TO, TX, TY><<<g, MG_THREADS, smem, s>>>(L.d, L.coef, L.cp, L.minv, r, L.x1, C.d, C.x3, out,
-                                                            omega, cscale, gate);
+    set_smem(post_kernel<TR, TO, TX, TY, CT>, smem);
+    post_kernel<TR, TO, TX, TY, CT><<<g, MG_THREADS, smem, s>>>(L.d, coef, L.cp, L.minv, r, L.x1, C.d, C.x3, out,
+                                                                omega, cscale, gate);
 }
 
 static std::atomic<long long> g_tma_posts{0};
@@ -1049,16 +1093,17 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, cuuint32_t rank, co
 // conditions do not hold: shared memory for nz levels, 16-byte aligned arrays
 // and row pitches.  Box x coordinates: i0 + XO = 32 bx + 8, i0 + XO - 4 and
 // (i0 >> 1) + XO - 3 = 16 bx + 4, all multiples of 4 floats (2 doubles).
-template <typename TR, typename TO>
-static bool post_tma(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, float omega, float cscale,
-                     const SolveState *gate, int *err, cudaStream_t s)
+template <typename TR, typename TO, typename CT = float>
+static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
+                     float cscale, const SolveState *gate, int *err, cudaStream_t s)
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const size_t smem = smem_bytes<TR>(d.nz);
+    const size_t smem = smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
-    const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15}, sco[2] = {(cuuint64_t)d.P * 4, (cuuint64_t)d.npad * 4};
+    const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
+                     sco[2] = {(cuuint64_t)d.P * sizeof(CT), (cuuint64_t)d.npad * sizeof(CT)};
     const cuuint64_t drow[2] = {(cuuint64_t)d.P, rows}, srow[1] = {(cuuint64_t)d.P * 4},
                      srr[1] = {(cuuint64_t)d.P * sizeof(TR)};
     const cuuint64_t dx1[3] = {(cuuint64_t)d.P, (cuuint64_t)d.mz, (cuuint64_t)d.my},
@@ -1068,30 +1113,37 @@ static bool post_tma(const MgLevel &L, const TR *r, const MgLevel &C, TO *out, f
     const cuuint32_t bco[3] = {TX, KC, 15}, brow[2] = {TX, KC}, bx1[3] = {X1W, WK, 3}, bxc[3] = {XCW, WK, 2};
     const CUtensorMapDataType f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const CUtensorMapDataType fr = sizeof(TR) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const CUtensorMapDataType fc = sizeof(CT) == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     CUtensorMap m[6];
-    if (!make_map(&m[0], f32, 3, L.coef, dco, sco, bco) || !make_map(&m[1], f32, 2, L.minv, drow, srow, brow) ||
+    if (!make_map(&m[0], fc, 3, coef, dco, sco, bco) || !make_map(&m[1], f32, 2, L.minv, drow, srow, brow) ||
         !make_map(&m[2], f32, 2, L.cp, drow, srow, brow) || !make_map(&m[3], fr, 2, r, drow, srr, brow) ||
         !make_map(&m[4], f32, 3, L.x1, dx1, sx1, bx1) || !make_map(&m[5], f32, 3, C.x3, dxc, sxc, bxc))
         return false;
     const int ntx = (d.nx + TX - 1) / TX, ntiles = ntx * d.ny;
     const int grid = std::min(ntiles, 2 * sm_count());
-    cudaFuncSetAttribute(post_tma_kernel<TR, TO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(post_tma_kernel<TR, TO, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int *e = gate ? const_cast<int *>(&gate->err) : err;
-    post_tma_kernel<TR, TO><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega, cscale,
-                                                        ntx, ntiles, gate, e);
+    post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
+                                                            cscale, ntx, ntiles, gate, e);
     g_tma_posts++;
     return true;
 }
 
+// coefh: the level's coefficients in BF16 (the finest level with mg_precision BF16), else nullptr
 template <typename TR, typename TO>
 static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel &C, TO *out, float omega,
-                        float cscale, const SolveState *gate, int use_tma, int *err, cudaStream_t s)
+                        float cscale, const SolveState *gate, int use_tma, int *err, cudaStream_t s,
+                        const __nv_bfloat16 *coefh = nullptr)
 {
     const double N = (double)L.d.nx * L.d.ny * L.d.nz;
-    ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + 60.0 + 4.0 + 1.0 + 8.0) * N, s);
-    if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, r, C, out, omega, cscale, gate, s);
-    else if (!(use_tma && post_tma<TR, TO>(L, r, C, out, omega, cscale, gate, err, s)))
-        post_t<TR, TO, 32, 1>(L, r, C, out, omega, cscale, gate, s);
+    ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + (coefh ? 30.0 : 60.0) + 4.0 + 1.0 + 8.0) * N, s);
+    if (coefh) {
+        if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, coefh, r, C, out, omega, cscale, gate, s);
+        else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s)))
+            post_t<TR, TO, 32, 1>(L, coefh, r, C, out, omega, cscale, gate, s);
+    } else if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, L.coef, r, C, out, omega, cscale, gate, s);
+    else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s)))
+        post_t<TR, TO, 32, 1>(L, L.coef, r, C, out, omega, cscale, gate, s);
     count_launch(1);
 }
 
@@ -1332,7 +1384,8 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     launch_restrict_pre<V>(F, in, C, 1, last ? C.x3 : C.x1, last ? 1.0f : w, gate, s, !mg.pre0);
     MgLevel Cr = C;
     Cr.x3 = const_cast<float *>(coarse_cycle(mg, 1, gate, s));
-    launch_post<V, V>(F, 0, in, Cr, out, w, mg.cscale, gate, mg.use_tma, mg.err, s);
+    launch_post<V, V>(F, 0, in, Cr, out, w, mg.cscale, gate, mg.use_tma, mg.err, s,
+                      mg.pre0 ? nullptr : mg.coef0h);
 }
 
 template void mg_apply<double>(const Mg &, const double *, double *, const SolveState *, cudaStream_t);

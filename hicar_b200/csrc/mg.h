@@ -1,5 +1,7 @@
 // mg.h -- multigrid V-cycle preconditioner (k_mg.cu).
 #pragma once
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace hw {
@@ -27,6 +29,9 @@ struct Mg {
     int fuse_level = 0;  // first level of the coarse part run by one thread-block cluster (0: every level its own
                          // launches; HICARW_MG_FUSE=0 at build time)
     int cluster_n = 0;   // CTAs of that cluster
+    int bf16 = 0;        // the finest level's smoother coefficients in BF16 (V(0,1) cycles; factors of the rounded
+                         // tridiagonal)
+    __nv_bfloat16 *coef0h = nullptr; // those coefficients (15 * npad)
     int *err = nullptr;  // device flag: a bounded copy wait of a smoother timed out (calls without a solve state)
     MgLevel lev[MG_MAX_LEVELS];
 };

@@ -55,6 +55,7 @@ class WindOptions:
     mg_coarse_scale: float = 1.35          # V-cycle over-correction of the aggregation coarse grid
     mg_skip_fine_presmooth: bool = False   # V-cycle: V(0,1) on the finest level (no pre-smoothing there)
     mg_w_levels: tuple = ()                # levels (>= 1) that correct twice from the coarse grid (W-cycle)
+    mg_precision: int = 0                  # 1: BF16 coefficients of the finest level's post-smoother (V(0,1))
 
     def to_c(self) -> _capi.Options:
         o = _capi.default_options()
@@ -74,6 +75,7 @@ class WindOptions:
         o.mg_coarse_scale = float(self.mg_coarse_scale)
         o.mg_skip_fine_presmooth = int(bool(self.mg_skip_fine_presmooth))
         o.mg_w_levels = sum(1 << int(l) for l in self.mg_w_levels if 1 <= int(l) < 31)
+        o.mg_precision = int(self.mg_precision)
         return o
 
 

@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define HICARW_ABI_VERSION 1
+#define HICARW_ABI_VERSION 2
 
 enum {
     HICARW_OK = 0,
@@ -128,6 +128,9 @@ typedef struct hicarw_options {
                                    smoother and one operator pass fewer per cycle) */
     int mg_w_levels;      /* V-cycle: bit l (l >= 1) makes level l correct twice from its coarse grid
                              (a W-cycle on those levels; bit 0 is ignored); 0 = V-cycle (default) */
+    int mg_precision;     /* V-cycle coefficient storage: 0 = FP32 (default); 1 = BF16 for the finest level's
+                             post-smoother (with mg_skip_fine_presmooth = 1, the only kernel that reads them;
+                             its Thomas factors are those of the BF16-rounded tridiagonal; FP32 arithmetic) */
 } hicarw_options;
 
 /* Domain fields the solver reads (domain%vars_3d / vars_2d / mapfac_*),

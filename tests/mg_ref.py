@@ -109,13 +109,20 @@ def post(C, cp, mi, r, x2, omega):
     return x2.astype(np.float64) + float(omega) * y.astype(np.float64)
 
 
+def bf16_round(a):
+    """FP32 values rounded to the nearest BF16 (ties to even), kept as FP32."""
+    u = np.asarray(a, f32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(f32)
+
+
 class VCycle:
     """fine_presmooth=False: V(0,1) on the finest level (its x1 is zero, level 1
     restricts the input itself).  wlevels: levels (>= 1) that correct twice from
     their coarse grid per visit (W-cycle there): the second restriction takes the
     residual of the first post-smoothed iterate, stored in FP32 as on the GPU."""
 
-    def __init__(self, coefs, omega=0.8, cscale=1.35, fine_presmooth=True, wlevels=()):
+    def __init__(self, coefs, omega=0.8, cscale=1.35, fine_presmooth=True, wlevels=(), fine_bf16=False):
         self.omega = omega
         self.cscale = cscale
         self.fine_presmooth = fine_presmooth
@@ -123,6 +130,8 @@ class VCycle:
         self.lev = [np.asarray(coefs, f32)]
         while self.lev[-1].shape[1] > 1 or self.lev[-1].shape[3] > 1:
             self.lev.append(coarsen(self.lev[-1]))
+        if fine_bf16:  # the finest level's smoother coefficients (and factors) in BF16; coarse grids from FP32
+            self.lev[0] = bf16_round(self.lev[0])
         self.fac = [factors(C) for C in self.lev]
 
     @staticmethod

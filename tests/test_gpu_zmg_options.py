@@ -322,3 +322,61 @@ def test_fused_coarse_cycle_solve(case, monkeypatch):
     assert res["1"][0]["status"] == 0
     assert res["1"][0]["iterations"] == res["0"][0]["iterations"]
     np.testing.assert_array_equal(res["1"][1], res["0"][1])
+
+
+@pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13)])
+def test_vcycle_bf16_finest_smoother(shape, monkeypatch):
+    """mg_precision = 1: the finest level's post-smoother reads its coefficients
+    in BF16 (tensor-copy and register-fed kernels alike, bit-identical) and
+    solves the BF16-rounded tridiagonal; against the numpy restatement with the
+    same rounding, V(0,1) with W on levels 2-3."""
+    import mg_ref
+    from hicar_b200 import wind, wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=33, adv_den=True, n_hills=10)
+    rng = np.random.default_rng(37)
+    x = np.zeros((ny + 2, nz + 2, nx + 2))
+    x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
+    cyc = dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3))
+    out = {}
+    for tma in ("1", "0"):
+        monkeypatch.setenv("HICARW_MG_TMA", tma)
+        wi.finalize_iter_winds()
+        wind.reset()
+        dom, _, _, _ = _calibrated(case)
+        h = wi.handle(dom.nest_indx)
+        wi.set_options(wi.WindOptions(mg_precision=1, **cyc))
+        y = np.empty_like(x)
+        _capi.check(_capi.load().hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
+        out[tma] = y
+        coefs = _coefs(dom)
+    np.testing.assert_array_equal(out["1"], out["0"])
+    want = mg_ref.VCycle(coefs, 1.0, fine_presmooth=False, wlevels=(2, 3), fine_bf16=True)(x[1:-1, 1:-1, 1:-1])
+    assert _rel(out["1"][1:-1, 1:-1, 1:-1], want) < 1e-5
+    f32 = mg_ref.VCycle(coefs, 1.0, fine_presmooth=False, wlevels=(2, 3))(x[1:-1, 1:-1, 1:-1])
+    assert _rel(out["1"][1:-1, 1:-1, 1:-1], f32) > 1e-6  # the rounding is really applied
+
+
+def test_mg_solve_bf16_finest_smoother(oracle_mod, case):
+    """The headline cycle with the BF16 finest-level smoother and FP32 Krylov
+    vectors (FP64 lambda) converges to the oracle's lambda at 1e-9."""
+    from hicar_b200 import wind, wind_iterative as wi
+    dom, opt, div, _ = _calibrated(case)
+    h = wi.handle(dom.nest_indx)
+    wi.set_options(wi.WindOptions(tol_rel=1e-9, wind_solver_iterations=3000, precond=_capi.PRECOND_MG,
+                                  stall_iters=50, mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4),
+                                  krylov_precision=_capi.KRYLOV_F32_X64, mg_precision=1))
+    dom.set_winds(case.u, case.v, case.w)
+    _capi.load().hicarw_reset_solution(h, None)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+    assert st["status"] == 0 and st["precond"] == _capi.PRECOND_MG
+    lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
+    _capi.load().hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None)
+    s = oracle_mod.OracleSolver(case.domain)
+    s.set_coefs(_coefs(dom), probed=True)
+    s.prepare(div.cpu().numpy())
+    s.set_vec("x", np.zeros_like(lam))
+    s.set_tolerance(1e-10)
+    assert s.bicgstab(3000)["status"] == 0
+    assert _rel(lam, s.vec("x")) < 1e-5
