@@ -661,9 +661,14 @@ def run_ours(args, wl):
             opt, name, table = pick_cycle(wi, step, solver_kwargs(args.solver))
             cycle = {"chosen": name, "warmup_solve_ms": table, **MG_CYCLES[name.split("/")[0]]}
         elif MG_CYCLE != "auto":
-            opt = wi.WindOptions(**{**solver_kwargs(args.solver), **MG_CYCLES[MG_CYCLE]})
+            extra = {}
+            if args.krylov_precision is not None:
+                extra["krylov_precision"] = args.krylov_precision
+            if args.mg_precision is not None:
+                extra["mg_precision"] = args.mg_precision
+            opt = wi.WindOptions(**{**solver_kwargs(args.solver), **MG_CYCLES[MG_CYCLE], **extra})
             wi.set_options(opt)
-            cycle = {"chosen": MG_CYCLE, **MG_CYCLES[MG_CYCLE]}
+            cycle = {"chosen": MG_CYCLE, **MG_CYCLES[MG_CYCLE], **extra}
         if cycle is not None:
             cycle = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cycle.items()}
     for _ in range(args.warmup):
@@ -1027,6 +1032,10 @@ def main():
                     help="cycle shape of the mg preset (auto: the fastest on the workload, picked in the warm-up)")
     ap.add_argument("--mg-w-levels", default="",
                     help="comma-separated V-cycle levels (>= 1) that correct twice from the coarse grid")
+    ap.add_argument("--krylov-precision", type=int, default=None, choices=[0, 2],
+                    help="with --mg-cycle NAME: Krylov vectors FP64 (0) or FP32 with FP64 lambda (2)")
+    ap.add_argument("--mg-precision", type=int, default=None, choices=[0, 1],
+                    help="with --mg-cycle NAME: finest-level smoother coefficients FP32 (0) or BF16 (1)")
     ap.add_argument("--mg-omega", type=float, default=None,
                     help="override the V-cycle's smoother damping of the solver preset")
     ap.add_argument("--fgmres-restart", type=int, default=None,
