@@ -663,7 +663,8 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
 // read-only path.
 // ---------------------------------------------------------------------------
 constexpr int MG_FUSE_COLS = 1024;  // first fused level: nx * ny at most this
-constexpr int MG_FUSE_STEPS = 48;   // longest recorded chain (else the per-level launches run)
+constexpr int MG_FUSE_STEPS = 128;  // longest recorded chain (else the per-level launches run); 128 steps
+                                    // of 232 bytes keep the kernel parameter under 32 KB
 constexpr int MG_FUSE_THREADS = 512;
 
 struct CoarseStep {
@@ -682,6 +683,7 @@ struct CoarseProg {
     int n;
     CoarseStep step[MG_FUSE_STEPS];
 };
+static_assert(sizeof(CoarseProg) <= 32000, "the recorded chain is passed as one kernel parameter (32 KB at most)");
 
 __device__ __forceinline__ unsigned cluster_rank()
 {
