@@ -214,6 +214,19 @@ def calibrated_handle(case):
     return dom, wi.handle(dom.nest_indx)
 
 
+def probed_handle(case):
+    """(DeviceDomain, handle) with the case's probed operator from the 27-colour
+    calibration alone (no solves before it): the operator is the same as
+    after update_winds' first update, which calibrates with the same alpha."""
+    from . import wind, wind_iterative as wi
+    from .domain import DeviceDomain
+    dom = DeviceDomain.from_case(case, "cuda")
+    opt = wi.WindOptions(tol_rel=1e-6)
+    wi.init_iter_winds(dom, opt)
+    wind.calibrate_projection_operator(dom, opt)
+    return dom, wi.handle(dom.nest_indx)
+
+
 SOLVER_ITERS = (1, 3, 8, 16, 32, 64, 128, 256)  # plain-solver iterations whose residuals are logged
 
 
@@ -298,7 +311,7 @@ def composite_pairs(case, net: UNet, ks=SOLVER_ITERS, tight_tol: float = 1e-10, 
     torch = _torch()
     from . import wind, wind_iterative as wi
     cycle = MG_CYCLE if cycle is None else cycle
-    dom, h = calibrated_handle(case)
+    dom, h = probed_handle(case)
     lib = _capi.load()
     shape = (dom.ny + 2, dom.nz + 2, dom.nx + 2)
     coefs = torch.empty((15, dom.ny, dom.nz, dom.nx), dtype=torch.float32, device="cuda")
