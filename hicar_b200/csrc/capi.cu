@@ -1568,6 +1568,7 @@ extern "C" int hicarw_dist_setup(hicarw_handle *h, const double *rhs, double *to
     OpCtx c = opctx(h);
     RedBuf rb{h->partials, h->red_blocks};
     enqueue_setup_prec(h, HICARW_KRYLOV_F64, c, rb, s, 0);
+    CK(cudaGetLastError());
     return dist_out(h, tot3, 3, mem_kind, s);
 }
 
@@ -1642,6 +1643,7 @@ extern "C" int hicarw_dist_spmv(hicarw_handle *h, int which, double *tot, int me
     CK(cudaMemsetAsync(st->dist_tot, 0, 5 * sizeof(double), s)); // a solve that has stopped publishes zeros
     if (which == 0) launch_spmv_sigma<double>(c, phat, v, rhat, st, rb, s);
     else launch_spmv_dot5<double>(c, shat, t, sv, rhat, st, h->hist, rb, s);
+    CK(cudaGetLastError());
     return dist_out(h, tot, which == 0 ? 1 : 5, mem_kind, s);
 }
 

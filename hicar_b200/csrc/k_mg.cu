@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -995,10 +996,30 @@ static const char *kLevelName[3][MG_MAX_LEVELS] = {
 // columns), 2 x 2 tiles on coarse levels so that they still spread over many CTAs.
 static bool small_level(const Dims &d, int tc) { return (long long)d.nx * d.ny < (long long)tc * 2 * 148; }
 
+// Raise a kernel's dynamic shared-memory limit to at least smem, never lower
+// it: a CUDA graph captured earlier may hold a launch of the same kernel with
+// more shared memory (levels and subdomains of other sizes).
+static void raise_smem(const void *kernel, size_t smem)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, size_t>> set;
+    if (smem <= 48 * 1024) return;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto &e : set)
+        if (e.first == kernel) {
+            if (e.second >= smem) return;
+            if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess)
+                e.second = smem;
+            return;
+        }
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess)
+        set.emplace_back(kernel, smem);
+}
+
 template <typename F>
 static void set_smem(F *kernel, size_t smem)
 {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem((const void *)kernel, smem);
 }
 
 template <typename TR, int TX, int TY>
@@ -1123,7 +1144,7 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
         return false;
     const int ntx = (d.nx + TX - 1) / TX, ntiles = ntx * d.ny;
     const int grid = std::min(ntiles, 2 * sm_count());
-    cudaFuncSetAttribute(post_tma_kernel<TR, TO, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
     int *e = gate ? const_cast<int *>(&gate->err) : err;
     post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
                                                             cscale, ntx, ntiles, gate, e);
@@ -1290,13 +1311,14 @@ static void fused_setup(Mg &mg)
             break;
         }
     if (!l0) return;
-    cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
     for (int cn : {16, 8}) {
         size_t smem = 0;
         if (!fused_smem(mg, l0, cn, (size_t)smem_optin(), &smem)) continue;
-        if (cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            continue;
+        raise_smem((const void *)coarse_cycle_kernel, smem);
         cudaLaunchAttribute at[1];
         cudaLaunchConfig_t cfg = fused_config(cn, smem, nullptr, at);
         int nclusters = 0;
@@ -1328,7 +1350,7 @@ static bool launch_fused(const Mg &mg, int l, const SolveState *gate, cudaStream
         bytes += p.kind == 0 ? (60.0 + 4.0 + 4.0) * N : (4.0 + 4.0 + 60.0 + 4.0 + 1.0 + 8.0) * N;
     }
     ProfScope ps_(kFusedName[l], bytes, s);
-    cudaFuncSetAttribute(coarse_cycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem((const void *)coarse_cycle_kernel, smem);
     cudaLaunchAttribute at[1];
     cudaLaunchConfig_t cfg = fused_config(mg.cluster_n, smem, s, at);
     cudaLaunchKernelEx(&cfg, coarse_cycle_kernel, prog, gate);
