@@ -183,6 +183,6 @@ def default_options() -> Options:
 
 def check(rc: int, handle=None, allow_status: bool = True) -> int:
     if rc < 0:
-        msg = load().hicarw_last_error(handle).decode() if handle is not None else ""
+        msg = load().hicarw_last_error(handle).decode()  # NULL handle: the calls without one (batches)
         raise HicarwError(f"{ERRORS.get(rc, rc)}: {msg}")
     return rc

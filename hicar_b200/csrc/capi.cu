@@ -24,6 +24,7 @@
 #include "mg.h"
 #include "fgmres.h"
 #include "unet.h"
+#include "krylov_dev.cuh"
 
 using namespace hw;
 
@@ -659,9 +660,13 @@ int unet_precond(hicarw_unet *n, const OpCtx &c, const double *in, double *out, 
 bool unet_matches(const hicarw_unet *n, const Dims &d);
 }  // namespace hw
 
-// z = M(r) + U(r - A M(r)): the V-cycle, then the U-Net's estimate of the error
-// left in its residual (V_T and V_PRES are free during FGMRES: they hold A M(r)
-// and the residual left by the V-cycle).
+// z = M(r) + theta U(r'), r' = r - A M(r): the V-cycle, then the U-Net's
+// estimate of the error left in the residual r' that the V-cycle leaves, taken
+// with the minimal-residual step theta = <r', A u> / <A u, A u> (u = U(r')), so
+// that ||r - A z|| = min over theta of ||r' - theta A u|| <= ||r'||: the composite
+// never leaves a larger residual than the V-cycle alone, whatever the network
+// returns.  Scratch: V_T (A M(r), then u), V_PRES (r'), V_V (A u); all three are
+// free during FGMRES.
 __global__ void mgl_residual_kernel(long long n, const double *__restrict__ r, double *__restrict__ az,
                                     double *__restrict__ res, const SolveState *gate)
 {
@@ -672,11 +677,30 @@ __global__ void mgl_residual_kernel(long long n, const double *__restrict__ r, d
     }
 }
 
-__global__ void mgl_add_kernel(long long n, const double *__restrict__ u, double *__restrict__ z, const SolveState *gate)
+// theta = <r', A u> / <A u, A u> (0 when A u = 0), left in st->mr_theta by the last CTA
+__global__ void __launch_bounds__(256) mgl_step_kernel(long long n, const double *__restrict__ res,
+                                                       const double *__restrict__ au, SolveState *st,
+                                                       double *partials, const SolveState *gate)
 {
     if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
+    double acc[2] = {0.0, 0.0};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const double a = au[q];
+        acc[0] += res[q] * a;
+        acc[1] += a * a;
+    }
+    double tot[2];
+    if (!grid_reduce<2>(acc, partials, &st->ticket[5], tot)) return;
+    if (threadIdx.x == 0) st->mr_theta = tot[1] > 0.0 ? tot[0] / tot[1] : 0.0;
+}
+
+__global__ void mgl_add_kernel(long long n, const double *__restrict__ u, double *__restrict__ z, const SolveState *st,
+                               const SolveState *gate)
+{
+    if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
+    const double theta = st->mr_theta;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        z[q] += u[q];
+        z[q] += theta * u[q];
 }
 
 static void mg_learned_apply(hicarw_handle *h, const double *in, double *out, const SolveState *gate, cudaStream_t s)
@@ -684,7 +708,8 @@ static void mg_learned_apply(hicarw_handle *h, const double *in, double *out, co
     const OpCtx c = opctx(h);
     const long long n = h->d.npad;
     const int g = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-    double *az = V<double>(h, V_T), *res = V<double>(h, V_PRES);
+    const int gr = std::min(g, h->red_blocks);
+    double *az = V<double>(h, V_T), *res = V<double>(h, V_PRES), *au = V<double>(h, V_V);
     mg_apply<double>(h->mg, in, out, gate, s);
     launch_spmv<double>(c, out, az, gate, s);
     {
@@ -693,8 +718,14 @@ static void mg_learned_apply(hicarw_handle *h, const double *in, double *out, co
         count_launch(1);
     }
     unet_precond(h->unet, c, res, az, gate, s);
+    launch_spmv<double>(c, az, au, gate, s);
+    {
+        ProfScope ps_("mgl_step", (double)n * 16.0, s);
+        mgl_step_kernel<<<gr, 256, 0, s>>>(n, res, au, h->st, h->partials, gate);
+        count_launch(1);
+    }
     ProfScope ps_("mgl_add", (double)n * 24.0, s);
-    mgl_add_kernel<<<g, 256, 0, s>>>(n, az, out, gate);
+    mgl_add_kernel<<<g, 256, 0, s>>>(n, az, out, h->st, gate);
     count_launch(1);
 }
 
@@ -1534,6 +1565,12 @@ static int dist_ready(hicarw_handle *h)
 {
     if (!h || !h->dist_buf || h->opt.solver != HICARW_SOLVER_REFERENCE || h->opt.krylov_precision != HICARW_KRYLOV_F64)
         return HICARW_ERR_STATE;
+    // an error left by an earlier call of this thread is reported as such, not as this step's
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_err(h, "a CUDA error pending before this decomposed-solve step", e);
+        return HICARW_ERR_CUDA;
+    }
     return 0;
 }
 
@@ -1732,13 +1769,18 @@ extern "C" int hicarw_smooth_alpha(hicarw_handle *h, float *alpha, int window, i
 // over `lanes` independent chains (longest-processing-time order by size) that
 // the GPU runs concurrently.  Every WHILE loop is also bounded by a body count
 // (max_iters / chunk + 2), so it ends even if a solve never sets its flag.
+// a failed batch call: the message is the one hicarw_last_error(NULL) returns
+static int batch_fail(int rc, const std::string &msg)
+{
+    g_err_noh = "hicarw batch: " + msg;
+    fprintf(stderr, "%s\n", g_err_noh.c_str());
+    return rc;
+}
+
 #define BCK(x)                                                                                                   \
     do {                                                                                                         \
         cudaError_t e_ = (x);                                                                                    \
-        if (e_ != cudaSuccess) {                                                                                 \
-            fprintf(stderr, "hicarw batch: %s: %s\n", #x, cudaGetErrorString(e_));                               \
-            return HICARW_ERR_CUDA;                                                                              \
-        }                                                                                                        \
+        if (e_ != cudaSuccess) return batch_fail(HICARW_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
 struct hicarw_batch {
@@ -1915,8 +1957,7 @@ static int batch_build(hicarw_batch *b, const hicarw_batch_item *items, int cold
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         b->exec = nullptr;
-        fprintf(stderr, "hicarw batch graph: %s\n", cudaGetErrorString(e));
-        return HICARW_ERR_CUDA;
+        return batch_fail(HICARW_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
     }
     b->nodes = nodes;
     b->built.assign(items, items + n);
@@ -1941,17 +1982,16 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
         select_precond(h, 1);
         if (h->use_mg && (h->mg_dirty || !h->mg.ready)) {
             mg_params(h);
-            if (mg_build_tuned(h, s) != 0) {
-                fprintf(stderr, "hicarw batch: multigrid build of subdomain %d failed\n", i);
-                return HICARW_ERR_CUDA;
-            }
+            if (mg_build_tuned(h, s) != 0)
+                return batch_fail(HICARW_ERR_CUDA, "multigrid build of subdomain " + std::to_string(i) + ": " + h->err);
             h->mg_dirty = 0;
             rebuild = true;
         }
         if (h->opt.solver == HICARW_SOLVER_FGMRES) {
             const bool dirty = (h->use_learned || h->use_mglearned) && h->unet_dirty;
             FgmresCtx f;
-            if ((rc = fgmres_ready(h, h->precond_n_sweeps, s, &f)) != 0) return rc;
+            if ((rc = fgmres_ready(h, h->precond_n_sweeps, s, &f)) != 0)
+                return batch_fail(rc, "FGMRES set-up of subdomain " + std::to_string(i) + ": " + h->err);
             if (dirty || b->fg[i].V != f.V || b->fg[i].m != f.m) rebuild = true;
             b->fg[i] = f;
         }
@@ -1971,20 +2011,17 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
     BCK(cudaStreamSynchronize(s));
     BCK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
     for (int i = 0; i < n; i++)
-        if (b->hs[i]->hst->err) {
-            fprintf(stderr, "hicarw batch: subdomain %d: a bounded device-side wait timed out\n", i);
-            return HICARW_ERR_TIMEOUT;
-        }
+        if (b->hs[i]->hst->err)
+            return batch_fail(HICARW_ERR_TIMEOUT, "subdomain " + std::to_string(i) + ": a bounded device-side wait timed out");
     for (int i = 0; i < n; i++) // FGMRES state -> the solve-state mirror
-        if (b->hs[i]->opt.solver == HICARW_SOLVER_FGMRES && (rc = fgmres_map_state(b->hs[i], 0, s)) != 0) return rc;
+        if (b->hs[i]->opt.solver == HICARW_SOLVER_FGMRES && (rc = fgmres_map_state(b->hs[i], 0, s)) != 0)
+            return batch_fail(rc, "FGMRES state of subdomain " + std::to_string(i) + ": " + b->hs[i]->err);
     std::vector<int> fell(n, 0);
     for (int i = 0; i < n; i++) { // a stalled or failed preconditioned solve: the reference solve decides
         hicarw_handle *h = b->hs[i];
         if (h->hst->status != 0 && (h->use_mg || h->use_learned)) {
-            if ((rc = zero_solution(h, s)) != 0 || (rc = bicgstab_solve(h, h->precond_n_sweeps, s, 0)) != 0) {
-                fprintf(stderr, "hicarw batch: fallback solve of subdomain %d: %s\n", i, h->err.c_str());
-                return rc;
-            }
+            if ((rc = zero_solution(h, s)) != 0 || (rc = bicgstab_solve(h, h->precond_n_sweeps, s, 0)) != 0)
+                return batch_fail(rc, "fallback solve of subdomain " + std::to_string(i) + ": " + h->err);
             fell[i] = 1;
         }
     }

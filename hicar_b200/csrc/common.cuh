@@ -84,6 +84,7 @@ struct SolveState {
     int dist;       // decomposed solve: reductions publish their local totals in dist_tot and the
                     // host applies the scalar steps to the totals summed over all ranks
     double dist_tot[5];
+    double mr_theta; // composite learned preconditioner: the minimal-residual step along the U-Net's correction
 };
 
 // Rank-edge sides of a decomposed subdomain (bit mask): their ring cells are

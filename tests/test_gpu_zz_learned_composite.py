@@ -1,9 +1,11 @@
 """GPU tests of the composite learned preconditioner HICARW_PRECOND_MG_LEARNED,
-z = M(r) + U(r - A M(r)): the V-cycle, then the U-Net's estimate of the error
-left in the residual the V-cycle leaves, inside FGMRES.
+z = M(r) + theta U(r'), r' = r - A M(r): the V-cycle, then the U-Net's estimate
+of the error left in the residual the V-cycle leaves, with the minimal-residual
+step theta, inside FGMRES.
 
 * The composite applied by the library equals its parts composed through the
-  C ABI (V-cycle, operator, U-Net apply).
+  C ABI (V-cycle, operator, U-Net apply, the step), and leaves no larger a
+  residual than the V-cycle alone.
 * FGMRES with the composite converges to the oracle's lambda.
 * The training-pair generator logs one pair per requested iterate of the
   plain solver, with finite, non-zero targets of the network's output shape.
@@ -71,9 +73,15 @@ def test_composite_equals_its_parts():
     _capi.check(lib.hicarw_apply_operator(h, z1.data_ptr(), az.data_ptr(), _capi.MEM_DEVICE, None), h)
     rp = r - az
     u = net.apply(h, rp)
-    want = z1 + u
+    au = torch.empty_like(r)
+    _capi.check(lib.hicarw_apply_operator(h, u.data_ptr(), au.data_ptr(), _capi.MEM_DEVICE, None), h)
+    theta = float((rp * au).sum() / (au * au).sum())  # the minimal-residual step along u
+    want = z1 + theta * u
     torch.cuda.synchronize()
     assert _rel(z.cpu().numpy(), want.cpu().numpy()) < 1e-12
+    # the composite leaves no larger a residual than the V-cycle alone
+    _capi.check(lib.hicarw_apply_operator(h, z.data_ptr(), az.data_ptr(), _capi.MEM_DEVICE, None), h)
+    assert float((r - az).norm()) <= float(rp.norm()) * (1.0 + 1e-12)
     lib.hicarw_set_learned_precond(h, None)
 
 
