@@ -569,7 +569,8 @@ def at_tolerance(opt, tol):
 
 def learned_report(lib, wi, dom, h, step, stream, tols, plain_ms, accuracy_solve=None):
     """The learned+mixed solver on the workload: FGMRES(30) with the composite
-    preconditioner z = M(r) + U(r - A M(r)) (the benchmark's V-cycle, then the
+    preconditioner z = M(r) + theta U(r'), r' = r - A M(r), theta the
+    minimal-residual step (the benchmark's V-cycle, then the
     U-Net trained on solver-logged pairs of 128x128x32 terrains, BF16 tensor-core
     convolutions), against the same outer loop with the V-cycle alone (the
     method without the network).  For each tolerance: solves/s of 3 timed
@@ -844,6 +845,9 @@ def run_ours(args, wl):
     wi.finalize_iter_winds()
     if world == 1 and not args.no_batch and args.workload == "mixed1024":
         torch.cuda.synchronize()
+        del dom, div, u0, v0, w0, case  # the headline workload's device memory goes back before the batch
+        net = compare = None
+        torch.cuda.empty_cache()
         try:
             b = batch_measure(args, WORKLOADS["batch96"], rank, world, dist, local, quick=True)
         except Exception as e:  # the headline line is printed all the same, with the reason

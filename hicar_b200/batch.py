@@ -31,10 +31,15 @@ def subdomain_cases(n: int, seed: int = 0, nxy=(96, 512, 32), nz=(20, 48, 4), n_
         yield cases.build_case(nx, ny, nzz, dx, n_hills, seed=seed * 100003 + i, adv_den=True)
 
 
+# Restart length of the learned subdomains' FGMRES: its basis holds 2m + 1 FP64
+# vectors per subdomain, so a long restart does not fit a large batch in HBM.
+LEARNED_RESTART = 10
+
+
 class BatchSolver:
     """Handles for every case (created, calibrated with the 27-colour probe on the
     device) and the batch that solves them together.  learned_every = m > 0
-    solves every m-th subdomain with FGMRES(30) and the composite learned
+    solves every m-th subdomain with FGMRES(LEARNED_RESTART) and the composite learned
     preconditioner (V-cycle + U-Net correction, parameters `learned_params`),
     the others with `options`."""
 
@@ -74,7 +79,7 @@ class BatchSolver:
                     net.attach(h)
                     self.nets.append(net)
                     lo = WindOptions(**{**self.options.__dict__, "solver": _capi.SOLVER_FGMRES,
-                                        "precond": _capi.PRECOND_MG_LEARNED, "fgmres_restart": 30,
+                                        "precond": _capi.PRECOND_MG_LEARNED, "fgmres_restart": LEARNED_RESTART,
                                         "stall_iters": 200, **L.MG_CYCLE})
                     _capi.check(self.lib.hicarw_set_options(h, C.byref(lo.to_c())), h)
             n = len(self.handles)

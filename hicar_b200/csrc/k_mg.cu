@@ -213,6 +213,26 @@ __device__ __forceinline__ double stencil_regs(const float (&cv)[15], const floa
     return y;
 }
 
+// The post-smoothers' residual r - A x2 of one cell (post_kernel, post_tma_kernel
+// and the fused coarse cycle's post steps, which must agree bit for bit).
+// HICARW_MG_POST_F32: FP32 products and sums in the fixed term order (fmaf),
+// one rounding of the difference; otherwise exact products summed in FP64.
+#ifndef HICARW_MG_POST_F32
+#define HICARW_MG_POST_F32 0
+#endif
+template <int SX, int SP>
+__device__ __forceinline__ float post_residual(double rv, const float (&cv)[15], const float *xs)
+{
+#if HICARW_MG_POST_F32
+    float y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y = fmaf(cv[q], xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]], y);
+    return (float)(rv - (double)y);
+#else
+    return (float)(rv - stencil_regs<SX, SP>(cv, xs));
+#endif
+}
+
 // Pre-smoothing from zero: out = w T^-1 r.  A CTA owns TX x TY columns, all k.
 template <typename TR, int TX, int TY>
 __global__ void __launch_bounds__(MG_THREADS) pre_kernel(Dims d, const float *__restrict__ coef,
@@ -332,7 +352,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) post_kernel(Dims d, const CT *_
                 vm[u] = __ldg(minv + o);
                 vp[u] = __ldg(cp + o);
                 vc[u] = k > 1 ? cv[CC] : 0.0f;
-                res2[u] = (float)(rv - stencil_regs<SX, SP>(cv, xs));
+                res2[u] = post_residual<SX, SP>(rv, cv, xs);
             }
         }
 #pragma unroll
@@ -512,7 +532,7 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
                     for (int q = 0; q < 15; q++) cv[q] = coef_val(sco[(q * KC + warp) * TX + lane]);
                     const float *xs = s_x2w + (WK + warp + 1) * WX + lane + 1;
                     const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
-                    res = (float)(rv - stencil_regs<WK * WX, WX>(cv, xs));
+                    res = post_residual<WK * WX, WX>(rv, cv, xs);
                     x2c = xs[0];
                     cpv = ((const float *)(st + O_CP))[warp * TX + lane];
                 }
@@ -711,6 +731,17 @@ __device__ __forceinline__ double stencil_regs_rt(const float (&cv)[15], const f
     for (int q = 0; q < 15; q++) y += (double)cv[q] * (double)xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]];
     return y;
 }
+__device__ __forceinline__ float post_residual_rt(double rv, const float (&cv)[15], const float *xs, int SX, int SP)
+{
+#if HICARW_MG_POST_F32
+    float y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y = fmaf(cv[q], xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]], y);
+    return (float)(rv - (double)y);
+#else
+    return (float)(rv - stencil_regs_rt(cv, xs, SX, SP));
+#endif
+}
 
 // stage_window with a runtime window shape; x1 and xc are read through L2
 __device__ __forceinline__ void stage_window_rt(const Dims &d, const float *x1, const Dims &dc, const float *xc, int ia,
@@ -812,7 +843,7 @@ __device__ void fused_post(const CoarseStep &p, int bx, int by, float *sm)
             vm = __ldg(p.minv_f + o);
             vp = __ldg(p.cp_f + o);
             vc = k > 1 ? cv[CC] : 0.0f;
-            res2 = (float)(rv - stencil_regs_rt(cv, xs, SX, SP));
+            res2 = post_residual_rt(rv, cv, xs, SX, SP);
         }
         s_res[t] = res2;
         s_c[t] = vc;

@@ -298,7 +298,7 @@ MG_CYCLE = dict(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_w_levels=(2, 3, 4)
 
 
 def composite_pairs(case, net: UNet, ks=SOLVER_ITERS, tight_tol: float = 1e-10, cycle=None):
-    """Training samples of the composite preconditioner z = M(r) + U(r - A M(r))
+    """Training samples of the composite preconditioner z = M(r) + theta U(r - A M(r))
     (HICARW_PRECOND_MG_LEARNED), logged from the plain solver on one terrain:
     the case's right-hand side b = -2 div(u, v, w) is solved once tightly
     (FGMRES + V-cycle, x*), then the reference BiCGStab (Jacobi-Richardson) is

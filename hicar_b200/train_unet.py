@@ -8,7 +8,7 @@ parameters (FP32 .npy), e.g.
         --out hicar_b200/weights/unet_mg_128x128x32.npy
 
 The composite source trains the second stage of HICARW_PRECOND_MG_LEARNED
-(z = M(r) + U(r - A M(r))) online: each seeded terrain's plain-solver iterates
+(z = M(r) + theta U(r'), r' = r - A M(r)) online: each seeded terrain's plain-solver iterates
 give (residual, error) pairs after the V-cycle (learned.composite_pairs), the
 pairs enter a replay buffer, and a few Adam steps follow each terrain, so that
 thousands of terrains stream through without being stored.

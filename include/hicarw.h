@@ -87,8 +87,10 @@ enum {
                                   Galerkin coarse operators down to one column (probed operator only) */
     HICARW_PRECOND_LEARNED = 2, /* the U-Net attached by hicarw_set_learned_precond (FGMRES only,
                                    probed operator only) */
-    HICARW_PRECOND_MG_LEARNED = 3 /* the V-cycle, then the attached U-Net's correction of the residual it
-                                     leaves: z = M(r) + U(r - A M(r)) (FGMRES only, probed operator only) */
+    HICARW_PRECOND_MG_LEARNED = 3 /* the V-cycle, then the attached U-Net's correction u = U(r') of the
+                                     residual r' = r - A M(r) it leaves, taken with the minimal-residual step:
+                                     z = M(r) + theta u, theta = <r', A u> / <A u, A u>, so ||r - A z|| <= ||r'||
+                                     (FGMRES only, probed operator only) */
 };
 
 /* Stopping rule. */
@@ -314,7 +316,9 @@ int hicarw_set_kernel_tuning(hicarw_handle *h, int spmv_levels, int mg_post_feed
  * the handle and the GPU stay usable. */
 int hicarw_debug_wait_timeout(hicarw_handle *h, double limit_us, void *stream);
 
-/* Last CUDA error string of this handle (static storage). */
+/* Last error string of this handle (valid until its next call); h = NULL: the
+ * last error of this thread's calls that take no handle (the batch entry points,
+ * a failed hicarw_init_iter_winds). */
 const char *hicarw_last_error(hicarw_handle *h);
 
 /* ---- batched solves of independent, unevenly sized subdomains (no reference counterpart) ----
