@@ -594,6 +594,236 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Post-smoothing fed by tensor copies, with the column recurrences moved off
+// the consumers' path.  The producer warp and the stage layout are those of
+// post_tma_kernel (two stages).  Eight consumer warps form x2 on the chunk's
+// window (double-buffered, so one CTA barrier per chunk) and the residuals,
+// release the stage as soon as their reads are done, and hand each chunk's
+// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a two-slot
+// ring.  The recurrence warp owns the tile's column arrays: it runs the forward
+// recurrence chunk by chunk and, at the end of a tile, the backward one,
+// writing each cell's result as soon as it is known; the consumers go on with
+// the next tile meanwhile.  Same statements per cell as post_tma_kernel, so
+// the results are bit-identical.  Every wait is bounded (on timeout: *err set,
+// the loops run to their end without waiting).
+// ---------------------------------------------------------------------------
+namespace pt2 {
+constexpr int NS = 2;                      // stages
+constexpr int NR = 2;                      // ring slots
+constexpr int RW = pt::KC;                 // recurrence warp
+constexpr int PW = pt::KC + 1;             // producer warp
+constexpr int THREADS = pt::CW + 64;
+constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
+constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
+constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
+template <typename TR, typename CT> size_t smem_bytes(int nz)
+{
+    return 128 + (size_t)NS * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
+           (size_t)2 * XW * 4 + 2 * (NS + NR) * 8 + 16;
+}
+}  // namespace pt2
+
+template <typename TR, typename TO, typename CT = float>
+__global__ void __launch_bounds__(pt2::THREADS, 2)
+    post_tma2_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
+                     const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
+                     const __grid_constant__ CUtensorMap tm_x1, const __grid_constant__ CUtensorMap tm_xc, Dims d,
+                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, const SolveState *gate,
+                     int *err)
+{
+    using namespace pt;
+    using pt2::NS;
+    using pt2::NR;
+    constexpr int SB = stage_bytes<TR, CT>();
+    constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(), O_XC = o_xc<CT>(),
+                  O_R = o_r<CT>();
+    constexpr int SLOT = pt2::RING_ROWS * KC * TX; // floats per ring slot
+    extern __shared__ unsigned char pt_smem[];
+    unsigned char *base = (unsigned char *)(((uintptr_t)pt_smem + 127) & ~(uintptr_t)127);
+    const int nz = d.nz, nch = (nz + KC - 1) / KC;
+    float *ring = (float *)(base + NS * SB);
+    float *s_d = ring + NR * SLOT; // recurrence warp: forward results, then the column solution
+    float *s_cp = s_d + nz * TX;
+    float *s_x2c = s_cp + nz * TX;
+    float *s_x2w = s_x2c + nz * TX; // two window buffers of pt2::XW floats
+    uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
+    uint64_t *empty = full + NS;
+    uint64_t *rfull = empty + NS;
+    uint64_t *rempty = rfull + NR;
+    int *s_skip = (int *)(rempty + NR);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
+        for (int q = 0; q < NS; q++) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&empty[q], KC); // one arrival per consumer warp
+        }
+        for (int q = 0; q < NR; q++) {
+            tc::mbar_init(&rfull[q], KC);
+            tc::mbar_init(&rempty[q], 1);
+        }
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (s_skip[0]) return; // the same value for every thread
+
+    if (warp == pt2::PW) { // ---- producer ----
+        if (lane != 0) return;
+        bool ok = true;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
+            for (int ch = 0; ch < nch; ch++, it++) {
+                const int s = it % NS;
+                if (it >= NS && !tc::mbar_wait(&empty[s], ((it / NS) - 1) & 1)) {
+                    atomicExch(err, 1);
+                    ok = false;
+                    break;
+                }
+                unsigned char *st = base + s * SB;
+                const int k0 = 1 + ch * KC, row = j * d.mz + k0;
+                tc::mbar_expect_tx(&full[s], tx_bytes<TR, CT>());
+                tc::tma_load_3d(st + O_COEF, &tm_coef, i0 + XO, row, 0, &full[s]);
+                tc::tma_load_2d(st + O_MINV, &tm_minv, i0 + XO, row, &full[s]);
+                tc::tma_load_2d(st + O_CP, &tm_cp, i0 + XO, row, &full[s]);
+                tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
+                tc::tma_load_3d(st + O_XC, &tm_xc, (i0 >> 1) + XO - 3, k0 - 1, j >> 1, &full[s]);
+                tc::tma_load_2d(st + O_R, &tm_r, i0 + XO, row, &full[s]);
+            }
+        }
+        // no copy may still be in flight when the CTA ends: wait for the last stages issued
+        for (int q = it > NS ? it - NS : 0; q < it; q++)
+            if (!tc::mbar_wait(&full[q % NS], (q / NS) & 1)) atomicExch(err, 1);
+        return;
+    }
+
+    if (warp == pt2::RW) { // ---- recurrence warp: lane = column ----
+        bool ok = true;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            const int bx = tile % ntx, j = tile / ntx + 1, i = bx * TX + 1 + lane;
+            const bool col = i <= d.nx;
+            float dprev = 0.0f;
+            for (int ch = 0; ch < nch; ch++, it++) {
+                const int q = it % NR;
+                if (ok && !tc::mbar_wait(&rfull[q], (it / NR) & 1)) {
+                    atomicExch(err, 1);
+                    ok = false;
+                }
+                const float *rs = ring + q * SLOT;
+                const int k0 = 1 + ch * KC;
+                if (col) {
+                    float rv[KC], xv[KC], pv[KC], cv[KC], mv[KC];
+#pragma unroll
+                    for (int u = 0; u < KC; u++) {
+                        rv[u] = rs[(0 * KC + u) * TX + lane];
+                        xv[u] = rs[(1 * KC + u) * TX + lane];
+                        pv[u] = rs[(2 * KC + u) * TX + lane];
+                        cv[u] = rs[(3 * KC + u) * TX + lane];
+                        mv[u] = rs[(4 * KC + u) * TX + lane];
+                    }
+#pragma unroll
+                    for (int u = 0; u < KC; u++) {
+                        if (k0 + u > nz) break;
+                        dprev = (rv[u] - cv[u] * dprev) * mv[u];
+                        const int t = (k0 + u - 1) * TX + lane;
+                        s_d[t] = dprev;
+                        s_cp[t] = pv[u];
+                        s_x2c[t] = xv[u];
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&rempty[q]);
+            }
+            if (col) { // backward recurrence, each level's result written as soon as it is known
+                float y = 0.0f;
+                int k = nz - 1;
+                for (; k + 1 >= THOMAS_U; k -= THOMAS_U) {
+                    float rv[THOMAS_U], pv[THOMAS_U], xv[THOMAS_U];
+#pragma unroll
+                    for (int u = 0; u < THOMAS_U; u++) {
+                        rv[u] = s_d[(k - u) * TX + lane];
+                        pv[u] = s_cp[(k - u) * TX + lane];
+                        xv[u] = s_x2c[(k - u) * TX + lane];
+                    }
+#pragma unroll
+                    for (int u = 0; u < THOMAS_U; u++) {
+                        y = rv[u] - pv[u] * y;
+                        out[kidx(d, i, k - u + 1, j)] = (TO)((double)xv[u] + (double)omega * (double)y);
+                    }
+                }
+                for (; k >= 0; k--) {
+                    y = s_d[k * TX + lane] - s_cp[k * TX + lane] * y;
+                    out[kidx(d, i, k + 1, j)] = (TO)((double)s_x2c[k * TX + lane] + (double)omega * (double)y);
+                }
+            }
+        }
+        return;
+    }
+
+    // ---- consumers: warp w owns level k0 + w of each chunk, lane = column ----
+    bool ok = true;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
+        const bool col = i0 + lane <= d.nx;
+        for (int ch = 0; ch < nch; ch++, it++) {
+            const int s = it % NS, q = it % NR;
+            const unsigned char *st = base + s * SB;
+            if (ok && !tc::mbar_wait(&full[s], (it / NS) & 1)) {
+                atomicExch(err, 1);
+                ok = false;
+            }
+            const int k0 = 1 + ch * KC;
+            // x2 = x1 + s P xc on the chunk's window, zero outside the interior
+            float *xw = s_x2w + (it & 1) * pt2::XW;
+            const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
+            for (int e = tid; e < 3 * WK * WX; e += CW) {
+                const int cc = e % WX, kw = (e / WX) % WK, jj = e / (WX * WK);
+                const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
+                float a = 0.0f;
+                if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
+                    a = sx1[(jj * WK + kw) * X1W + cc + 3];
+                    a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
+                }
+                xw[e] = a;
+            }
+            // every consumer has finished the previous chunk (whose window buffer the next chunk reuses)
+            tc::named_sync(1, CW);
+            const int k = k0 + warp;
+            float res = 0.0f, x2c = 0.0f, cpv = 0.0f, ccv = 0.0f, mv = 0.0f;
+            if (k <= nz && col) {
+                const CT *sco = (const CT *)(st + O_COEF);
+                float cv[15];
+#pragma unroll
+                for (int qq = 0; qq < 15; qq++) cv[qq] = coef_val(sco[(qq * KC + warp) * TX + lane]);
+                const float *xs = xw + (WK + warp + 1) * WX + lane + 1;
+                const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
+                res = post_residual<WK * WX, WX>(rv, cv, xs);
+                x2c = xs[0];
+                cpv = ((const float *)(st + O_CP))[warp * TX + lane];
+                mv = ((const float *)(st + O_MINV))[warp * TX + lane];
+                ccv = k > 1 ? cv[CC] : 0.0f;
+            }
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&empty[s]); // this warp's reads of the stage are done
+            if (ok && it >= NR && !tc::mbar_wait(&rempty[q], ((it / NR) - 1) & 1)) {
+                atomicExch(err, 1);
+                ok = false;
+            }
+            float *rs = ring + q * SLOT;
+            rs[(0 * KC + warp) * TX + lane] = res;
+            rs[(1 * KC + warp) * TX + lane] = x2c;
+            rs[(2 * KC + warp) * TX + lane] = cpv;
+            rs[(3 * KC + warp) * TX + lane] = ccv;
+            rs[(4 * KC + warp) * TX + lane] = mv;
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&rfull[q]);
+        }
+    }
+}
+
 // Restriction of level f fused with the pre-smoothing of level c = f + 1:
 // r_c = R^T (r_f - A_f x1_f) for a tile of TX x TY coarse columns (fine x1 of
 // the children and their ring staged in shared memory; one thread sums the four
@@ -1143,6 +1373,17 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, cuuint32_t rank, co
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The tensor-copy post-smoother's form: post_tma_kernel unless
+// HICARW_MG_POST_V=2 selects post_tma2_kernel (recurrences on their own warp); read once.
+static bool post_tma_v2()
+{
+    static const bool v2 = [] {
+        const char *e = getenv("HICARW_MG_POST_V");
+        return e && e[0] == '2';
+    }();
+    return v2;
+}
+
 // Launch post_tma_kernel on a wide level; false (nothing launched) when its
 // conditions do not hold: shared memory for nz levels, 16-byte aligned arrays
 // and row pitches.  Box x coordinates: i0 + XO = 32 bx + 8, i0 + XO - 4 and
@@ -1153,7 +1394,8 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const size_t smem = smem_bytes<TR, CT>(d.nz);
+    const bool v2 = post_tma_v2();
+    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz) : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
     const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
@@ -1175,10 +1417,16 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
         return false;
     const int ntx = (d.nx + TX - 1) / TX, ntiles = ntx * d.ny;
     const int grid = std::min(ntiles, 2 * sm_count());
-    raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
     int *e = gate ? const_cast<int *>(&gate->err) : err;
-    post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
-                                                            cscale, ntx, ntiles, gate, e);
+    if (v2) {
+        raise_smem((const void *)post_tma2_kernel<TR, TO, CT>, smem);
+        post_tma2_kernel<TR, TO, CT><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out,
+                                                                      omega, cscale, ntx, ntiles, gate, e);
+    } else {
+        raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
+        post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
+                                                                cscale, ntx, ntiles, gate, e);
+    }
     g_tma_posts++;
     return true;
 }
