@@ -61,14 +61,17 @@ REF_ITERS_SOURCE = {"plain512": "the CPU oracle run to convergence on the host (
                                  "run to convergence on the GPU on this case (1245 iterations; about 13 min on "
                                  "the host cores)"}
 REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "learn128": None, "eval768": None, "batch12": None, "batch96": None}
-# DRAM bytes per interior cell of one launch of a dominant kernel, from one ncu
-# capture on a smaller case (256x256x48 = 3145728 cells); the kernel reads and
-# writes each cell's data once, so its traffic scales with the cells of the
-# workload.  mg_post_l0 is the tensor-copy post-smoother (291.86 MB per launch
-# of that case), or the register-fed one when the environment sets
-# HICARW_MG_TMA=0 (290.45 MB).
-TRAFFIC_PER_CELL = {"mg_post_l0": (290.454272e6 if os.environ.get("HICARW_MG_TMA", "1")[:1] == "0"
-                                   else 291.858944e6) / (256 * 256 * 48)}
+# DRAM bytes per interior cell of one launch of the dominant kernel, from one
+# ncu capture on a smaller case (the kernel reads and writes each cell's data
+# once, so its traffic scales with the cells of the workload), keyed by the
+# kernel and whether the Krylov vectors it reads and writes are FP64:
+#   mg_post_l0, FP64 vectors: 291.86 MB per launch at 256x256x48 (3145728 cells);
+#   mg_post_l0, FP32 vectors: 70.84 MB per launch of the same tensor-copy kernel
+#   on the 128x128x48 second level of the 256x256x48 case (786432 cells).
+# None with the register-fed smoother (HICARW_MG_TMA=0), which was not captured.
+TRAFFIC_PER_CELL = {} if os.environ.get("HICARW_MG_TMA", "1")[:1] == "0" else {
+    ("mg_post_l0", True): 291.858944e6 / (256 * 256 * 48),
+    ("mg_post_l0", False): (68.966144e6 + 1.870336e6) / (128 * 128 * 48)}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega
@@ -447,9 +450,8 @@ def profile_roofline(lib, h, stream, ncu_range: bool, cells: int, fp64_vectors: 
     ach = dom_k["bytes"] / (dom_k["ms"] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": dom_k["kernel"], "achieved": ach, "peak": peak, "unit": "GB/s",
             "frac": ach / peak, "peak_kind": peak_kind,
-            # the captured traffic is that of the FP64-vector kernels; none for another variant
-            "traffic": (TRAFFIC_PER_CELL[dom_k["kernel"]] * cells
-                        if dom_k["kernel"] in TRAFFIC_PER_CELL and fp64_vectors else None),
+            "traffic": (TRAFFIC_PER_CELL[(dom_k["kernel"], fp64_vectors)] * cells
+                        if (dom_k["kernel"], fp64_vectors) in TRAFFIC_PER_CELL else None),
             "share": dom_k["share_ms"] / tot,
             "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in p.items()} for p in prof]}
 
@@ -883,7 +885,7 @@ def batch_measure(args, wl, rank, world, dist, local, quick=False):
     import numpy as np
     import torch
     from hicar_b200 import _capi
-    from hicar_b200.batch import BatchSolver, subdomain_cases
+    from hicar_b200.batch import LEARNED_RESTART, BatchSolver, subdomain_cases
     from hicar_b200.domain import ptr
     from hicar_b200.train_unet import COMPOSITE_WEIGHTS, load_params
     from hicar_b200.wind_iterative import WindOptions
@@ -990,8 +992,8 @@ def batch_measure(args, wl, rank, world, dist, local, quick=False):
                 "config": {"workload": f"batch{bs.n}: {bs.n} subdomains, nx,ny in {wl['nxy'][0]}..{wl['nxy'][1]} "
                                        f"step {wl['nxy'][2]}, nz in {wl['nz'][0]}..{wl['nz'][1]} step {wl['nz'][2]}, "
                                        f"{bs.cells} cells, {wl['n_hills']} hills each, adv_den={wl['adv_den']}",
-                           "solver": f"batched: BiCGStab + V-cycle ({bs.n - n_learned}), FGMRES(30) + V-cycle + "
-                                     f"U-Net correction ({n_learned}); one graph launch per step",
+                           "solver": f"batched: BiCGStab + V-cycle ({bs.n - n_learned}), FGMRES({LEARNED_RESTART}) + "
+                                     f"V-cycle + U-Net correction ({n_learned}); one graph launch per step",
                            "mg_cycle": cyc, "tol_rel": TOL, "fields": "f32", "krylov": "f64",
                            "lanes": lanes, "chunk": chunk, "autotune_best_ms": tuned_ms, "kernel_autotune": kt,
                            "learned_subdomains": n_learned,
