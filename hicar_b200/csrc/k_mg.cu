@@ -973,20 +973,30 @@ __device__ __forceinline__ float post_residual_rt(double rv, const float (&cv)[1
 #endif
 }
 
-// stage_window with a runtime window shape; x1 and xc are read through L2
+// stage_window with a runtime window shape; x1 and xc are read through L2,
+// MG_BATCH elements per thread in flight
 __device__ __forceinline__ void stage_window_rt(const Dims &d, const float *x1, const Dims &dc, const float *xc, int ia,
                                                 int ja, int SX, int SY, float *s_x, float cs)
 {
     const int SP = SX * SY, nst = SP * (d.nz + 2);
-    for (int t = threadIdx.x; t < nst; t += blockDim.x) {
-        const int lx = t % SX, ly = (t / SX) % SY, k = t / SP;
-        const int i = ia + lx, j = ja + ly;
-        float a = 0.0f;
-        if (inside(d, i, k, j)) {
-            a = __ldcg(x1 + kidx(d, i, k, j));
-            if (xc) a += cs * __ldcg(xc + kidx(dc, (i + 1) >> 1, k, (j + 1) >> 1));
+    for (int base = threadIdx.x; base < nst; base += blockDim.x * MG_BATCH) {
+        float a[MG_BATCH], b[MG_BATCH];
+#pragma unroll
+        for (int u = 0; u < MG_BATCH; u++) {
+            const int t = base + u * blockDim.x;
+            const int lx = t % SX, ly = (t / SX) % SY, k = t / SP;
+            const int i = ia + lx, j = ja + ly;
+            a[u] = b[u] = 0.0f;
+            if (t < nst && inside(d, i, k, j)) {
+                a[u] = __ldcg(x1 + kidx(d, i, k, j));
+                if (xc) b[u] = __ldcg(xc + kidx(dc, (i + 1) >> 1, k, (j + 1) >> 1));
+            }
         }
-        s_x[t] = a;
+#pragma unroll
+        for (int u = 0; u < MG_BATCH; u++) {
+            const int t = base + u * blockDim.x;
+            if (t < nst) s_x[t] = xc ? a[u] + cs * b[u] : a[u];
+        }
     }
 }
 
@@ -1059,26 +1069,42 @@ __device__ void fused_post(const CoarseStep &p, int bx, int by, float *sm)
     const int i0 = bx * TX + 1, j0 = by * TY + 1;
     stage_window_rt(d, p.x1_f, p.c, p.xc, i0 - 1, j0 - 1, SX, SY, s_x, p.cscale);
     __syncthreads();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        const int c = t % TC, k = t / TC + 1;
-        const int lx = c % TX, ly = c / TX;
-        const int i = i0 + lx, j = j0 + ly;
-        float res2 = 0.0f, vc = 0.0f, vm = 0.0f, vp = 0.0f;
-        if (i <= d.nx && j <= d.ny) {
-            const long long o = kidx(d, i, k, j);
-            const float *xs = s_x + k * SP + (ly + 1) * SX + (lx + 1);
-            float cv[15];
-            load_coefs(p.coef_f, d.npad, o, cv);
-            const double rv = (double)__ldcg(p.r_f + o);
-            vm = __ldg(p.minv_f + o);
-            vp = __ldg(p.cp_f + o);
-            vc = k > 1 ? cv[CC] : 0.0f;
-            res2 = post_residual_rt(rv, cv, xs, SX, SP);
+    constexpr int FB = 2; // cells per thread whose operands are in flight together
+    for (int base = threadIdx.x; base < n; base += blockDim.x * FB) {
+        float cv[FB][15], rr[FB], vm[FB], vp[FB];
+        bool ok[FB];
+#pragma unroll
+        for (int u = 0; u < FB; u++) {
+            const int t = base + u * blockDim.x;
+            const int c = t % TC, k = t / TC + 1;
+            const int i = i0 + c % TX, j = j0 + c / TX;
+            ok[u] = t < n && i <= d.nx && j <= d.ny;
+            rr[u] = vm[u] = vp[u] = 0.0f;
+            if (ok[u]) {
+                const long long o = kidx(d, i, k, j);
+                load_coefs(p.coef_f, d.npad, o, cv[u]);
+                rr[u] = __ldcg(p.r_f + o);
+                vm[u] = __ldg(p.minv_f + o);
+                vp[u] = __ldg(p.cp_f + o);
+            }
         }
-        s_res[t] = res2;
-        s_c[t] = vc;
-        s_m[t] = vm;
-        s_cp[t] = vp;
+#pragma unroll
+        for (int u = 0; u < FB; u++) {
+            const int t = base + u * blockDim.x;
+            if (t >= n) continue;
+            const int c = t % TC, k = t / TC + 1;
+            const int lx = c % TX, ly = c / TX;
+            float res2 = 0.0f, vc = 0.0f;
+            if (ok[u]) {
+                const float *xs = s_x + k * SP + (ly + 1) * SX + (lx + 1);
+                vc = k > 1 ? cv[u][CC] : 0.0f;
+                res2 = post_residual_rt((double)rr[u], cv[u], xs, SX, SP);
+            }
+            s_res[t] = res2;
+            s_c[t] = vc;
+            s_m[t] = vm[u];
+            s_cp[t] = vp[u];
+        }
     }
     __syncthreads();
     if (threadIdx.x < TC) {
