@@ -196,7 +196,7 @@ static void mg_params(hicarw_handle *h)
 static int mg_build_tuned(hicarw_handle *h, cudaStream_t s)
 {
     if (mg_build(h->mg, h->d, h->coef, s) != 0) return -1;
-    if (h->tune_mg_feed >= 0) h->mg.use_tma = h->tune_mg_feed;
+    if (h->tune_mg_feed >= 0) h->mg.use_tma = h->tune_mg_feed ? 2 : 0;
     return 0;
 }
 
@@ -308,6 +308,7 @@ static int normalize_options(hicarw_options *o)
 extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options *opt, const hicarw_metrics *m,
                                       int mem_kind, void *stream, hicarw_handle **out)
 {
+    api_entry();
     if (!g || !m || !out || g->nx < 3 || g->ny < 3 || g->nz < 2 || !(g->dx > 0.0f)) return HICARW_ERR_ARG;
     hicarw_options o0;
     if (opt) o0 = *opt;
@@ -379,6 +380,7 @@ extern "C" int hicarw_init_iter_winds(const hicarw_grid *g, const hicarw_options
 
 extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
 {
+    api_entry();
     if (!h) return HICARW_ERR_ARG;
     cudaDeviceSynchronize();
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
@@ -412,6 +414,7 @@ extern "C" int hicarw_finalize_iter_winds(hicarw_handle *h)
 
 extern "C" int hicarw_set_options(hicarw_handle *h, const hicarw_options *opt)
 {
+    api_entry();
     if (!h || !opt) return HICARW_ERR_ARG;
     hicarw_options o = *opt;
     if (normalize_options(&o) != 0) return HICARW_ERR_ARG;
@@ -917,6 +920,7 @@ static int zero_solution(hicarw_handle *h, cudaStream_t s)
 
 extern "C" int hicarw_reset_solution(hicarw_handle *h, void *stream)
 {
+    api_entry();
     if (!h) return HICARW_ERR_ARG;
     return zero_solution(h, (cudaStream_t)stream);
 }
@@ -938,6 +942,7 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
                                       int adv_den, float *u, float *v, float *w, int mem_kind, void *stream,
                                       hicarw_stats *stats)
 {
+    api_entry();
     if (!h || !alpha || !div || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1033,6 +1038,7 @@ extern "C" int hicarw_calc_divergence(hicarw_handle *h, const float *u, const fl
                                       const float *density, float *div, int adv_den, int horz_only, int use_dqdt,
                                       int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !w || !div || (adv_den && !density)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1058,6 +1064,7 @@ extern "C" int hicarw_calc_divergence(hicarw_handle *h, const float *u, const fl
 // ---- probing -------------------------------------------------------------
 extern "C" int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int cc, void *stream)
 {
+    api_entry();
     if (!h || ca < 0 || ca > 2 || cb < 0 || cb > 2 || cc < 0 || cc > 2) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     if (x64(h)) launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
@@ -1067,6 +1074,7 @@ extern "C" int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int
 
 extern "C" int hicarw_probe_zero_corrections(hicarw_handle *h, float *u, float *v, float *w, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !w) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1084,6 +1092,7 @@ extern "C" int hicarw_probe_zero_corrections(hicarw_handle *h, float *u, float *
 extern "C" int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alpha, const float *density, int adv_den,
                                               float *u, float *v, float *w, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !alpha || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1110,6 +1119,7 @@ extern "C" int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alp
 extern "C" int hicarw_probe_record(hicarw_handle *h, const float *Tfield, int ca, int cb, int cc, float *max_leak,
                                    int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !Tfield || !max_leak) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const float *T;
@@ -1128,6 +1138,7 @@ extern "C" int hicarw_probe_record(hicarw_handle *h, const float *Tfield, int ca
 
 extern "C" int hicarw_probe_finalize(hicarw_handle *h, float max_leak, void *stream)
 {
+    api_entry();
     if (!h) return HICARW_ERR_ARG;
     h->operator_probed = 1;
     h->structure_uploaded = 1;
@@ -1144,6 +1155,7 @@ extern "C" int hicarw_calibrate_projection_operator(hicarw_handle *h, const floa
                                                     int adv_den, float *u, float *v, float *w, float *max_leak,
                                                     int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !alpha || !u || !v || !w || (adv_den && !density)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1194,6 +1206,7 @@ extern "C" int hicarw_calibrate_projection_operator(hicarw_handle *h, const floa
 // ---- extensions ----------------------------------------------------------
 extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !lambda) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1222,6 +1235,7 @@ extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind,
 
 extern "C" int hicarw_get_coefs(hicarw_handle *h, float *coefs, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !coefs) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1239,6 +1253,7 @@ extern "C" int hicarw_get_coefs(hicarw_handle *h, float *coefs, int mem_kind, vo
 
 extern "C" int hicarw_set_coefs(hicarw_handle *h, const float *coefs, int probed, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !coefs) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1277,6 +1292,7 @@ static int get_padded(hicarw_handle *h, const double *src, double *dst, int mem_
 
 extern "C" int hicarw_apply_operator(hicarw_handle *h, const double *x, double *y, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !x || !y) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1296,6 +1312,7 @@ extern "C" int hicarw_apply_operator(hicarw_handle *h, const double *x, double *
 
 extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y, int sweeps, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !x || !y) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1349,6 +1366,7 @@ extern "C" int hicarw_apply_precond(hicarw_handle *h, const double *x, double *y
 
 extern "C" int hicarw_solve_rhs(hicarw_handle *h, const double *rhs, int mem_kind, void *stream, hicarw_stats *stats)
 {
+    api_entry();
     if (!h || !rhs) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
@@ -1378,6 +1396,7 @@ extern "C" int hicarw_solve_rhs(hicarw_handle *h, const double *rhs, int mem_kin
 
 extern "C" int hicarw_get_history(hicarw_handle *h, double *out, int cap)
 {
+    api_entry();
     if (!h) return HICARW_ERR_ARG;
     int n = h->hst->it + 1;
     if (out && cap > 0) {
@@ -1405,6 +1424,7 @@ __global__ void prof_state_kernel(SolveState *s, int on)
 extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names, double *ms, double *bytes,
                                         int *per_iter, int cap, void *stream)
 {
+    api_entry();
     if (!h || reps < 1 || cap < 1) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int solver = h->opt.solver;
@@ -1480,6 +1500,7 @@ extern "C" int hicarw_profile_iteration(hicarw_handle *h, int reps, char *names,
 
 extern "C" int hicarw_set_learned_precond(hicarw_handle *h, hicarw_unet *n)
 {
+    api_entry();
     if (!h) return HICARW_ERR_ARG;
     if (n && !unet_matches(n, h->d)) {
         h->err = "learned preconditioner: network grid differs from the handle's";
@@ -1508,6 +1529,7 @@ static int ensure_work(hicarw_handle *h)
 extern "C" int hicarw_calc_w_real(hicarw_handle *h, const float *u, const float *v, const float *w_grid, float *w_real,
                                   int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !w_real || device_only(mem_kind)) return HICARW_ERR_ARG;
     launch_w_real(h->d, metrics_of(h), u, v, w_grid, w_real, (cudaStream_t)stream);
     CK(cudaGetLastError());
@@ -1517,6 +1539,7 @@ extern "C" int hicarw_calc_w_real(hicarw_handle *h, const float *u, const float 
 extern "C" int hicarw_calc_idealized_wgrid(hicarw_handle *h, const float *u, const float *v, const float *w_real,
                                            float *w, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !w_real || !w || device_only(mem_kind)) return HICARW_ERR_ARG;
     launch_idealized_wgrid(h->d, metrics_of(h), u, v, w_real, w, (cudaStream_t)stream);
     CK(cudaGetLastError());
@@ -1526,6 +1549,7 @@ extern "C" int hicarw_calc_idealized_wgrid(hicarw_handle *h, const float *u, con
 extern "C" int hicarw_balance_uvw(hicarw_handle *h, const float *u, const float *v, const float *density, float *w,
                                   int adv_den, int use_dqdt, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !w || (adv_den && !density) || device_only(mem_kind)) return HICARW_ERR_ARG;
     int rc;
     if ((rc = ensure_work(h)) != 0) return rc;
@@ -1540,6 +1564,7 @@ extern "C" int hicarw_balance_uvw(hicarw_handle *h, const float *u, const float 
 extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *alpha, int halo, int mem_kind,
                                  void *stream)
 {
+    api_entry();
     if (!h || !froude || !alpha || halo < 0 || 2 * halo >= h->d.nx || 2 * halo >= h->d.ny || device_only(mem_kind))
         return HICARW_ERR_ARG;
     launch_calc_alpha(h->d, froude, alpha, halo, (cudaStream_t)stream);
@@ -1552,6 +1577,7 @@ extern "C" int hicarw_calc_alpha(hicarw_handle *h, const float *froude, float *a
 // caller communicates (NCCL, MPI or copies) between the steps ----
 extern "C" int hicarw_dist_configure(hicarw_handle *h, int edges)
 {
+    api_entry();
     if (!h || edges < 0 || edges > 15) return HICARW_ERR_ARG;
     cudaDeviceSynchronize();
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
@@ -1565,12 +1591,6 @@ static int dist_ready(hicarw_handle *h)
 {
     if (!h || !h->dist_buf || h->opt.solver != HICARW_SOLVER_REFERENCE || h->opt.krylov_precision != HICARW_KRYLOV_F64)
         return HICARW_ERR_STATE;
-    // an error left by an earlier call of this thread is reported as such, not as this step's
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        set_err(h, "a CUDA error pending before this decomposed-solve step", e);
-        return HICARW_ERR_CUDA;
-    }
     return 0;
 }
 
@@ -1585,6 +1605,7 @@ static int dist_out(hicarw_handle *h, double *tot, int n, int mem_kind, cudaStre
 
 extern "C" int hicarw_dist_setup(hicarw_handle *h, const double *rhs, double *tot3, int mem_kind, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0 || !rhs || !tot3) return rc ? rc : HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1611,6 +1632,7 @@ extern "C" int hicarw_dist_setup(hicarw_handle *h, const double *rhs, double *to
 
 extern "C" int hicarw_dist_apply(hicarw_handle *h, int kind, const double *tot, int mem_kind, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     if (kind < 0 || kind > 2 || !tot) return HICARW_ERR_ARG;
@@ -1628,6 +1650,7 @@ extern "C" int hicarw_dist_apply(hicarw_handle *h, int kind, const double *tot, 
 
 extern "C" int hicarw_dist_precond(hicarw_handle *h, int which, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     if (which < 0 || which > 1) return HICARW_ERR_ARG;
@@ -1657,6 +1680,7 @@ extern "C" int hicarw_dist_precond(hicarw_handle *h, int which, void *stream)
 
 extern "C" int hicarw_dist_face(hicarw_handle *h, int vec, int side, double *buf, int unpack, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     if (vec < 0 || vec > 2 || side < 0 || side > 3 || !buf) return HICARW_ERR_ARG;
@@ -1668,6 +1692,7 @@ extern "C" int hicarw_dist_face(hicarw_handle *h, int vec, int side, double *buf
 
 extern "C" int hicarw_dist_spmv(hicarw_handle *h, int which, double *tot, int mem_kind, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     if (which < 0 || which > 1 || !tot) return HICARW_ERR_ARG;
@@ -1686,6 +1711,7 @@ extern "C" int hicarw_dist_spmv(hicarw_handle *h, int which, double *tot, int me
 
 extern "C" int hicarw_dist_update(hicarw_handle *h, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     double *x = V<double>(h, V_X), *r = V<double>(h, V_R), *p = V<double>(h, V_P), *phat = V<double>(h, V_PHAT),
@@ -1697,6 +1723,7 @@ extern "C" int hicarw_dist_update(hicarw_handle *h, void *stream)
 
 extern "C" int hicarw_dist_state(hicarw_handle *h, int *stop, hicarw_stats *stats, void *stream)
 {
+    api_entry();
     int rc;
     if ((rc = dist_ready(h)) != 0) return rc;
     if ((rc = fetch_state(h, (cudaStream_t)stream)) != 0) return rc;
@@ -1707,19 +1734,21 @@ extern "C" int hicarw_dist_state(hicarw_handle *h, int *stop, hicarw_stats *stat
 
 extern "C" int hicarw_set_kernel_tuning(hicarw_handle *h, int spmv_levels, int mg_post_feed)
 {
+    api_entry();
     if (!h || spmv_levels < 0 || spmv_levels > 1024 || mg_post_feed < -1 || mg_post_feed > 1) return HICARW_ERR_ARG;
     cudaDeviceSynchronize();
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second.exec);
     h->graphs.clear();
     h->tune_kc = spmv_levels;
     h->tune_mg_feed = mg_post_feed;
-    if (mg_post_feed >= 0) h->mg.use_tma = mg_post_feed;
+    if (mg_post_feed >= 0) h->mg.use_tma = mg_post_feed ? 2 : 0;
     else h->mg_dirty = 1; // the build decides again
     return HICARW_OK;
 }
 
 extern "C" int hicarw_debug_wait_timeout(hicarw_handle *h, double limit_us, void *stream)
 {
+    api_entry();
     if (!h || !(limit_us >= 1.0 && limit_us <= 100000.0)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemsetAsync(&h->st->err, 0, sizeof(int), s));
@@ -1736,6 +1765,7 @@ extern "C" int hicarw_update_stability(hicarw_handle *h, const float *u, const f
                                        const float *theta, const float *froude_terrain, int nsect, int froude_mode,
                                        float *froude, float *blk_ri, int mem_kind, void *stream)
 {
+    api_entry();
     if (!h || !u || !v || !z || !theta || !froude || !blk_ri || h->d.nz < 5 || device_only(mem_kind) ||
         (froude_mode && (!froude_terrain || nsect < 1)))
         return HICARW_ERR_ARG;
@@ -1748,6 +1778,7 @@ extern "C" int hicarw_update_stability(hicarw_handle *h, const float *u, const f
 extern "C" int hicarw_smooth_alpha(hicarw_handle *h, float *alpha, int window, int nsmooths, int mem_kind,
                                    void *stream)
 {
+    api_entry();
     if (!h || !alpha || window < 0 || nsmooths < 0 || device_only(mem_kind)) return HICARW_ERR_ARG;
     int rc;
     if ((rc = ensure_work(h)) != 0) return rc;
@@ -2051,6 +2082,7 @@ static int batch_run(hicarw_batch *b, const hicarw_batch_item *items, int adv_de
 
 extern "C" int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_batch **out)
 {
+    api_entry();
     if (n < 1 || !handles || !out) return HICARW_ERR_ARG;
     for (int i = 0; i < n; i++) {
         hicarw_handle *h = handles[i];
@@ -2078,6 +2110,7 @@ extern "C" int hicarw_batch_create(int n, hicarw_handle *const *handles, hicarw_
 
 extern "C" int hicarw_batch_destroy(hicarw_batch *b)
 {
+    api_entry();
     if (!b) return HICARW_ERR_ARG;
     cudaDeviceSynchronize();
     batch_drop_graph(b);
@@ -2092,6 +2125,7 @@ extern "C" int hicarw_batch_destroy(hicarw_batch *b)
 
 extern "C" int hicarw_batch_config(hicarw_batch *b, int lanes, int chunk)
 {
+    api_entry();
     if (!b || chunk < 1 || chunk > 64) return HICARW_ERR_ARG;
     b->lanes = lanes;
     b->chunk = chunk;
@@ -2100,6 +2134,7 @@ extern "C" int hicarw_batch_config(hicarw_batch *b, int lanes, int chunk)
 
 extern "C" int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *chunk)
 {
+    api_entry();
     if (!b) return HICARW_ERR_ARG;
     if (lanes) *lanes = b->lanes <= 0 ? (int)b->hs.size() : b->lanes;
     if (chunk) *chunk = b->chunk;
@@ -2109,6 +2144,7 @@ extern "C" int hicarw_batch_get_config(const hicarw_batch *b, int *lanes, int *c
 extern "C" int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, int cold,
                                             void *stream, hicarw_stats *stats)
 {
+    api_entry();
     if (!b || !items) return HICARW_ERR_ARG;
     for (size_t i = 0; i < b->hs.size(); i++)
         if (!items[i].alpha || !items[i].div || !items[i].u || !items[i].v || !items[i].w ||
@@ -2121,6 +2157,7 @@ extern "C" int hicarw_batch_calc_iter_winds(hicarw_batch *b, const hicarw_batch_
 // start of the batch graph to the end of that subdomain's solve loop.
 extern "C" int hicarw_batch_latencies(hicarw_batch *b, double *ms)
 {
+    api_entry();
     if (!b || !ms || !b->exec) return HICARW_ERR_ARG;
     const int n = (int)b->hs.size();
     std::vector<unsigned long long> t(n + 1);
@@ -2134,6 +2171,7 @@ extern "C" int hicarw_batch_latencies(hicarw_batch *b, double *ms)
 extern "C" int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int adv_den, void *stream,
                                      double *best_ms)
 {
+    api_entry();
     if (!b || !items) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int n = (int)b->hs.size();

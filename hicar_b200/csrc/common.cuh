@@ -98,4 +98,11 @@ __host__ __device__ __forceinline__ bool owned_row(const Dims &d, int edges, int
 
 constexpr double BREAKDOWN_EPS = 1.0e-30; // wind_iterative.F90:61
 
+// Every C entry point starts here: it clears an error that an earlier CUDA call
+// of the calling thread left pending (the host program's own, or another
+// library's), so that the entry point's launch checks report its own errors
+// only.  An error that breaks the context comes back from the next call that
+// touches the device.
+inline void api_entry() { (void)cudaGetLastError(); }
+
 }  // namespace hw

@@ -213,12 +213,15 @@ __device__ __forceinline__ double stencil_regs(const float (&cv)[15], const floa
     return y;
 }
 
-// The post-smoothers' residual r - A x2 of one cell (post_kernel, post_tma_kernel
-// and the fused coarse cycle's post steps, which must agree bit for bit).
-// HICARW_MG_POST_F32: FP32 products and sums in the fixed term order (fmaf),
-// one rounding of the difference; otherwise exact products summed in FP64.
+// The post-smoothers' residual r - A x2 of one cell (post_kernel, the
+// tensor-copy kernels and the fused coarse cycle's post steps, which must agree
+// bit for bit).  HICARW_MG_POST_F32 = 1 (the default): FP32 products and sums in
+// the fixed term order (fmaf), one rounding of the difference; 0: exact
+// products summed in FP64 (the restriction's sums stay FP64 either way).
+// Measured at 1024x1024x64 with the benchmark's cycle: the same 10 iterations,
+// the level-0 post-smoother 1.59 -> 1.41 ms per launch.
 #ifndef HICARW_MG_POST_F32
-#define HICARW_MG_POST_F32 0
+#define HICARW_MG_POST_F32 1
 #endif
 template <int SX, int SP>
 __device__ __forceinline__ float post_residual(double rv, const float (&cv)[15], const float *xs)
@@ -768,6 +771,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
         const bool col = i0 + lane <= d.nx;
+        // window columns i0 - 1 + lane and i0 + 31 + lane inside the interior
+        const bool in0 = i0 - 1 + lane >= 1 && i0 - 1 + lane <= d.nx, in1 = i0 + 31 + lane <= d.nx;
         for (int ch = 0; ch < nch; ch++, it++) {
             const int s = it % NS, q = it % NR;
             const unsigned char *st = base + s * SB;
@@ -776,18 +781,31 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 ok = false;
             }
             const int k0 = 1 + ch * KC;
-            // x2 = x1 + s P xc on the chunk's window, zero outside the interior
+            // x2 = x1 + s P xc on the chunk's window, zero outside the interior: the
+            // window's 3 x WK rows (j, k) go round the warps, a row's WX = 34
+            // columns are the lanes (and lanes 0-1 once more for columns 32, 33)
             float *xw = s_x2w + (it & 1) * pt2::XW;
             const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
-            for (int e = tid; e < 3 * WK * WX; e += CW) {
-                const int cc = e % WX, kw = (e / WX) % WK, jj = e / (WX * WK);
-                const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
+            for (int row = warp; row < 3 * WK; row += KC) {
+                const int jj = row / WK, kw = row - jj * WK;
+                const int kq = k0 - 1 + kw, jq = j - 1 + jj;
+                const bool rok = jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz;
+                const float *x1r = sx1 + row * X1W + 3;
+                const float *xcr = sxc + ((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + 3;
                 float a = 0.0f;
-                if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
-                    a = sx1[(jj * WK + kw) * X1W + cc + 3];
-                    a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
+                if (rok && in0) {
+                    a = x1r[lane];
+                    a += cscale * xcr[(lane + 1) >> 1];
                 }
-                xw[e] = a;
+                xw[row * WX + lane] = a;
+                if (lane < WX - 32) {
+                    float b = 0.0f;
+                    if (rok && in1) {
+                        b = x1r[32 + lane];
+                        b += cscale * xcr[(33 + lane) >> 1];
+                    }
+                    xw[row * WX + 32 + lane] = b;
+                }
             }
             // every consumer has finished the previous chunk (whose window buffer the next chunk reuses)
             tc::named_sync(1, CW);
@@ -1232,7 +1250,7 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
     if (!mg.pre0 && mg.nlev > 0) // V(0,1) on the finest level: its x1 must read as zero
         cudaMemsetAsync(mg.lev[0].x1, 0, (size_t)mg.lev[0].d.npad * sizeof(float), s);
     const char *tma = getenv("HICARW_MG_TMA");
-    mg.use_tma = !(tma && tma[0] == '0');
+    mg.use_tma = tma && tma[0] == '0' ? 0 : tma && tma[0] == '1' ? 1 : 2;
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
         sm_count();
         smem_optin();
@@ -1399,28 +1417,16 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, cuuint32_t rank, co
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// The tensor-copy post-smoother's form: post_tma_kernel unless
-// HICARW_MG_POST_V=2 selects post_tma2_kernel (recurrences on their own warp); read once.
-static bool post_tma_v2()
-{
-    static const bool v2 = [] {
-        const char *e = getenv("HICARW_MG_POST_V");
-        return e && e[0] == '2';
-    }();
-    return v2;
-}
-
-// Launch post_tma_kernel on a wide level; false (nothing launched) when its
+// Launch post_tma2_kernel (v2) or post_tma_kernel on a wide level; false (nothing launched) when its
 // conditions do not hold: shared memory for nz levels, 16-byte aligned arrays
 // and row pitches.  Box x coordinates: i0 + XO = 32 bx + 8, i0 + XO - 4 and
 // (i0 >> 1) + XO - 3 = 16 bx + 4, all multiples of 4 floats (2 doubles).
 template <typename TR, typename TO, typename CT = float>
 static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
-                     float cscale, const SolveState *gate, int *err, cudaStream_t s)
+                     float cscale, const SolveState *gate, int *err, cudaStream_t s, bool v2)
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const bool v2 = post_tma_v2();
     const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz) : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
@@ -1467,10 +1473,10 @@ static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel 
     ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + (coefh ? 30.0 : 60.0) + 4.0 + 1.0 + 8.0) * N, s);
     if (coefh) {
         if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, coefh, r, C, out, omega, cscale, gate, s);
-        else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s)))
+        else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s, use_tma == 2)))
             post_t<TR, TO, 32, 1>(L, coefh, r, C, out, omega, cscale, gate, s);
     } else if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, L.coef, r, C, out, omega, cscale, gate, s);
-    else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s)))
+    else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s, use_tma == 2)))
         post_t<TR, TO, 32, 1>(L, L.coef, r, C, out, omega, cscale, gate, s);
     count_launch(1);
 }
@@ -1601,14 +1607,15 @@ static cudaLaunchConfig_t fused_config(int cn, size_t smem, cudaStream_t s, cuda
 }
 
 // Decide at build time (outside any stream capture) whether and where the
-// coarse part is fused, and the cluster size: 16 CTAs where the device can
-// place such a cluster with this shared memory, else 8, else no fusion.
+// coarse part is fused (HICARW_MG_FUSE=1 in the environment), and the cluster
+// size: 16 CTAs where the device can place such a cluster with this shared
+// memory, else 8, else no fusion.
 static void fused_setup(Mg &mg)
 {
     mg.fuse_level = 0;
     mg.cluster_n = 0;
     const char *e = getenv("HICARW_MG_FUSE");
-    if (e && e[0] == '0') return;
+    if (!(e && e[0] == '1')) return; // opt-in: the per-level launches measured faster in a graph
     int l0 = 0;
     for (int l = 2; l + 1 < mg.nlev; l++)
         if ((long long)mg.lev[l].d.nx * mg.lev[l].d.ny <= MG_FUSE_COLS) {

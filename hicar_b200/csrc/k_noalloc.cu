@@ -175,6 +175,7 @@ static const char *noalloc_scratch(NoallocScratch **out)
 extern "C" int hicarw_residual_norm_noalloc(hicarw_handle *h, const double *x, const double *rhs, double *norm,
                                             void *stream)
 {
+    api_entry();
     if (!h || !x || !rhs || !norm) return HICARW_ERR_ARG;
     OpCtx c;
     handle_operator(h, &c);

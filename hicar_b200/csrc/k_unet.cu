@@ -554,6 +554,7 @@ static int ualloc(hicarw_unet *n, void **p, size_t bytes)
 
 extern "C" int hicarw_unet_destroy(hicarw_unet *n)
 {
+    api_entry();
     if (!n) return HICARW_ERR_ARG;
     cudaDeviceSynchronize();
     for (void *p : n->allocs) cudaFree(p);
@@ -563,6 +564,7 @@ extern "C" int hicarw_unet_destroy(hicarw_unet *n)
 
 extern "C" int hicarw_unet_create(int nx, int ny, int nz, unsigned long long seed, hicarw_unet **out)
 {
+    api_entry();
     if (!out || nx < 1 || ny < 1 || nz < 1) return HICARW_ERR_ARG;
     hicarw_unet *n = new hicarw_unet();
     n->nx[0] = nx;
@@ -678,10 +680,12 @@ static cudaMemcpyKind kind_of(int mem_kind, bool to_device)
     return cudaMemcpyDeviceToDevice;
 }
 
-extern "C" long long hicarw_unet_num_params(const hicarw_unet *n) { return n ? (long long)n->nparam : -1; }
+extern "C" long long hicarw_unet_num_params(const hicarw_unet *n) {
+    api_entry(); return n ? (long long)n->nparam : -1; }
 
 extern "C" int hicarw_unet_grid(const hicarw_unet *n, int *nx, int *ny, int *nz)
 {
+    api_entry();
     if (!n) return HICARW_ERR_ARG;
     if (nx) *nx = n->nx[0];
     if (ny) *ny = n->ny[0];
@@ -691,6 +695,7 @@ extern "C" int hicarw_unet_grid(const hicarw_unet *n, int *nx, int *ny, int *nz)
 
 extern "C" int hicarw_unet_get_params(hicarw_unet *n, float *out, int mem_kind, void *stream)
 {
+    api_entry();
     if (!n || !out) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemcpyAsync(out, n->P, n->nparam * 4, kind_of(mem_kind, false), s);
@@ -699,6 +704,7 @@ extern "C" int hicarw_unet_get_params(hicarw_unet *n, float *out, int mem_kind, 
 
 extern "C" int hicarw_unet_set_params(hicarw_unet *n, const float *in, int mem_kind, void *stream)
 {
+    api_entry();
     if (!n || !in) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemcpyAsync(n->P, in, n->nparam * 4, kind_of(mem_kind, true), s);
@@ -708,6 +714,7 @@ extern "C" int hicarw_unet_set_params(hicarw_unet *n, const float *in, int mem_k
 
 extern "C" int hicarw_unet_get_grads(hicarw_unet *n, float *out, int mem_kind, void *stream)
 {
+    api_entry();
     if (!n || !out) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemcpyAsync(out, n->Gr, n->nparam * 4, kind_of(mem_kind, false), s);
@@ -716,6 +723,7 @@ extern "C" int hicarw_unet_get_grads(hicarw_unet *n, float *out, int mem_kind, v
 
 extern "C" int hicarw_unet_zero_grads(hicarw_unet *n, void *stream)
 {
+    api_entry();
     if (!n) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(n->Gr, 0, n->nparam * 4, s);
@@ -725,6 +733,7 @@ extern "C" int hicarw_unet_zero_grads(hicarw_unet *n, void *stream)
 
 extern "C" int hicarw_unet_forward(hicarw_unet *n, const void *x0, float *out0, void *stream)
 {
+    api_entry();
     if (!n || !x0) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(n->err, 0, 4, s);
@@ -735,6 +744,7 @@ extern "C" int hicarw_unet_forward(hicarw_unet *n, const void *x0, float *out0, 
 
 extern "C" int hicarw_unet_backward(hicarw_unet *n, const float *target, float weight, float *loss, void *stream)
 {
+    api_entry();
     if (!n || !target || !n->x_in) return HICARW_ERR_ARG;
     if (ensure_grads(n)) return HICARW_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
@@ -747,6 +757,7 @@ extern "C" int hicarw_unet_backward(hicarw_unet *n, const float *target, float w
 extern "C" int hicarw_unet_backward_residual(hicarw_unet *n, const float *coef, const float *rhat, float weight,
                                              float *loss, void *stream)
 {
+    api_entry();
     if (!n || !coef || !rhat || !n->x_in) return HICARW_ERR_ARG;
     if (ensure_grads(n)) return HICARW_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
@@ -758,6 +769,7 @@ extern "C" int hicarw_unet_backward_residual(hicarw_unet *n, const float *coef, 
 
 extern "C" int hicarw_unet_adam_step(hicarw_unet *n, float lr, void *stream)
 {
+    api_entry();
     if (!n || n->nsamples < 1) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     n->adam_t++;
@@ -774,6 +786,7 @@ extern "C" int hicarw_unet_adam_step(hicarw_unet *n, float lr, void *stream)
 extern "C" int hicarw_unet_features(hicarw_unet *n, hicarw_handle *h, const double *r, void *x0, float *rms,
                                     void *stream)
 {
+    api_entry();
     if (!n || !h || !r || !x0) return HICARW_ERR_ARG;
     OpCtx c;
     handle_operator(h, &c);
@@ -791,6 +804,7 @@ extern "C" int hicarw_unet_features(hicarw_unet *n, hicarw_handle *h, const doub
 
 extern "C" int hicarw_unet_apply(hicarw_unet *n, hicarw_handle *h, const double *r, double *z, void *stream)
 {
+    api_entry();
     if (!n || !h || !r || !z) return HICARW_ERR_ARG;
     OpCtx c;
     handle_operator(h, &c);
@@ -810,6 +824,7 @@ extern "C" int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const 
                                const float *bias, const void *skip, const void *mask, int relu, int transpose, void *out,
                                float *out0, void *stream)
 {
+    api_entry();
     if (nx <= 0 || ny <= 0 || nz <= 0 || !in || !w || (!out && !out0)) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int ci = transpose ? cout : cin, co = transpose ? cin : cout;
@@ -859,6 +874,7 @@ extern "C" int hicarw_nn_conv3(int cin, int cout, int nx, int ny, int nz, const 
 extern "C" int hicarw_nn_conv3_time(int cin, int cout, int nx, int ny, int nz, const void *in, const float *w,
                                     const float *bias, void *out, int reps, void *stream, float *ms)
 {
+    api_entry();
     if (nx <= 0 || ny <= 0 || nz <= 0 || !in || !w || !out || reps < 1 || !ms) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     uint4 *img = nullptr;
@@ -902,6 +918,7 @@ extern "C" int hicarw_nn_conv3_time(int cin, int cout, int nx, int ny, int nz, c
 extern "C" int hicarw_nn_conv3_wgrad(int cin, int cout, int nx, int ny, int nz, const void *x, const void *dy, float *dw,
                                      float *db, void *stream)
 {
+    api_entry();
     if (nx <= 0 || ny <= 0 || nz <= 0 || !x || !dy || !dw || !db) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     int *err = nullptr;

@@ -25,7 +25,9 @@ struct Mg {
     float cscale = 1.0f; // scale of the prolongated coarse-grid correction (over-correction > 1)
     int pre0 = 1;        // pre-smooth the finest level (0: V(0,1) there, its x1 kept at zero)
     int wmask = 0;       // bit l (l >= 1): level l corrects twice from the coarse grid (W-cycle there)
-    int use_tma = 1;     // post-smoothers of the wide levels fed by tensor copies (HICARW_MG_TMA=0: register-fed)
+    int use_tma = 2;     // post-smoothers of the wide levels: 2 tensor copies, recurrences on their own warp
+                         // (post_tma2_kernel); 1 tensor copies, post_tma_kernel (HICARW_MG_TMA=1);
+                         // 0 register-fed (HICARW_MG_TMA=0)
     int fuse_level = 0;  // first level of the coarse part run by one thread-block cluster (0: every level its own
                          // launches; HICARW_MG_FUSE=0 at build time)
     int cluster_n = 0;   // CTAs of that cluster

@@ -123,10 +123,12 @@ def test_stall_falls_back_to_reference_solve(case):
 
 
 def _fresh_handle(case, monkeypatch, tma):
-    """A new handle whose V-cycle is built with the tensor-copy post-smoother
-    switched on (tma=True) or off (the register-fed kernel)."""
+    """A new handle whose V-cycle is built with the given post-smoother of the
+    wide levels: "0" register-fed, "1" tensor copies with the recurrences on
+    the consumer warps (post_tma_kernel), "2" tensor copies with the
+    recurrences on their own warp (post_tma2_kernel, the default)."""
     from hicar_b200 import wind, wind_iterative as wi
-    monkeypatch.setenv("HICARW_MG_TMA", "1" if tma else "0")
+    monkeypatch.setenv("HICARW_MG_TMA", tma)
     wi.finalize_iter_winds()
     wind.reset()
     return _calibrated(case)
@@ -134,7 +136,7 @@ def _fresh_handle(case, monkeypatch, tma):
 
 @pytest.mark.parametrize("shape", [(131, 75, 21), (128, 96, 16)])
 def test_tma_post_smoother_matches_register_path(shape, monkeypatch):
-    """The post-smoother fed by tensor copies (wide levels: here the finest)
+    """Both post-smoothers fed by tensor copies (wide levels: here the finest)
     against the register-fed kernel on the same V-cycle input: bit-identical,
     on a ragged grid (nx not a multiple of the 32-column tile, odd nx and ny,
     nz not a multiple of the 8-level chunk) and a regular one; and against the
@@ -148,19 +150,20 @@ def test_tma_post_smoother_matches_register_path(shape, monkeypatch):
     x = np.zeros((ny + 2, nz + 2, nx + 2))
     x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
     out = {}
-    for tma in (False, True):
+    for tma in ("0", "1", "2"):
         dom, _, _, _ = _fresh_handle(case, monkeypatch, tma)
         h = wi.handle(dom.nest_indx)
         n0 = lib.hicarw_mg_tma_launches()
         y = np.empty_like(x)
         _capi.check(lib.hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
         out[tma] = (y, lib.hicarw_mg_tma_launches() - n0, _coefs(dom))
-    assert out[False][1] == 0 and out[True][1] >= 1
-    np.testing.assert_array_equal(out[True][2], out[False][2])
-    np.testing.assert_array_equal(out[True][0], out[False][0])
-    ref = mg_ref.VCycle(out[True][2], 0.8)(x[1:-1, 1:-1, 1:-1])
-    assert _rel(out[True][0][1:-1, 1:-1, 1:-1], ref) < 1e-5
-    y = out[True][0]
+    assert out["0"][1] == 0 and out["1"][1] >= 1 and out["2"][1] >= 1
+    for tma in ("1", "2"):
+        np.testing.assert_array_equal(out[tma][2], out["0"][2])
+        np.testing.assert_array_equal(out[tma][0], out["0"][0])
+    ref = mg_ref.VCycle(out["2"][2], 0.8)(x[1:-1, 1:-1, 1:-1])
+    assert _rel(out["2"][0][1:-1, 1:-1, 1:-1], ref) < 1e-5
+    y = out["2"][0]
     assert not y[0].any() and not y[-1].any() and not y[:, 0].any() and not y[:, -1].any()
     assert not y[:, :, 0].any() and not y[:, :, -1].any()
 
@@ -173,7 +176,7 @@ def test_tma_post_smoother_solve_identical(monkeypatch):
     case = cases.build_case(131, 75, 21, seed=8, adv_den=True, n_hills=12)
     lib = _capi.load()
     res = {}
-    for tma in (False, True):
+    for tma in ("0", "1", "2"):
         dom, _, div, _ = _fresh_handle(case, monkeypatch, tma)
         h = wi.handle(dom.nest_indx)
         wi.set_options(wi.WindOptions(tol_rel=1e-8, precond=_capi.PRECOND_MG, stall_iters=50))
@@ -185,8 +188,9 @@ def test_tma_post_smoother_solve_identical(monkeypatch):
         lam = np.empty((dom.ny + 2, dom.nz + 2, dom.nx + 2))
         _capi.check(lib.hicarw_get_lambda(h, lam.ctypes.data, _capi.MEM_HOST, None), h)
         res[tma] = (st, lam, lib.hicarw_mg_tma_launches() - n0)
-    assert res[False][2] == 0 and res[True][2] >= 1
-    for tma in (False, True):
+    assert res["0"][2] == 0 and res["1"][2] >= 1 and res["2"][2] >= 1
+    for tma in ("0", "1", "2"):
         assert res[tma][0]["status"] == 0 and res[tma][0]["precond"] == _capi.PRECOND_MG
-    assert res[True][0]["iterations"] == res[False][0]["iterations"]
-    np.testing.assert_array_equal(res[True][1], res[False][1])
+    for tma in ("1", "2"):
+        assert res[tma][0]["iterations"] == res["0"][0]["iterations"]
+        np.testing.assert_array_equal(res[tma][1], res["0"][1])
