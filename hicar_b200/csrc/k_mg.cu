@@ -600,29 +600,31 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // ---------------------------------------------------------------------------
 // Post-smoothing fed by tensor copies, with the column recurrences moved off
 // the consumers' path.  The producer warp and the stage layout are those of
-// post_tma_kernel (two stages).  Eight consumer warps form x2 on the chunk's
+// post_tma_kernel (three stages).  Eight consumer warps form x2 on the chunk's
 // window (double-buffered, so one CTA barrier per chunk) and the residuals,
-// release the stage as soon as their reads are done, and hand each chunk's
-// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a two-slot
-// ring.  The recurrence warp owns the tile's column arrays: it runs the forward
-// recurrence chunk by chunk and, at the end of a tile, the backward one,
-// writing each cell's result as soon as it is known; the consumers go on with
-// the next tile meanwhile.  Same statements per cell as post_tma_kernel, so
-// the results are bit-identical.  Every wait is bounded (on timeout: *err set,
-// the loops run to their end without waiting).
+// and hand each chunk's residual and x2 rows to a recurrence warp through a
+// two-slot ring.  The recurrence warp reads the chunk's cp, c and 1/m from the
+// stage, releases the stage, and owns the tile's column arrays: it runs the
+// forward recurrence chunk by chunk and, at the end of a tile, the backward
+// one, writing each cell's result as soon as it is known; the consumers go on
+// with the next tile meanwhile.  x1z: the iterate x1 is zero (the finest level
+// without pre-smoothing), so its window is neither loaded nor read.  Same
+// statements per cell as post_tma_kernel, so the results are bit-identical.
+// Every wait is bounded (on timeout: *err set, the loops run to their end
+// without waiting).
 // ---------------------------------------------------------------------------
 namespace pt2 {
-constexpr int NS = 2;                      // stages
+constexpr int NS = 3;                      // stages at most (the launch picks 2 or 3: two CTAs per SM)
 constexpr int NR = 2;                      // ring slots
 constexpr int RW = pt::KC;                 // recurrence warp
 constexpr int PW = pt::KC + 1;             // producer warp
 constexpr int THREADS = pt::CW + 64;
-constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
+constexpr int RING_ROWS = 2;               // residual, x2
 constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
 constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
-template <typename TR, typename CT> size_t smem_bytes(int nz)
+template <typename TR, typename CT> size_t smem_bytes(int nz, int ns)
 {
-    return 128 + (size_t)NS * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
+    return 128 + (size_t)ns * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
            (size_t)2 * XW * 4 + 2 * (NS + NR) * 8 + 16;
 }
 }  // namespace pt2
@@ -632,11 +634,10 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     post_tma2_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
                      const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
                      const __grid_constant__ CUtensorMap tm_x1, const __grid_constant__ CUtensorMap tm_xc, Dims d,
-                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, const SolveState *gate,
-                     int *err)
+                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, int x1z, int NS,
+                     const SolveState *gate, int *err)
 {
     using namespace pt;
-    using pt2::NS;
     using pt2::NR;
     constexpr int SB = stage_bytes<TR, CT>();
     constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(), O_XC = o_xc<CT>(),
@@ -651,8 +652,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     float *s_x2c = s_cp + nz * TX;
     float *s_x2w = s_x2c + nz * TX; // two window buffers of pt2::XW floats
     uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
-    uint64_t *empty = full + NS;
-    uint64_t *rfull = empty + NS;
+    uint64_t *empty = full + pt2::NS;
+    uint64_t *rfull = empty + pt2::NS;
     uint64_t *rempty = rfull + NR;
     int *s_skip = (int *)(rempty + NR);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -660,10 +661,10 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
         s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
         for (int q = 0; q < NS; q++) {
             tc::mbar_init(&full[q], 1);
-            tc::mbar_init(&empty[q], KC); // one arrival per consumer warp
+            tc::mbar_init(&empty[q], 1); // the recurrence warp releases a stage
         }
         for (int q = 0; q < NR; q++) {
-            tc::mbar_init(&rfull[q], KC);
+            tc::mbar_init(&rfull[q], KC); // one arrival per consumer warp
             tc::mbar_init(&rempty[q], 1);
         }
         tc::mbar_fence_init();
@@ -673,6 +674,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
 
     if (warp == pt2::PW) { // ---- producer ----
         if (lane != 0) return;
+        const uint32_t txb = tx_bytes<TR, CT>() - (x1z ? (uint32_t)B_X1 : 0u);
         bool ok = true;
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -686,11 +688,11 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 }
                 unsigned char *st = base + s * SB;
                 const int k0 = 1 + ch * KC, row = j * d.mz + k0;
-                tc::mbar_expect_tx(&full[s], tx_bytes<TR, CT>());
+                tc::mbar_expect_tx(&full[s], txb);
                 tc::tma_load_3d(st + O_COEF, &tm_coef, i0 + XO, row, 0, &full[s]);
                 tc::tma_load_2d(st + O_MINV, &tm_minv, i0 + XO, row, &full[s]);
                 tc::tma_load_2d(st + O_CP, &tm_cp, i0 + XO, row, &full[s]);
-                tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
+                if (!x1z) tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
                 tc::tma_load_3d(st + O_XC, &tm_xc, (i0 >> 1) + XO - 3, k0 - 1, j >> 1, &full[s]);
                 tc::tma_load_2d(st + O_R, &tm_r, i0 + XO, row, &full[s]);
             }
@@ -709,23 +711,32 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
             const bool col = i <= d.nx;
             float dprev = 0.0f;
             for (int ch = 0; ch < nch; ch++, it++) {
-                const int q = it % NR;
+                const int q = it % NR, s = it % NS;
                 if (ok && !tc::mbar_wait(&rfull[q], (it / NR) & 1)) {
                     atomicExch(err, 1);
                     ok = false;
                 }
                 const float *rs = ring + q * SLOT;
+                const unsigned char *st = base + s * SB;
+                const CT *sco = (const CT *)(st + O_COEF);
+                const float *smv = (const float *)(st + O_MINV), *scp = (const float *)(st + O_CP);
                 const int k0 = 1 + ch * KC;
-                if (col) {
-                    float rv[KC], xv[KC], pv[KC], cv[KC], mv[KC];
+                float rv[KC], xv[KC], pv[KC], cv[KC], mv[KC];
 #pragma unroll
-                    for (int u = 0; u < KC; u++) {
-                        rv[u] = rs[(0 * KC + u) * TX + lane];
-                        xv[u] = rs[(1 * KC + u) * TX + lane];
-                        pv[u] = rs[(2 * KC + u) * TX + lane];
-                        cv[u] = rs[(3 * KC + u) * TX + lane];
-                        mv[u] = rs[(4 * KC + u) * TX + lane];
-                    }
+                for (int u = 0; u < KC; u++) {
+                    const int kq = k0 + u;
+                    rv[u] = rs[u * TX + lane];
+                    xv[u] = rs[(KC + u) * TX + lane];
+                    pv[u] = scp[u * TX + lane];
+                    cv[u] = kq > 1 ? coef_val(sco[(CC * KC + u) * TX + lane]) : 0.0f;
+                    mv[u] = smv[u * TX + lane];
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    tc::mbar_arrive(&rempty[q]); // the ring slot and the stage are read
+                    tc::mbar_arrive(&empty[s]);
+                }
+                if (col) {
 #pragma unroll
                     for (int u = 0; u < KC; u++) {
                         if (k0 + u > nz) break;
@@ -736,8 +747,6 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                         s_x2c[t] = xv[u];
                     }
                 }
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&rempty[q]);
             }
             if (col) { // backward recurrence, each level's result written as soon as it is known
                 float y = 0.0f;
@@ -771,8 +780,6 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
         const bool col = i0 + lane <= d.nx;
-        // window columns i0 - 1 + lane and i0 + 31 + lane inside the interior
-        const bool in0 = i0 - 1 + lane >= 1 && i0 - 1 + lane <= d.nx, in1 = i0 + 31 + lane <= d.nx;
         for (int ch = 0; ch < nch; ch++, it++) {
             const int s = it % NS, q = it % NR;
             const unsigned char *st = base + s * SB;
@@ -781,36 +788,23 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 ok = false;
             }
             const int k0 = 1 + ch * KC;
-            // x2 = x1 + s P xc on the chunk's window, zero outside the interior: the
-            // window's 3 x WK rows (j, k) go round the warps, a row's WX = 34
-            // columns are the lanes (and lanes 0-1 once more for columns 32, 33)
+            // x2 = x1 + s P xc on the chunk's window, zero outside the interior
             float *xw = s_x2w + (it & 1) * pt2::XW;
             const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
-            for (int row = warp; row < 3 * WK; row += KC) {
-                const int jj = row / WK, kw = row - jj * WK;
-                const int kq = k0 - 1 + kw, jq = j - 1 + jj;
-                const bool rok = jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz;
-                const float *x1r = sx1 + row * X1W + 3;
-                const float *xcr = sxc + ((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + 3;
+            for (int e = tid; e < 3 * WK * WX; e += CW) {
+                const int cc = e % WX, kw = (e / WX) % WK, jj = e / (WX * WK);
+                const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
                 float a = 0.0f;
-                if (rok && in0) {
-                    a = x1r[lane];
-                    a += cscale * xcr[(lane + 1) >> 1];
+                if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
+                    if (!x1z) a = sx1[(jj * WK + kw) * X1W + cc + 3];
+                    a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
                 }
-                xw[row * WX + lane] = a;
-                if (lane < WX - 32) {
-                    float b = 0.0f;
-                    if (rok && in1) {
-                        b = x1r[32 + lane];
-                        b += cscale * xcr[(33 + lane) >> 1];
-                    }
-                    xw[row * WX + 32 + lane] = b;
-                }
+                xw[e] = a;
             }
             // every consumer has finished the previous chunk (whose window buffer the next chunk reuses)
             tc::named_sync(1, CW);
             const int k = k0 + warp;
-            float res = 0.0f, x2c = 0.0f, cpv = 0.0f, ccv = 0.0f, mv = 0.0f;
+            float res = 0.0f, x2c = 0.0f;
             if (k <= nz && col) {
                 const CT *sco = (const CT *)(st + O_COEF);
                 float cv[15];
@@ -820,24 +814,16 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
                 res = post_residual<WK * WX, WX>(rv, cv, xs);
                 x2c = xs[0];
-                cpv = ((const float *)(st + O_CP))[warp * TX + lane];
-                mv = ((const float *)(st + O_MINV))[warp * TX + lane];
-                ccv = k > 1 ? cv[CC] : 0.0f;
             }
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&empty[s]); // this warp's reads of the stage are done
             if (ok && it >= NR && !tc::mbar_wait(&rempty[q], ((it / NR) - 1) & 1)) {
                 atomicExch(err, 1);
                 ok = false;
             }
             float *rs = ring + q * SLOT;
-            rs[(0 * KC + warp) * TX + lane] = res;
-            rs[(1 * KC + warp) * TX + lane] = x2c;
-            rs[(2 * KC + warp) * TX + lane] = cpv;
-            rs[(3 * KC + warp) * TX + lane] = ccv;
-            rs[(4 * KC + warp) * TX + lane] = mv;
+            rs[warp * TX + lane] = res;
+            rs[(KC + warp) * TX + lane] = x2c;
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&rfull[q]);
+            if (lane == 0) tc::mbar_arrive(&rfull[q]); // this warp's reads of the stage are done too
         }
     }
 }
@@ -1198,6 +1184,7 @@ void mg_free(Mg &mg)
 
 static int sm_count();
 static int smem_optin();
+static int smem_per_sm();
 static void fused_setup(Mg &mg);
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
@@ -1254,6 +1241,7 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
         sm_count();
         smem_optin();
+        smem_per_sm();
         if (!tensor_map_encoder()) mg.use_tma = 0;
     }
     mg.lev[0].coef = fine_coef;
@@ -1384,6 +1372,17 @@ static int smem_optin()
     return n;
 }
 
+static int smem_per_sm()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    }
+    return n;
+}
+
 // The driver's tensor-map encoder, looked up through the runtime so that the
 // library does not link the driver library itself (nullptr if unavailable).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
@@ -1423,11 +1422,13 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, cuuint32_t rank, co
 // (i0 >> 1) + XO - 3 = 16 bx + 4, all multiples of 4 floats (2 doubles).
 template <typename TR, typename TO, typename CT = float>
 static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
-                     float cscale, const SolveState *gate, int *err, cudaStream_t s, bool v2)
+                     float cscale, const SolveState *gate, int *err, cudaStream_t s, bool v2, bool x1z)
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz) : smem_bytes<TR, CT>(d.nz);
+    // v2: three stages where two CTAs per SM still fit, else two
+    const int ns2 = pt2::smem_bytes<TR, CT>(d.nz, 3) + 1024 <= (size_t)smem_per_sm() / 2 ? 3 : 2;
+    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz, ns2) : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
     const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
@@ -1453,7 +1454,8 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
     if (v2) {
         raise_smem((const void *)post_tma2_kernel<TR, TO, CT>, smem);
         post_tma2_kernel<TR, TO, CT><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out,
-                                                                      omega, cscale, ntx, ntiles, gate, e);
+                                                                      omega, cscale, ntx, ntiles, x1z ? 1 : 0,
+                                                                      ns2, gate, e);
     } else {
         raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
         post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
@@ -1463,20 +1465,24 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
     return true;
 }
 
-// coefh: the level's coefficients in BF16 (the finest level with mg_precision BF16), else nullptr
+// coefh: the level's coefficients in BF16 (the finest level with mg_precision BF16), else nullptr;
+// x1z: the level's iterate x1 is zero (the finest level without pre-smoothing);
+// the recurrence-warp kernel then neither loads nor reads it.
 template <typename TR, typename TO>
 static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel &C, TO *out, float omega,
                         float cscale, const SolveState *gate, int use_tma, int *err, cudaStream_t s,
-                        const __nv_bfloat16 *coefh = nullptr)
+                        const __nv_bfloat16 *coefh = nullptr, bool x1z = false)
 {
     const double N = (double)L.d.nx * L.d.ny * L.d.nz;
-    ProfScope ps_(kLevelName[1][level], (sizeof(TR) + sizeof(TO) + (coefh ? 30.0 : 60.0) + 4.0 + 1.0 + 8.0) * N, s);
+    const bool v2 = use_tma == 2, skip = v2 && x1z && !small_level(L.d, 32);
+    ProfScope ps_(kLevelName[1][level],
+                  (sizeof(TR) + sizeof(TO) + (coefh ? 30.0 : 60.0) + (skip ? 0.0 : 4.0) + 1.0 + 8.0) * N, s);
     if (coefh) {
         if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, coefh, r, C, out, omega, cscale, gate, s);
-        else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s, use_tma == 2)))
+        else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s, v2, x1z)))
             post_t<TR, TO, 32, 1>(L, coefh, r, C, out, omega, cscale, gate, s);
     } else if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, L.coef, r, C, out, omega, cscale, gate, s);
-    else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s, use_tma == 2)))
+    else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s, v2, x1z)))
         post_t<TR, TO, 32, 1>(L, L.coef, r, C, out, omega, cscale, gate, s);
     count_launch(1);
 }
@@ -1721,7 +1727,7 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     MgLevel Cr = C;
     Cr.x3 = const_cast<float *>(coarse_cycle(mg, 1, gate, s));
     launch_post<V, V>(F, 0, in, Cr, out, w, mg.cscale, gate, mg.use_tma, mg.err, s,
-                      mg.pre0 ? nullptr : mg.coef0h);
+                      mg.pre0 ? nullptr : mg.coef0h, !mg.pre0);
 }
 
 template void mg_apply<double>(const Mg &, const double *, double *, const SolveState *, cudaStream_t);
