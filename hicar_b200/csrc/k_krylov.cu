@@ -107,13 +107,13 @@ static int march4_grid(K *kernel, const OpCtx &c, int cap)
 }
 
 // ---- the float4 column-marching kernels ----
-// Resident CTAs per SM the compiler must allow for (registers); 1 leaves the
-// register count to the compiler (160 and 3 CTAs of 128 threads per SM).
-#ifndef M4_MIN_CTAS
-#define M4_MIN_CTAS 1
-#endif
+// Resident CTAs per SM the compiler must allow for (registers): measured at
+// 1024x1024x64, four CTAs of 128 threads (128 registers, a few spilled) made
+// spmv_sigma 0.99 -> 0.94 ms and spmv_dot5 1.05 -> 1.09 ms, so the
+// five-dot kernel keeps three (up to 168 registers, none spilled).
+constexpr int M4_CTAS = 4, M4_CTAS_DOT5 = 3;
 template <typename V>
-__global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_m4_kernel(OpCtx c, const V *__restrict__ x, V *__restrict__ y,
+__global__ void __launch_bounds__(ROWT, M4_CTAS) spmv_m4_kernel(OpCtx c, const V *__restrict__ x, V *__restrict__ y,
                                                        const SolveState *gate)
 {
     if (gated(gate)) return;
@@ -129,11 +129,11 @@ __global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_m4_kernel(OpCtx c, con
 }
 
 template <typename V>
-__global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
+__global__ void __launch_bounds__(ROWT, M4_CTAS) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
                                                              const V *__restrict__ rhat, SolveState *stt,
                                                              double *partials);
 template <typename V>
-__global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
+__global__ void __launch_bounds__(ROWT, M4_CTAS_DOT5) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
                                                             const V *__restrict__ sv, const V *__restrict__ rhat,
                                                             SolveState *stt, double *hist, double *partials);
 
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(ROWT) spmv_sigma_march_kernel(OpCtx c, const V
 
 // The same with float4 column-marching rows.
 template <typename V>
-__global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
+__global__ void __launch_bounds__(ROWT, M4_CTAS) spmv_sigma_m4_kernel(OpCtx c, const V *__restrict__ phat, V *__restrict__ v,
                                                              const V *__restrict__ rhat, SolveState *stt,
                                                              double *partials)
 {
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(ROWT) spmv_dot5_march_kernel(OpCtx c, const V 
 
 // The same with float4 column-marching rows.
 template <typename V>
-__global__ void __launch_bounds__(ROWT, M4_MIN_CTAS) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
+__global__ void __launch_bounds__(ROWT, M4_CTAS_DOT5) spmv_dot5_m4_kernel(OpCtx c, const V *__restrict__ shat, V *__restrict__ t,
                                                             const V *__restrict__ sv, const V *__restrict__ rhat,
                                                             SolveState *stt, double *hist, double *partials)
 {

@@ -40,6 +40,18 @@ __device__ __forceinline__ bool inside(const Dims &d, int i, int k, int j)
     return i >= 1 && i <= d.nx && j >= 1 && j <= d.ny && k >= 1 && k <= d.nz;
 }
 
+// Programmatic dependent launch (the small levels' kernels, launched with the
+// programmatic-serialization attribute): wait until every earlier kernel of the
+// stream has completed and its writes are visible (a no-op for an ordinary
+// launch), then let the next kernel be launched while this one runs; the next
+// kernel reads nothing before its own wait.
+__device__ __forceinline__ void pdl_prologue()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 // offsets (dk, dj, di) of the 15 coefficients A..O
 __constant__ int c_off[15][3] = {{0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {0, 0, 1},  {0, 0, -1},
                                  {0, 1, 0},  {0, -1, 0}, {1, 0, 1},  {1, 0, -1}, {-1, 0, 1},
@@ -243,6 +255,7 @@ __global__ void __launch_bounds__(MG_THREADS) pre_kernel(Dims d, const float *__
                                                          const TR *__restrict__ r, float *__restrict__ out,
                                                          float omega, const SolveState *gate)
 {
+    pdl_prologue();
     if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
     constexpr int TC = TX * TY;
     extern __shared__ float sm[];
@@ -329,6 +342,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) post_kernel(Dims d, const CT *_
                                                           const float *__restrict__ xc, TO *__restrict__ out,
                                                           float omega, float cscale, const SolveState *gate)
 {
+    pdl_prologue();
     if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
     constexpr int TC = TX * TY, SX = TX + 2, SY = TY + 2, SP = SX * SY;
     extern __shared__ float sm[];
@@ -600,31 +614,29 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // ---------------------------------------------------------------------------
 // Post-smoothing fed by tensor copies, with the column recurrences moved off
 // the consumers' path.  The producer warp and the stage layout are those of
-// post_tma_kernel (three stages).  Eight consumer warps form x2 on the chunk's
+// post_tma_kernel (two stages: with three, measured slower).  Eight consumer warps form x2 on the chunk's
 // window (double-buffered, so one CTA barrier per chunk) and the residuals,
-// and hand each chunk's residual and x2 rows to a recurrence warp through a
-// two-slot ring.  The recurrence warp reads the chunk's cp, c and 1/m from the
-// stage, releases the stage, and owns the tile's column arrays: it runs the
-// forward recurrence chunk by chunk and, at the end of a tile, the backward
-// one, writing each cell's result as soon as it is known; the consumers go on
-// with the next tile meanwhile.  x1z: the iterate x1 is zero (the finest level
-// without pre-smoothing), so its window is neither loaded nor read.  Same
-// statements per cell as post_tma_kernel, so the results are bit-identical.
-// Every wait is bounded (on timeout: *err set, the loops run to their end
-// without waiting).
+// release the stage as soon as their reads are done, and hand each chunk's
+// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a two-slot
+// ring.  The recurrence warp owns the tile's column arrays: it runs the forward
+// recurrence chunk by chunk and, at the end of a tile, the backward one,
+// writing each cell's result as soon as it is known; the consumers go on with
+// the next tile meanwhile.  Same statements per cell as post_tma_kernel, so
+// the results are bit-identical.  Every wait is bounded (on timeout: *err set,
+// the loops run to their end without waiting).
 // ---------------------------------------------------------------------------
 namespace pt2 {
-constexpr int NS = 3;                      // stages at most (the launch picks 2 or 3: two CTAs per SM)
+constexpr int NS = 2;                      // stages
 constexpr int NR = 2;                      // ring slots
 constexpr int RW = pt::KC;                 // recurrence warp
 constexpr int PW = pt::KC + 1;             // producer warp
 constexpr int THREADS = pt::CW + 64;
-constexpr int RING_ROWS = 2;               // residual, x2
+constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
 constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
 constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
-template <typename TR, typename CT> size_t smem_bytes(int nz, int ns)
+template <typename TR, typename CT> size_t smem_bytes(int nz)
 {
-    return 128 + (size_t)ns * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
+    return 128 + (size_t)NS * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
            (size_t)2 * XW * 4 + 2 * (NS + NR) * 8 + 16;
 }
 }  // namespace pt2
@@ -634,10 +646,11 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     post_tma2_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
                      const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
                      const __grid_constant__ CUtensorMap tm_x1, const __grid_constant__ CUtensorMap tm_xc, Dims d,
-                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, int x1z, int NS,
+                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, int x1z,
                      const SolveState *gate, int *err)
 {
     using namespace pt;
+    using pt2::NS;
     using pt2::NR;
     constexpr int SB = stage_bytes<TR, CT>();
     constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(), O_XC = o_xc<CT>(),
@@ -652,8 +665,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     float *s_x2c = s_cp + nz * TX;
     float *s_x2w = s_x2c + nz * TX; // two window buffers of pt2::XW floats
     uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
-    uint64_t *empty = full + pt2::NS;
-    uint64_t *rfull = empty + pt2::NS;
+    uint64_t *empty = full + NS;
+    uint64_t *rfull = empty + NS;
     uint64_t *rempty = rfull + NR;
     int *s_skip = (int *)(rempty + NR);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -661,10 +674,10 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
         s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
         for (int q = 0; q < NS; q++) {
             tc::mbar_init(&full[q], 1);
-            tc::mbar_init(&empty[q], 1); // the recurrence warp releases a stage
+            tc::mbar_init(&empty[q], KC); // one arrival per consumer warp
         }
         for (int q = 0; q < NR; q++) {
-            tc::mbar_init(&rfull[q], KC); // one arrival per consumer warp
+            tc::mbar_init(&rfull[q], KC);
             tc::mbar_init(&rempty[q], 1);
         }
         tc::mbar_fence_init();
@@ -711,32 +724,23 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
             const bool col = i <= d.nx;
             float dprev = 0.0f;
             for (int ch = 0; ch < nch; ch++, it++) {
-                const int q = it % NR, s = it % NS;
+                const int q = it % NR;
                 if (ok && !tc::mbar_wait(&rfull[q], (it / NR) & 1)) {
                     atomicExch(err, 1);
                     ok = false;
                 }
                 const float *rs = ring + q * SLOT;
-                const unsigned char *st = base + s * SB;
-                const CT *sco = (const CT *)(st + O_COEF);
-                const float *smv = (const float *)(st + O_MINV), *scp = (const float *)(st + O_CP);
                 const int k0 = 1 + ch * KC;
-                float rv[KC], xv[KC], pv[KC], cv[KC], mv[KC];
-#pragma unroll
-                for (int u = 0; u < KC; u++) {
-                    const int kq = k0 + u;
-                    rv[u] = rs[u * TX + lane];
-                    xv[u] = rs[(KC + u) * TX + lane];
-                    pv[u] = scp[u * TX + lane];
-                    cv[u] = kq > 1 ? coef_val(sco[(CC * KC + u) * TX + lane]) : 0.0f;
-                    mv[u] = smv[u * TX + lane];
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    tc::mbar_arrive(&rempty[q]); // the ring slot and the stage are read
-                    tc::mbar_arrive(&empty[s]);
-                }
                 if (col) {
+                    float rv[KC], xv[KC], pv[KC], cv[KC], mv[KC];
+#pragma unroll
+                    for (int u = 0; u < KC; u++) {
+                        rv[u] = rs[(0 * KC + u) * TX + lane];
+                        xv[u] = rs[(1 * KC + u) * TX + lane];
+                        pv[u] = rs[(2 * KC + u) * TX + lane];
+                        cv[u] = rs[(3 * KC + u) * TX + lane];
+                        mv[u] = rs[(4 * KC + u) * TX + lane];
+                    }
 #pragma unroll
                     for (int u = 0; u < KC; u++) {
                         if (k0 + u > nz) break;
@@ -747,6 +751,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                         s_x2c[t] = xv[u];
                     }
                 }
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&rempty[q]);
             }
             if (col) { // backward recurrence, each level's result written as soon as it is known
                 float y = 0.0f;
@@ -804,7 +810,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
             // every consumer has finished the previous chunk (whose window buffer the next chunk reuses)
             tc::named_sync(1, CW);
             const int k = k0 + warp;
-            float res = 0.0f, x2c = 0.0f;
+            float res = 0.0f, x2c = 0.0f, cpv = 0.0f, ccv = 0.0f, mv = 0.0f;
             if (k <= nz && col) {
                 const CT *sco = (const CT *)(st + O_COEF);
                 float cv[15];
@@ -814,16 +820,24 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
                 res = post_residual<WK * WX, WX>(rv, cv, xs);
                 x2c = xs[0];
+                cpv = ((const float *)(st + O_CP))[warp * TX + lane];
+                mv = ((const float *)(st + O_MINV))[warp * TX + lane];
+                ccv = k > 1 ? cv[CC] : 0.0f;
             }
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&empty[s]); // this warp's reads of the stage are done
             if (ok && it >= NR && !tc::mbar_wait(&rempty[q], ((it / NR) - 1) & 1)) {
                 atomicExch(err, 1);
                 ok = false;
             }
             float *rs = ring + q * SLOT;
-            rs[warp * TX + lane] = res;
-            rs[(KC + warp) * TX + lane] = x2c;
+            rs[(0 * KC + warp) * TX + lane] = res;
+            rs[(1 * KC + warp) * TX + lane] = x2c;
+            rs[(2 * KC + warp) * TX + lane] = cpv;
+            rs[(3 * KC + warp) * TX + lane] = ccv;
+            rs[(4 * KC + warp) * TX + lane] = mv;
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&rfull[q]); // this warp's reads of the stage are done too
+            if (lane == 0) tc::mbar_arrive(&rfull[q]);
         }
     }
 }
@@ -841,6 +855,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
     const float *__restrict__ coef_c, const float *__restrict__ cp_c, const float *__restrict__ minv_c,
     float *__restrict__ r_c, float *__restrict__ out_c, float omega, const SolveState *gate)
 {
+    pdl_prologue();
     if (gate && *(volatile const int *)&gate->stop && !gate->profile) return;
     constexpr int TC = TX * TY, FX = 2 * TX + 2, FY = 2 * TY + 2, FP = FX * FY;
     extern __shared__ float sm[];
@@ -1184,7 +1199,6 @@ void mg_free(Mg &mg)
 
 static int sm_count();
 static int smem_optin();
-static int smem_per_sm();
 static void fused_setup(Mg &mg);
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
@@ -1241,7 +1255,6 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
         sm_count();
         smem_optin();
-        smem_per_sm();
         if (!tensor_map_encoder()) mg.use_tma = 0;
     }
     mg.lev[0].coef = fine_coef;
@@ -1315,13 +1328,48 @@ static void set_smem(F *kernel, size_t smem)
     raise_smem((const void *)kernel, smem);
 }
 
+// The small levels' kernels (2 x 2 column tiles) are launched with programmatic
+// stream serialization: each may be launched while the kernel before it runs
+// and waits in its prologue (pdl_prologue) for that kernel's results, which
+// hides the launch latency that bounds those levels.  HICARW_MG_PDL=0 in the
+// environment: ordinary launches.  Read once.
+static bool mg_pdl()
+{
+    static const bool on = [] {
+        const char *e = getenv("HICARW_MG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename K, typename... A>
+static void launch_mg(bool small, K *kernel, dim3 g, size_t smem, cudaStream_t s, A... args)
+{
+    if (!(small && mg_pdl())) {
+        kernel<<<g, MG_THREADS, smem, s>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = g;
+    cfg.blockDim = dim3(MG_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <typename TR, int TX, int TY>
 static void pre_t(const MgLevel &L, const TR *r, float *out, float omega, const SolveState *gate, cudaStream_t s)
 {
     dim3 g((L.d.nx + TX - 1) / TX, (L.d.ny + TY - 1) / TY);
     size_t smem = (size_t)4 * TX * TY * L.d.nz * sizeof(float);
     set_smem(pre_kernel<TR, TX, TY>, smem);
-    pre_kernel<TR, TX, TY><<<g, MG_THREADS, smem, s>>>(L.d, L.coef, L.cp, L.minv, r, out, omega, gate);
+    launch_mg(TX == 2 && TY == 2, pre_kernel<TR, TX, TY>, g, smem, s, L.d, (const float *)L.coef,
+              (const float *)L.cp, (const float *)L.minv, r, out, omega, gate);
 }
 
 template <typename TR>
@@ -1342,8 +1390,8 @@ static void post_t(const MgLevel &L, const CT *coef, const TR *r, const MgLevel 
     dim3 g((L.d.nx + TX - 1) / TX, (L.d.ny + TY - 1) / TY);
     size_t smem = ((size_t)4 * TX * TY * L.d.nz + (size_t)(TX + 2) * (TY + 2) * (L.d.nz + 2)) * sizeof(float);
     set_smem(post_kernel<TR, TO, TX, TY, CT>, smem);
-    post_kernel<TR, TO, TX, TY, CT><<<g, MG_THREADS, smem, s>>>(L.d, coef, L.cp, L.minv, r, L.x1, C.d, C.x3, out,
-                                                                omega, cscale, gate);
+    launch_mg(TX == 2 && TY == 2, post_kernel<TR, TO, TX, TY, CT>, g, smem, s, L.d, coef, (const float *)L.cp,
+              (const float *)L.minv, r, (const float *)L.x1, C.d, (const float *)C.x3, out, omega, cscale, gate);
 }
 
 static std::atomic<long long> g_tma_posts{0};
@@ -1368,17 +1416,6 @@ static int smem_optin()
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    }
-    return n;
-}
-
-static int smem_per_sm()
-{
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     }
     return n;
 }
@@ -1426,9 +1463,7 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    // v2: three stages where two CTAs per SM still fit, else two
-    const int ns2 = pt2::smem_bytes<TR, CT>(d.nz, 3) + 1024 <= (size_t)smem_per_sm() / 2 ? 3 : 2;
-    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz, ns2) : smem_bytes<TR, CT>(d.nz);
+    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz) : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
     const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
@@ -1455,7 +1490,7 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
         raise_smem((const void *)post_tma2_kernel<TR, TO, CT>, smem);
         post_tma2_kernel<TR, TO, CT><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out,
                                                                       omega, cscale, ntx, ntiles, x1z ? 1 : 0,
-                                                                      ns2, gate, e);
+                                                                      gate, e);
     } else {
         raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
         post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
@@ -1495,8 +1530,9 @@ static void restrict_t(const MgLevel &F, const TR *r, const MgLevel &C, float *o
     size_t smem = ((size_t)4 * TX * TY * C.d.nz + (NOX ? 0 : (size_t)(2 * TX + 2) * (2 * TY + 2) * (C.d.nz + 2))) *
                   sizeof(float);
     set_smem(restrict_pre_kernel<TR, TX, TY, NOX>, smem);
-    restrict_pre_kernel<TR, TX, TY, NOX><<<g, MG_THREADS, smem, s>>>(F.d, F.coef, r, F.x1, C.d, C.coef, C.cp,
-                                                                     C.minv, C.r, out, omega, gate);
+    launch_mg(TX == 2 && TY == 2, restrict_pre_kernel<TR, TX, TY, NOX>, g, smem, s, F.d, (const float *)F.coef, r,
+              (const float *)F.x1, C.d, (const float *)C.coef, (const float *)C.cp, (const float *)C.minv, C.r, out,
+              omega, gate);
 }
 
 // nox: level f was not pre-smoothed (its x1 is zero): restrict r_f alone.
