@@ -80,6 +80,15 @@ MG_W_LEVELS = ()  # --mg-w-levels
 FGMRES_RESTART = None  # --fgmres-restart
 
 
+def bf16_sustained():
+    """Measured sustained dense BF16 TFLOP/s of this pool's B200s (None if not recorded)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f).get("bf16_tflops_sustained") or 0.0) or None
+    return None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -607,6 +616,13 @@ def learned_report(lib, wi, dom, h, step, stream, tols, plain_ms, accuracy_solve
                 out[key].update(accuracy_solve())
     lib.hicarw_set_learned_precond(h, None)
     net.close()
+    # the U-Net's full-resolution 16 -> 16 convolution on this grid, against the
+    # tensor-core and HBM rooflines (the Krylov part's bytes are the V-cycle's)
+    c = L.conv_benchmark(16, 16, dom.nx, dom.ny, dom.nz, reps=5)
+    tc_peak = bf16_sustained()
+    hbm, _ = peaks()
+    out["conv16"] = {**c, "tflops_frac_of_sustained_bf16": c["tflops"] / tc_peak if tc_peak else None,
+                     "hbm_frac": c["gbs"] / hbm}
     return out
 
 
@@ -819,6 +835,10 @@ def run_ours(args, wl):
                     acc_keys[f"{tag}{name}_speedup_vs_plain_gpu"] = r_["speedup_vs_plain_gpu"]
                     if "lambda_rel_l2" in r_:
                         acc_keys[f"{tag}{name}_lambda_rel_l2"] = r_["lambda_rel_l2"]
+        if learned.get("conv16"):
+            acc_keys["learned_conv16_tflops"] = learned["conv16"]["tflops"]
+            acc_keys["learned_conv16_frac_of_sustained_bf16"] = learned["conv16"]["tflops_frac_of_sustained_bf16"]
+            acc_keys["learned_conv16_hbm_frac"] = learned["conv16"]["hbm_frac"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": ("f64" if opt.krylov_precision == 0 else "f32+f64") + ("+bf16" if opt.mg_precision else ""),
