@@ -614,19 +614,21 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // ---------------------------------------------------------------------------
 // Post-smoothing fed by tensor copies, with the column recurrences moved off
 // the consumers' path.  The producer warp and the stage layout are those of
-// post_tma_kernel (two stages: with three, measured slower).  Eight consumer warps form x2 on the chunk's
-// window (double-buffered, so one CTA barrier per chunk) and the residuals,
-// release the stage as soon as their reads are done, and hand each chunk's
-// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a two-slot
-// ring.  The recurrence warp owns the tile's column arrays: it runs the forward
-// recurrence chunk by chunk and, at the end of a tile, the backward one,
-// writing each cell's result as soon as it is known; the consumers go on with
-// the next tile meanwhile.  Same statements per cell as post_tma_kernel, so
-// the results are bit-identical.  Every wait is bounded (on timeout: *err set,
-// the loops run to their end without waiting).
+// post_tma_kernel (two stages; three when the x1 window is not staged).  Eight
+// consumer warps form x2 on the chunk's window (double-buffered, so one CTA
+// barrier per chunk) and the residuals, release the stage as soon as their
+// reads are done, and hand each chunk's rows (residual, x2, cp, c, 1/m) to a
+// recurrence warp through a two-slot ring.  The recurrence warp owns the
+// tile's column arrays: it runs the forward recurrence chunk by chunk and, at
+// the end of a tile, the backward one, writing each cell's result as soon as
+// it is known; the consumers go on with the next tile meanwhile.  NX1: the
+// iterate x1 is zero (the finest level without pre-smoothing), so its window
+// is neither loaded nor read, and the stage without it leaves room for a third
+// stage.  Same statements per cell as post_tma_kernel, so the results are
+// bit-identical.  Every wait is bounded (on timeout: *err set, the loops run
+// to their end without waiting).
 // ---------------------------------------------------------------------------
 namespace pt2 {
-constexpr int NS = 2;                      // stages
 constexpr int NR = 2;                      // ring slots
 constexpr int RW = pt::KC;                 // recurrence warp
 constexpr int PW = pt::KC + 1;             // producer warp
@@ -634,27 +636,40 @@ constexpr int THREADS = pt::CW + 64;
 constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
 constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
 constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
-template <typename TR, typename CT> size_t smem_bytes(int nz)
+// Stage layout: that of post_tma_kernel, without the x1 window when the iterate
+// is zero (NX1); the bytes that frees hold a third stage.
+template <bool NX1> constexpr int ns() { return NX1 ? 3 : 2; }
+template <typename CT, bool NX1> constexpr int o_xc() { return pt::o_x1<CT>() + (NX1 ? 0 : pt::up128(pt::B_X1)); }
+template <typename CT, bool NX1> constexpr int o_r() { return o_xc<CT, NX1>() + pt::up128(pt::B_XC); }
+template <typename TR, typename CT, bool NX1> constexpr int stage_bytes()
 {
-    return 128 + (size_t)NS * pt::stage_bytes<TR, CT>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
-           (size_t)2 * XW * 4 + 2 * (NS + NR) * 8 + 16;
+    return o_r<CT, NX1>() + pt::up128(pt::KC * pt::TX * (int)sizeof(TR));
+}
+template <typename TR, typename CT, bool NX1> constexpr uint32_t tx_bytes()
+{
+    return pt::tx_bytes<TR, CT>() - (NX1 ? (uint32_t)pt::B_X1 : 0u);
+}
+template <typename TR, typename CT, bool NX1> size_t smem_bytes(int nz)
+{
+    return 128 + (size_t)ns<NX1>() * stage_bytes<TR, CT, NX1>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
+           (size_t)2 * XW * 4 + 2 * (3 + NR) * 8 + 16;
 }
 }  // namespace pt2
 
-template <typename TR, typename TO, typename CT = float>
+template <typename TR, typename TO, typename CT, bool NX1>
 __global__ void __launch_bounds__(pt2::THREADS, 2)
     post_tma2_kernel(const __grid_constant__ CUtensorMap tm_coef, const __grid_constant__ CUtensorMap tm_minv,
                      const __grid_constant__ CUtensorMap tm_cp, const __grid_constant__ CUtensorMap tm_r,
                      const __grid_constant__ CUtensorMap tm_x1, const __grid_constant__ CUtensorMap tm_xc, Dims d,
-                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, int x1z,
-                     const SolveState *gate, int *err)
+                     TO *__restrict__ out, float omega, float cscale, int ntx, int ntiles, const SolveState *gate,
+                     int *err)
 {
     using namespace pt;
-    using pt2::NS;
     using pt2::NR;
-    constexpr int SB = stage_bytes<TR, CT>();
-    constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(), O_XC = o_xc<CT>(),
-                  O_R = o_r<CT>();
+    constexpr int NS = pt2::ns<NX1>();
+    constexpr int SB = pt2::stage_bytes<TR, CT, NX1>();
+    constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(),
+                  O_XC = pt2::o_xc<CT, NX1>(), O_R = pt2::o_r<CT, NX1>();
     constexpr int SLOT = pt2::RING_ROWS * KC * TX; // floats per ring slot
     extern __shared__ unsigned char pt_smem[];
     unsigned char *base = (unsigned char *)(((uintptr_t)pt_smem + 127) & ~(uintptr_t)127);
@@ -665,8 +680,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     float *s_x2c = s_cp + nz * TX;
     float *s_x2w = s_x2c + nz * TX; // two window buffers of pt2::XW floats
     uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
-    uint64_t *empty = full + NS;
-    uint64_t *rfull = empty + NS;
+    uint64_t *empty = full + 3;
+    uint64_t *rfull = empty + 3;
     uint64_t *rempty = rfull + NR;
     int *s_skip = (int *)(rempty + NR);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -687,7 +702,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
 
     if (warp == pt2::PW) { // ---- producer ----
         if (lane != 0) return;
-        const uint32_t txb = tx_bytes<TR, CT>() - (x1z ? (uint32_t)B_X1 : 0u);
+        constexpr uint32_t txb = pt2::tx_bytes<TR, CT, NX1>();
         bool ok = true;
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -705,7 +720,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 tc::tma_load_3d(st + O_COEF, &tm_coef, i0 + XO, row, 0, &full[s]);
                 tc::tma_load_2d(st + O_MINV, &tm_minv, i0 + XO, row, &full[s]);
                 tc::tma_load_2d(st + O_CP, &tm_cp, i0 + XO, row, &full[s]);
-                if (!x1z) tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
+                if (!NX1) tc::tma_load_3d(st + O_X1, &tm_x1, i0 + XO - 4, k0 - 1, j - 1, &full[s]);
                 tc::tma_load_3d(st + O_XC, &tm_xc, (i0 >> 1) + XO - 3, k0 - 1, j >> 1, &full[s]);
                 tc::tma_load_2d(st + O_R, &tm_r, i0 + XO, row, &full[s]);
             }
@@ -802,7 +817,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
                 float a = 0.0f;
                 if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
-                    if (!x1z) a = sx1[(jj * WK + kw) * X1W + cc + 3];
+                    if (!NX1) a = sx1[(jj * WK + kw) * X1W + cc + 3];
                     a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
                 }
                 xw[e] = a;
@@ -1463,7 +1478,8 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const size_t smem = v2 ? pt2::smem_bytes<TR, CT>(d.nz) : smem_bytes<TR, CT>(d.nz);
+    const size_t smem = v2 ? (x1z ? pt2::smem_bytes<TR, CT, true>(d.nz) : pt2::smem_bytes<TR, CT, false>(d.nz))
+                           : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
     const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
@@ -1486,11 +1502,14 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
     const int ntx = (d.nx + TX - 1) / TX, ntiles = ntx * d.ny;
     const int grid = std::min(ntiles, 2 * sm_count());
     int *e = gate ? const_cast<int *>(&gate->err) : err;
-    if (v2) {
-        raise_smem((const void *)post_tma2_kernel<TR, TO, CT>, smem);
-        post_tma2_kernel<TR, TO, CT><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out,
-                                                                      omega, cscale, ntx, ntiles, x1z ? 1 : 0,
-                                                                      gate, e);
+    if (v2 && x1z) {
+        raise_smem((const void *)post_tma2_kernel<TR, TO, CT, true>, smem);
+        post_tma2_kernel<TR, TO, CT, true><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d,
+                                                                            out, omega, cscale, ntx, ntiles, gate, e);
+    } else if (v2) {
+        raise_smem((const void *)post_tma2_kernel<TR, TO, CT, false>, smem);
+        post_tma2_kernel<TR, TO, CT, false><<<grid, pt2::THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d,
+                                                                             out, omega, cscale, ntx, ntiles, gate, e);
     } else {
         raise_smem((const void *)post_tma_kernel<TR, TO, CT>, smem);
         post_tma_kernel<TR, TO, CT><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], d, out, omega,
