@@ -1677,9 +1677,15 @@ static void fused_setup(Mg &mg)
     mg.cluster_n = 0;
     const char *e = getenv("HICARW_MG_FUSE");
     if (!(e && e[0] == '1')) return; // opt-in: the per-level launches measured faster in a graph
+    // HICARW_MG_FUSE_COLS: the first fused level has at most this many columns
+    // (default MG_FUSE_COLS); HICARW_MG_FUSE_CTAS: the cluster size (default 16,
+    // else 8; 1: one CTA walks the chain)
+    const char *ec = getenv("HICARW_MG_FUSE_COLS"), *en = getenv("HICARW_MG_FUSE_CTAS");
+    const long long cols = ec ? std::max(1, std::min(MG_FUSE_COLS, atoi(ec))) : MG_FUSE_COLS;
+    const int want = en ? atoi(en) : 0;
     int l0 = 0;
     for (int l = 2; l + 1 < mg.nlev; l++)
-        if ((long long)mg.lev[l].d.nx * mg.lev[l].d.ny <= MG_FUSE_COLS) {
+        if ((long long)mg.lev[l].d.nx * mg.lev[l].d.ny <= cols) {
             l0 = l;
             break;
         }
@@ -1688,7 +1694,8 @@ static void fused_setup(Mg &mg)
         cudaGetLastError();
         return;
     }
-    for (int cn : {16, 8}) {
+    for (int cn : {16, 8, 1}) {
+        if (want > 0 ? cn != want : cn == 1) continue;
         size_t smem = 0;
         if (!fused_smem(mg, l0, cn, (size_t)smem_optin(), &smem)) continue;
         raise_smem((const void *)coarse_cycle_kernel, smem);
