@@ -614,22 +614,22 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // ---------------------------------------------------------------------------
 // Post-smoothing fed by tensor copies, with the column recurrences moved off
 // the consumers' path.  The producer warp and the stage layout are those of
-// post_tma_kernel (two stages; three when the x1 window is not staged).  Eight
-// consumer warps form x2 on the chunk's window (double-buffered, so one CTA
-// barrier per chunk) and the residuals, release the stage as soon as their
-// reads are done, and hand each chunk's rows (residual, x2, cp, c, 1/m) to a
-// recurrence warp through a two-slot ring.  The recurrence warp owns the
+// post_tma_kernel (three stages).  Eight consumer warps form x2 on the chunk's
+// window (double-buffered, so one CTA barrier per chunk) and the residuals,
+// release the stage as soon as their reads are done, and hand each chunk's
+// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a ring of one
+// or two slots.  The recurrence warp owns the
 // tile's column arrays: it runs the forward recurrence chunk by chunk and, at
 // the end of a tile, the backward one, writing each cell's result as soon as
 // it is known; the consumers go on with the next tile meanwhile.  NX1: the
 // iterate x1 is zero (the finest level without pre-smoothing), so its window
-// is neither loaded nor read, and the stage without it leaves room for a third
-// stage.  Same statements per cell as post_tma_kernel, so the results are
+// is neither loaded nor read, and the smaller stage leaves room for a second
+// ring slot.  Same statements per cell as post_tma_kernel, so the results are
 // bit-identical.  Every wait is bounded (on timeout: *err set, the loops run
 // to their end without waiting).
 // ---------------------------------------------------------------------------
 namespace pt2 {
-constexpr int NR = 2;                      // ring slots
+constexpr int NR_MAX = 2;                  // ring slots at most
 constexpr int RW = pt::KC;                 // recurrence warp
 constexpr int PW = pt::KC + 1;             // producer warp
 constexpr int THREADS = pt::CW + 64;
@@ -637,8 +637,10 @@ constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
 constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
 constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
 // Stage layout: that of post_tma_kernel, without the x1 window when the iterate
-// is zero (NX1); the bytes that frees hold a third stage.
-template <bool NX1> constexpr int ns() { return NX1 ? 3 : 2; }
+// is zero (NX1).  Three stages either way: with the x1 window the ring has one
+// slot instead of two, so that two CTAs per SM still fit at nz = 64.
+template <bool NX1> constexpr int ns() { return 3; }
+template <bool NX1> constexpr int nr() { return NX1 ? 2 : 1; }
 template <typename CT, bool NX1> constexpr int o_xc() { return pt::o_x1<CT>() + (NX1 ? 0 : pt::up128(pt::B_X1)); }
 template <typename CT, bool NX1> constexpr int o_r() { return o_xc<CT, NX1>() + pt::up128(pt::B_XC); }
 template <typename TR, typename CT, bool NX1> constexpr int stage_bytes()
@@ -651,8 +653,8 @@ template <typename TR, typename CT, bool NX1> constexpr uint32_t tx_bytes()
 }
 template <typename TR, typename CT, bool NX1> size_t smem_bytes(int nz)
 {
-    return 128 + (size_t)ns<NX1>() * stage_bytes<TR, CT, NX1>() + (size_t)NR * B_SLOT + (size_t)3 * nz * pt::TX * 4 +
-           (size_t)2 * XW * 4 + 2 * (3 + NR) * 8 + 16;
+    return 128 + (size_t)ns<NX1>() * stage_bytes<TR, CT, NX1>() + (size_t)nr<NX1>() * B_SLOT +
+           (size_t)3 * nz * pt::TX * 4 + (size_t)2 * XW * 4 + 2 * (3 + NR_MAX) * 8 + 16;
 }
 }  // namespace pt2
 
@@ -665,7 +667,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                      int *err)
 {
     using namespace pt;
-    using pt2::NR;
+    constexpr int NR = pt2::nr<NX1>();
     constexpr int NS = pt2::ns<NX1>();
     constexpr int SB = pt2::stage_bytes<TR, CT, NX1>();
     constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(),
@@ -682,8 +684,8 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
     uint64_t *empty = full + 3;
     uint64_t *rfull = empty + 3;
-    uint64_t *rempty = rfull + NR;
-    int *s_skip = (int *)(rempty + NR);
+    uint64_t *rempty = rfull + pt2::NR_MAX;
+    int *s_skip = (int *)(rempty + pt2::NR_MAX);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
@@ -1214,6 +1216,7 @@ void mg_free(Mg &mg)
 
 static int sm_count();
 static int smem_optin();
+static int smem_per_sm();
 static void fused_setup(Mg &mg);
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
@@ -1270,6 +1273,7 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
     if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
         sm_count();
         smem_optin();
+        smem_per_sm();
         if (!tensor_map_encoder()) mg.use_tma = 0;
     }
     mg.lev[0].coef = fine_coef;
@@ -1435,6 +1439,17 @@ static int smem_optin()
     return n;
 }
 
+static int smem_per_sm()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    }
+    return n;
+}
+
 // The driver's tensor-map encoder, looked up through the runtime so that the
 // library does not link the driver library itself (nullptr if unavailable).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
@@ -1478,8 +1493,10 @@ static bool post_tma(const MgLevel &L, const CT *coef, const TR *r, const MgLeve
 {
     using namespace pt;
     const Dims &d = L.d, &dc = C.d;
-    const size_t smem = v2 ? (x1z ? pt2::smem_bytes<TR, CT, true>(d.nz) : pt2::smem_bytes<TR, CT, false>(d.nz))
-                           : smem_bytes<TR, CT>(d.nz);
+    // the recurrence-warp kernel where two of its CTAs fit on an SM, else post_tma_kernel
+    const size_t smem2 = x1z ? pt2::smem_bytes<TR, CT, true>(d.nz) : pt2::smem_bytes<TR, CT, false>(d.nz);
+    if (v2 && 2 * (smem2 + 1024) > (size_t)smem_per_sm()) v2 = false;
+    const size_t smem = v2 ? smem2 : smem_bytes<TR, CT>(d.nz);
     if (smem > (size_t)smem_optin() || !err || dc.mz != d.mz) return false;
     const cuuint64_t rows = (cuuint64_t)d.my * d.mz;
     const cuuint64_t dco[3] = {(cuuint64_t)d.P, rows, 15},
