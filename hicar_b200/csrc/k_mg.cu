@@ -949,7 +949,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
 // the kernel are read back with ld.global.cg (L2), never through the
 // read-only path.
 // ---------------------------------------------------------------------------
-constexpr int MG_FUSE_COLS = 1024;  // first fused level: nx * ny at most this
+constexpr int MG_FUSE_COLS = 256;   // first fused level: nx * ny at most this (1024x1024: level 6, 16 x 16)
 constexpr int MG_FUSE_STEPS = 128;  // longest recorded chain (else the per-level launches run); 128 steps
                                     // of 232 bytes keep the kernel parameter under 32 KB
 constexpr int MG_FUSE_THREADS = 512;
@@ -1685,20 +1685,23 @@ static cudaLaunchConfig_t fused_config(int cn, size_t smem, cudaStream_t s, cuda
 }
 
 // Decide at build time (outside any stream capture) whether and where the
-// coarse part is fused (HICARW_MG_FUSE=1 in the environment), and the cluster
-// size: 16 CTAs where the device can place such a cluster with this shared
-// memory, else 8, else no fusion.
+// coarse part is fused (HICARW_MG_FUSE=0 in the environment: never), and the
+// cluster size: 16 CTAs where the device can place such a cluster with this
+// shared memory, else 8, else no fusion.  Measured at 1024x1024x64 with W on
+// levels 2-4: fused from level 6 (16 x 16 columns) 8.63 solves/s against 8.56
+// with one launch per level; from level 5 (32 x 32) 8.30 against 8.37; one CTA
+// walking the chain from level 7 8.30.
 static void fused_setup(Mg &mg)
 {
     mg.fuse_level = 0;
     mg.cluster_n = 0;
     const char *e = getenv("HICARW_MG_FUSE");
-    if (!(e && e[0] == '1')) return; // opt-in: the per-level launches measured faster in a graph
+    if (e && e[0] == '0') return; // one launch per level
     // HICARW_MG_FUSE_COLS: the first fused level has at most this many columns
     // (default MG_FUSE_COLS); HICARW_MG_FUSE_CTAS: the cluster size (default 16,
     // else 8; 1: one CTA walks the chain)
     const char *ec = getenv("HICARW_MG_FUSE_COLS"), *en = getenv("HICARW_MG_FUSE_CTAS");
-    const long long cols = ec ? std::max(1, std::min(MG_FUSE_COLS, atoi(ec))) : MG_FUSE_COLS;
+    const long long cols = ec ? std::max(1, std::min(1024, atoi(ec))) : MG_FUSE_COLS;
     const int want = en ? atoi(en) : 0;
     int l0 = 0;
     for (int l = 2; l + 1 < mg.nlev; l++)

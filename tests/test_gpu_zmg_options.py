@@ -268,7 +268,7 @@ def _profile_names(h):
 @pytest.mark.parametrize("shape", [(48, 40, 20), (197, 101, 13), (130, 66, 24)])
 def test_fused_coarse_cycle_bitexact(shape, monkeypatch):
     """The coarse part of the cycle run by one thread-block cluster (levels of
-    at most 1024 columns; the default) gives the per-level launches' V-cycle bit
+    at most 256 columns; the default) gives the per-level launches' V-cycle bit
     for bit, for the V-cycle and for W-cycles that reach into the fused levels,
     on a small grid, a ragged one and one with odd coarse extents."""
     from hicar_b200 import wind, wind_iterative as wi
