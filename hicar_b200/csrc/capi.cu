@@ -263,9 +263,6 @@ static int ensure_vectors(hicarw_handle *h, int prec)
 template <typename T>
 static T *V(hicarw_handle *h, int q) { return (T *)h->vec[q]; }
 
-// lambda (V_X) is FP64 for the FP64 vectors and for FP32 vectors with FP64 accumulation
-static bool x64(const hicarw_handle *h) { return h->vprec != HICARW_KRYLOV_F32; }
-
 // Krylov vector precision of the configured solve: the reference schedule takes
 // the option, FGMRES is FP64.
 static int solve_precision(const hicarw_handle *h)
@@ -288,10 +285,11 @@ static int stage_in(hicarw_handle *h, const float *src, float **buf, size_t n, i
 // Options as the solve uses them.  HICARW_SOLVER_MIXED names the reference
 // schedule with FP32 Krylov vectors, FP64 reductions and FP64 lambda, periodic
 // FP64 residual replacement and the FP64 true-residual stop; the fused FP32
-// schedule (HICARW_SOLVER_FUSED) no longer exists.
+// schedule (HICARW_SOLVER_FUSED) and FP32 lambda (HICARW_KRYLOV_F32) no longer
+// exist.
 static int normalize_options(hicarw_options *o)
 {
-    if (o->krylov_precision < HICARW_KRYLOV_F64 || o->krylov_precision > HICARW_KRYLOV_F32_X64) return HICARW_ERR_ARG;
+    if (o->krylov_precision != HICARW_KRYLOV_F64 && o->krylov_precision != HICARW_KRYLOV_F32_X64) return HICARW_ERR_ARG;
     if (o->solver == HICARW_SOLVER_FUSED) return HICARW_ERR_ARG;
     if (o->solver == HICARW_SOLVER_MIXED) {
         o->solver = HICARW_SOLVER_REFERENCE;
@@ -489,8 +487,7 @@ static void enqueue_iteration(hicarw_handle *h, XT *x, int sweeps, cudaStream_t 
 static void enqueue_iteration_prec(hicarw_handle *h, int prec, int sweeps, cudaStream_t s)
 {
     if (prec == HICARW_KRYLOV_F64) enqueue_iteration<double, double>(h, V<double>(h, V_X), sweeps, s);
-    else if (prec == HICARW_KRYLOV_F32_X64) enqueue_iteration<float, double>(h, V<double>(h, V_X), sweeps, s);
-    else enqueue_iteration<float, float>(h, V<float>(h, V_X), sweeps, s);
+    else enqueue_iteration<float, double>(h, V<double>(h, V_X), sweeps, s);
 }
 
 // The set-up kernel (r = b - A x, r^ = p = r and the first dots) in the vector
@@ -501,12 +498,9 @@ static void enqueue_setup_prec(hicarw_handle *h, int prec, const OpCtx &c, const
     if (prec == HICARW_KRYLOV_F64)
         launch_setup<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), V<double>(h, V_R),
                                      V<double>(h, V_RHAT), V<double>(h, V_P), h->st, h->hist, rb, restart, s);
-    else if (prec == HICARW_KRYLOV_F32_X64)
+    else
         launch_setup<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
                                     V<float>(h, V_P), h->st, h->hist, rb, restart, s);
-    else
-        launch_setup<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), V<float>(h, V_R), V<float>(h, V_RHAT),
-                                   V<float>(h, V_P), h->st, h->hist, rb, restart, s);
 }
 
 // FP64 true residual of the current solution in the vector precision prec:
@@ -519,12 +513,9 @@ static void enqueue_true_residual_prec(hicarw_handle *h, int prec, int mode, cud
     if (prec == HICARW_KRYLOV_F64)
         launch_true_residual<double, double>(c, V<double>(h, V_X), V<double>(h, V_RHS), mode ? V<double>(h, V_R) : nullptr,
                                              mode ? V<double>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
-    else if (prec == HICARW_KRYLOV_F32_X64)
+    else
         launch_true_residual<float, double>(c, V<double>(h, V_X), V<float>(h, V_RHS), mode ? V<float>(h, V_R) : nullptr,
                                             mode ? V<float>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
-    else
-        launch_true_residual<float, float>(c, V<float>(h, V_X), V<float>(h, V_RHS), mode ? V<float>(h, V_R) : nullptr,
-                                           mode ? V<float>(h, V_RHAT) : nullptr, h->st, mode, rb, s);
 }
 
 static int get_graph(hicarw_handle *h, int prec, int sweeps, int chunk, GraphRec **out)
@@ -906,15 +897,13 @@ static void fill_stats(hicarw_handle *h, hicarw_stats *o, int sweeps, int retrie
 static int enqueue_winds(hicarw_handle *h, const float *rho, int adv_den, float *u, float *v, float *w, cudaStream_t s)
 {
     Metrics m = metrics_of(h);
-    if (x64(h)) launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
-    else launch_winds<float>(h->d, m, V<float>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
+    launch_winds<double>(h->d, m, V<double>(h, V_X), h->alpha, rho, u, v, w, adv_den, s);
     return 0;
 }
 
 static int zero_solution(hicarw_handle *h, cudaStream_t s)
 {
-    size_t es = x64(h) ? 8 : 4;
-    CK(cudaMemsetAsync(h->vec[V_X], 0, (size_t)h->d.npad * es, s));
+    CK(cudaMemsetAsync(h->vec[V_X], 0, (size_t)h->d.npad * 8, s));
     return 0;
 }
 
@@ -1067,8 +1056,7 @@ extern "C" int hicarw_probe_lambda_pattern(hicarw_handle *h, int ca, int cb, int
     api_entry();
     if (!h || ca < 0 || ca > 2 || cb < 0 || cb > 2 || cc < 0 || cc > 2) return HICARW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (x64(h)) launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
-    else launch_probe_pattern<float>(h->d, V<float>(h, V_X), ca, cb, cc, s);
+    launch_probe_pattern<double>(h->d, V<double>(h, V_X), ca, cb, cc, s);
     return HICARW_OK;
 }
 
@@ -1105,8 +1093,7 @@ extern "C" int hicarw_probe_apply_corrections(hicarw_handle *h, const float *alp
     if ((rc = stage_in(h, v, &h->sv, n_v(d), mem_kind, s, &dv)) != 0) return rc;
     if ((rc = stage_in(h, w, &h->sw, n_cell(d), mem_kind, s, &dw)) != 0) return rc;
     Metrics m = metrics_of(h);
-    if (x64(h)) launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
-    else launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
+    launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, (float *)du, (float *)dv, (float *)dw, adv_den, s);
     if (mem_kind == HICARW_MEM_HOST) {
         CK(cudaMemcpyAsync(u, du, n_u(d) * 4, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(v, dv, n_v(d) * 4, cudaMemcpyDeviceToHost, s));
@@ -1182,15 +1169,11 @@ extern "C" int hicarw_calibrate_projection_operator(hicarw_handle *h, const floa
     for (int cc = 0; cc < 3; cc++)
         for (int cb = 0; cb < 3; cb++)
             for (int ca = 0; ca < 3; ca++) {
-                if (x64(h)) launch_probe_pattern<double>(d, V<double>(h, V_X), ca, cb, cc, s);
-                else launch_probe_pattern<float>(d, V<float>(h, V_X), ca, cb, cc, s);
+                launch_probe_pattern<double>(d, V<double>(h, V_X), ca, cb, cc, s);
                 CK(cudaMemsetAsync(h->sprobe_u, 0, n_u(d) * 4, s));
                 CK(cudaMemsetAsync(h->sprobe_v, 0, n_v(d) * 4, s));
                 CK(cudaMemsetAsync(h->sprobe_w, 0, n_cell(d) * 4, s));
-                if (x64(h))
-                    launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
-                else
-                    launch_winds<float>(d, m, V<float>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
+                launch_winds<double>(d, m, V<double>(h, V_X), h->alpha, rho, h->sprobe_u, h->sprobe_v, h->sprobe_w, adv_den, s);
                 launch_divergence(d, m, h->sprobe_u, h->sprobe_v, h->sprobe_w, rho, h->sT, adv_den, 0, 1, s);
                 launch_probe_record(d, h->sT, h->coef, ca, cb, cc, h->scan + 3, s);
             }
@@ -1211,15 +1194,9 @@ extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind,
     cudaStream_t s = (cudaStream_t)stream;
     const Dims &d = h->d;
     size_t n = (size_t)d.mx * d.mz * d.my;
-    double *conv = nullptr, *gath = nullptr;
-    CK(cudaMalloc((void **)&conv, (size_t)d.npad * 8));
+    double *gath = nullptr;
     CK(cudaMalloc((void **)&gath, n * 8));
-    const double *src64 = nullptr;
-    if (x64(h)) src64 = V<double>(h, V_X);
-    else {
-        launch_convert<float, double>(d.npad, V<float>(h, V_X), conv, s);
-        src64 = conv;
-    }
+    const double *src64 = V<double>(h, V_X);
     // gather the padded rows into the (nx+2, nz+2, ny+2) Fortran layout
     cudaError_t e = cudaMemcpy2DAsync(gath, sizeof(double) * d.mx, src64 + XO, sizeof(double) * d.P,
                                       sizeof(double) * d.mx, (size_t)d.mz * d.my, cudaMemcpyDeviceToDevice, s);
@@ -1227,7 +1204,6 @@ extern "C" int hicarw_get_lambda(hicarw_handle *h, double *lambda, int mem_kind,
         e = cudaMemcpyAsync(lambda, gath, n * 8,
                             mem_kind == HICARW_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
     cudaError_t e2 = cudaStreamSynchronize(s);
-    cudaFree(conv);
     cudaFree(gath);
     if (e != cudaSuccess || e2 != cudaSuccess) { set_err(h, "get_lambda", e != cudaSuccess ? e : e2); return HICARW_ERR_CUDA; }
     return HICARW_OK;

@@ -767,22 +767,15 @@ INST_V(float)
 template void launch_update_xrp<double, double>(const Dims &, double *, const double *, const double *, double *,
                                                 const double *, const double *, double *, const double *,
                                                 const SolveState *, cudaStream_t);
-template void launch_update_xrp<float, float>(const Dims &, float *, const float *, const float *, float *,
-                                              const float *, const float *, float *, const float *, const SolveState *,
-                                              cudaStream_t);
 template void launch_update_xrp<float, double>(const Dims &, double *, const float *, const float *, float *,
                                                const float *, const float *, float *, const float *, const SolveState *,
                                                cudaStream_t);
 template void launch_setup<double, double>(const OpCtx &, const double *, const double *, double *, double *,
                                            double *, SolveState *, double *, const RedBuf &, int, cudaStream_t);
-template void launch_setup<float, float>(const OpCtx &, const float *, const float *, float *, float *, float *,
-                                         SolveState *, double *, const RedBuf &, int, cudaStream_t);
 template void launch_setup<float, double>(const OpCtx &, const double *, const float *, float *, float *, float *,
                                           SolveState *, double *, const RedBuf &, int, cudaStream_t);
 template void launch_true_residual<double, double>(const OpCtx &, const double *, const double *, double *,
                                                    const double *, SolveState *, int, const RedBuf &, cudaStream_t);
-template void launch_true_residual<float, float>(const OpCtx &, const float *, const float *, float *, const float *,
-                                                 SolveState *, int, const RedBuf &, cudaStream_t);
 template void launch_true_residual<float, double>(const OpCtx &, const double *, const float *, float *,
                                                   const float *, SolveState *, int, const RedBuf &, cudaStream_t);
 template void launch_convert<double, float>(long long, const double *, float *, cudaStream_t);

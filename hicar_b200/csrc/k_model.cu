@@ -177,8 +177,6 @@ void launch_winds(const Dims &d, const Metrics &m, const V *x, const float *alph
 }
 template void launch_winds<double>(const Dims &, const Metrics &, const double *, const float *, const float *, float *,
                                    float *, float *, int, cudaStream_t);
-template void launch_winds<float>(const Dims &, const Metrics &, const float *, const float *, const float *, float *,
-                                  float *, float *, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Probing (:1096-1248).
@@ -202,7 +200,6 @@ void launch_probe_pattern(const Dims &d, V *x, int ca, int cb, int cc, cudaStrea
     count_launch(1);
 }
 template void launch_probe_pattern<double>(const Dims &, double *, int, int, int, cudaStream_t);
-template void launch_probe_pattern<float>(const Dims &, float *, int, int, int, cudaStream_t);
 
 __global__ void probe_record_kernel(Dims d, const float *__restrict__ T, float *coef, int ca, int cb, int cc,
                                     unsigned int *max_leak_bits)

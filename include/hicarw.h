@@ -62,7 +62,8 @@ enum { HICARW_MEM_DEVICE = 0, HICARW_MEM_HOST = 1 };
 /* Krylov vector precision. */
 enum {
     HICARW_KRYLOV_F64 = 0,    /* reference precision: FP64 vectors, FP64 reductions */
-    HICARW_KRYLOV_F32 = 1,    /* FP32 vectors, FP64 reductions */
+    HICARW_KRYLOV_F32 = 1,    /* withdrawn (FP32 vectors and FP32 lambda: the solution drifts, and the
+                                 schedule diverged at 512x512x48): rejected with HICARW_ERR_ARG */
     HICARW_KRYLOV_F32_X64 = 2 /* FP32 vectors, FP64 reductions and FP64 accumulation of lambda (the
                                  solution): the true residual follows the recurrence residual (reference
                                  schedule) */

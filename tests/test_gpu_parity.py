@@ -196,20 +196,14 @@ def test_same_input_solve_matches_in_method(oracle_mod, case64):
     assert _rel(_lambda(dom), s.vec("x")) < 1e-6
 
 
-def test_fp32_and_mixed_solves(oracle_mod, case64):
-    """FP32 Krylov vectors (reference schedule) and the MIXED shorthand (FP32
-    vectors, FP64 lambda, periodic FP64 residual replacement, restarts until
-    the FP64 true residual meets the target) against the oracle's
-    reference-precision solve driven to 1e-10; the withdrawn fused schedule is
-    rejected."""
+def test_mixed_solve_and_withdrawn_modes(oracle_mod, case64):
+    """The MIXED shorthand (FP32 vectors, FP64 lambda, periodic FP64 residual
+    replacement, restarts until the FP64 true residual meets the target)
+    against the oracle's reference-precision solve driven to 1e-10; the
+    withdrawn fused schedule and FP32 lambda are rejected."""
     s, u, v, w, st1, st2, leak = oracle_mod.update_winds_first(case64, tol_rel=1e-10)
     lam_ref = s.vec("x")
-    dom, stats = _gpu_first_update(case64, krylov_precision=_capi.KRYLOV_F32, tol_rel=1e-6)
-    assert stats[1]["status"] == 0
-    e32 = _rel(_lambda(dom), lam_ref)
-    assert e32 < 1e-3, e32
-    from hicar_b200 import wind, wind_iterative as wi
-    wi.finalize_iter_winds(); wind.reset()
+    from hicar_b200 import wind_iterative as wi
     dom, stats = _gpu_first_update(case64, solver=_capi.SOLVER_MIXED, criterion=_capi.CRIT_TRUE,
                                    tol_rel=1e-8, replace_every=20)
     assert stats[1]["status"] == 0
@@ -220,6 +214,7 @@ def test_fp32_and_mixed_solves(oracle_mod, case64):
         assert _rel(_np(g), r) < 1e-5
     h = wi.handle(dom.nest_indx)
     assert _capi.load().hicarw_set_options(h, C.byref(wi.WindOptions(solver=_capi.SOLVER_FUSED).to_c())) == -1
+    assert _capi.load().hicarw_set_options(h, C.byref(wi.WindOptions(krylov_precision=_capi.KRYLOV_F32).to_c())) == -1
 
 
 def test_host_pointers_match_device_pointers(case64):
