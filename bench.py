@@ -736,7 +736,8 @@ def run_ours(args, wl):
     hu, hv, hw_ = (torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in (u0, v0, w0))
     for src, dst in ((u0, hu), (v0, hv), (w0, hw_)):
         dst.copy_(src.cpu())
-    ou, ov, ow = (torch.empty_like(a) for a in (hu, hv, hw_))
+    # pinned results too (empty_like would not pin them): a device -> pageable copy blocks the host
+    ou, ov, ow = (torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in (hu, hv, hw_))
     h2d = sum(a.numel() * 4 for a in (hu, hv, hw_))
     d2h = h2d
     cstream = torch.cuda.Stream(device=f"cuda:{local}")
@@ -1008,7 +1009,7 @@ def batch_measure(args, wl, rank, world, dist, local, quick=False):
         for hs, sv in zip(host, bs.saved):
             for dst, src in zip(hs, sv):
                 dst.copy_(src.cpu())
-        outs = [[torch.empty_like(a) for a in hs] for hs in host]
+        outs = [[torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for a in hs] for hs in host]
         h2d = sum(a.numel() * 4 for hs in host for a in hs)
 
         def e2e_step():
