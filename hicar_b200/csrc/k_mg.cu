@@ -882,60 +882,7 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
     if (!NOX) stage_window<FX, FY>(f, x1_f, f, nullptr, 2 * I0 - 2, 2 * J0 - 2, s_x);
     __syncthreads();
     const long long cofs = (long long)CC * dc.npad;
-    if constexpr (NOX) { // r_c = R^T r_f: the operands of RB cells per thread in flight together
-        constexpr int RB = 4;
-        for (int base = threadIdx.x; base < n; base += MG_THREADS * RB) {
-            TR rf[RB][4];
-            float vc[RB], vm[RB], vp[RB];
-            bool ok[RB];
-            long long ocs[RB];
-#pragma unroll
-            for (int u = 0; u < RB; u++) {
-                const int t = base + u * MG_THREADS;
-                const int c = t % TC, k = t / TC + 1;
-                const int I = I0 + c % TX, J = J0 + c / TX;
-                ok[u] = t < n && I <= dc.nx && J <= dc.ny;
-                vc[u] = vm[u] = vp[u] = 0.0f;
-#pragma unroll
-                for (int q = 0; q < 4; q++) rf[u][q] = (TR)0;
-                ocs[u] = 0;
-                if (ok[u]) {
-                    const long long oc = kidx(dc, I, k, J);
-                    ocs[u] = oc;
-                    vc[u] = k > 1 ? coef_c[cofs + oc] : 0.0f;
-                    vm[u] = minv_c[oc];
-                    vp[u] = cp_c[oc];
-#pragma unroll
-                    for (int pj = 0; pj < 2; pj++) {
-                        const int j = 2 * J - 1 + pj, i0c = 2 * I - 1;
-                        if (j > f.ny) continue;
-                        const long long o0 = kidx(f, i0c, k, j);
-                        rf[u][2 * pj] = r_f[o0];
-                        if (i0c + 1 <= f.nx) rf[u][2 * pj + 1] = r_f[o0 + 1];
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < RB; u++) {
-                const int t = base + u * MG_THREADS;
-                if (!ok[u]) continue;
-                const int c = t % TC, J = J0 + c / TX, I = I0 + c % TX;
-                double acc = 0.0;
-#pragma unroll
-                for (int pj = 0; pj < 2; pj++) {
-                    if (2 * J - 1 + pj > f.ny) continue;
-                    acc += (double)rf[u][2 * pj];
-                    if (2 * I <= f.nx) acc += (double)rf[u][2 * pj + 1];
-                }
-                const float rc = (float)acc;
-                r_c[ocs[u]] = rc;
-                s_res[t] = rc;
-                s_c[t] = vc[u];
-                s_m[t] = vm[u];
-                s_cp[t] = vp[u];
-            }
-        }
-    } else for (int t = threadIdx.x; t < n; t += MG_THREADS) {
+    for (int t = threadIdx.x; t < n; t += MG_THREADS) {
         int c = t % TC, k = t / TC + 1;
         int lX = c % TX, lY = c / TX;
         int I = I0 + lX, J = J0 + lY;
