@@ -695,6 +695,8 @@ def run_ours(args, wl):
                 extra["krylov_precision"] = args.krylov_precision
             if args.mg_precision is not None:
                 extra["mg_precision"] = args.mg_precision
+            if MG_OMEGA is not None:  # the command line's smoother damping over the cycle's
+                extra["mg_omega"] = MG_OMEGA
             opt = wi.WindOptions(**{**solver_kwargs(args.solver), **MG_CYCLES[MG_CYCLE], **extra})
             wi.set_options(opt)
             cycle = {"chosen": MG_CYCLE, **MG_CYCLES[MG_CYCLE], **extra}
