@@ -802,7 +802,8 @@ def run_ours(args, wl):
     te = e0.elapsed_time(e1)
     te = reduce_max(te, dist, f"cuda:{local}")
     e2e_value = world * e2e_steps / (te / 1000.0)
-    assert np.allclose(ou.numpy()[:1], dom.u_dqdt[:1].cpu().numpy()), "the downloaded winds are the last step's"
+    assert np.array_equal(ou.numpy()[:1], dom.u_dqdt[:1].cpu().numpy(), equal_nan=True), \
+        "the downloaded winds are the last step's"
 
     # ---- dominant kernel: per-launch CUDA-event profile of one iteration ----
     roofline = profile_roofline(lib, h, stream, args.ncu_range == "profile", dom.nx * dom.ny * dom.nz,

@@ -603,7 +603,9 @@ static int precond_kind(const hicarw_handle *h)
                                              : h->use_mg ? HICARW_PRECOND_MG : HICARW_PRECOND_JACOBI;
 }
 
-static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allow_mg = 1)
+// prec >= 0: the Krylov vector precision of this solve instead of the options'
+// (the vectors, the right-hand side and the diagonal must already be in it).
+static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allow_mg = 1, int prec_in = -1)
 {
     int rc;
     select_precond(h, allow_mg);
@@ -614,7 +616,7 @@ static int bicgstab_solve(hicarw_handle *h, int sweeps, cudaStream_t s, int allo
     }
     if (h->opt.solver == HICARW_SOLVER_FGMRES) return fgmres_solve(h, sweeps, s);
     const int solver = h->opt.solver;
-    const int prec = solve_precision(h);
+    const int prec = prec_in >= 0 ? prec_in : solve_precision(h);
     rc = ensure_vectors(h, prec);
     if (rc) return rc;
     OpCtx c = opctx(h);
@@ -979,8 +981,12 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
         if (h->opt.verbose)
             fprintf(stderr, " HICAR multigrid BiCGStab status=%d after %d iterations: falling back to Jacobi\n",
                     h->hst->status, h->hst->it);
+        // the reference's method in the reference's precision: with FP32 vectors
+        // the Jacobi-preconditioned recurrences can drift to NaN on hard systems
+        if ((rc = ensure_vectors(h, HICARW_KRYLOV_F64)) != 0) return rc;
+        prepare_system(h, s);
         if ((rc = zero_solution(h, s)) != 0) return rc;
-        if ((rc = bicgstab_solve(h, sweeps, s, 0)) != 0) return rc;
+        if ((rc = bicgstab_solve(h, sweeps, s, 0, HICARW_KRYLOV_F64)) != 0) return rc;
         fell_back = 1;
     }
     int retries = 0;
@@ -995,7 +1001,8 @@ extern "C" int hicarw_calc_iter_winds(hicarw_handle *h, const float *alpha, cons
             h->precond_n_sweeps++;
             sweeps = h->precond_n_sweeps;
             if ((rc = zero_solution(h, s)) != 0) return rc;
-            if ((rc = bicgstab_solve(h, sweeps, s)) != 0) return rc;
+            if ((rc = fell_back ? bicgstab_solve(h, sweeps, s, 0, HICARW_KRYLOV_F64) : bicgstab_solve(h, sweeps, s)) != 0)
+                return rc;
             retries++;
             res0 = h->hst->res0; resf = h->hst->rnorm; status = h->hst->status; iters = h->hst->it;
             if (h->opt.verbose)
