@@ -104,14 +104,17 @@ def test_mg_solve_matches_oracle_and_cuts_iterations(oracle_mod, case):
     assert _rel(u_m, u_j) < 1e-5
 
 
-def test_stall_falls_back_to_reference_solve(case):
+@pytest.mark.parametrize("krylov", [_capi.KRYLOV_F64, _capi.KRYLOV_F32_X64])
+def test_stall_falls_back_to_reference_solve(case, krylov):
     """A deliberately useless multigrid damping (omega = 3) makes the
     preconditioned solve stall; the stall detector stops it and the reference
-    Jacobi-preconditioned solve produces the answer (status 3 = fell back)."""
+    Jacobi-preconditioned solve, in FP64 Krylov vectors whatever the options
+    ask, produces the answer (status 3 = fell back); the next solve runs in the
+    options' precision again."""
     from hicar_b200 import wind, wind_iterative as wi
     dom, opt, div, _ = _calibrated(case)
     wi.set_options(wi.WindOptions(tol_rel=1e-6, precond=_capi.PRECOND_MG, stall_iters=10, mg_omega=3.0,
-                                  wind_solver_iterations=400))
+                                  wind_solver_iterations=400, krylov_precision=krylov))
     h = wi.handle(dom.nest_indx)
     _capi.load().hicarw_reset_solution(h, None)
     dom.set_winds(case.u, case.v, case.w)
@@ -119,6 +122,14 @@ def test_stall_falls_back_to_reference_solve(case):
     st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
     assert st["status"] == _capi.HICARW_FELL_BACK
     assert st["precond"] == _capi.PRECOND_JACOBI
+    assert st["true_res"] <= 1.01e-6 * st["b_norm"]
+    wi.set_options(wi.WindOptions(tol_rel=1e-6, precond=_capi.PRECOND_MG, stall_iters=50,
+                                  wind_solver_iterations=400, krylov_precision=krylov))
+    _capi.load().hicarw_reset_solution(h, None)
+    dom.set_winds(case.u, case.v, case.w)
+    wind.calc_divergence(div, dom, use_dqdt=True)
+    st = wi.calc_iter_winds(dom, dom.wind_alpha, div, True)
+    assert st["status"] == 0 and st["precond"] == _capi.PRECOND_MG, st
     assert st["true_res"] <= 1.01e-6 * st["b_norm"]
 
 
