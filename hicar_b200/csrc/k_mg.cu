@@ -614,33 +614,32 @@ __global__ void __launch_bounds__(pt::THREADS, 2)
 // ---------------------------------------------------------------------------
 // Post-smoothing fed by tensor copies, with the column recurrences moved off
 // the consumers' path.  The producer warp and the stage layout are those of
-// post_tma_kernel (three stages).  Eight consumer warps form x2 on the chunk's
-// window (double-buffered, so one CTA barrier per chunk) and the residuals,
+// post_tma_kernel.  Eight consumer warps read each cell's 15 neighbours of x2
+// = x1 + s P xc straight from the staged x1 and coarse rows (P is piecewise
+// constant over the 2 x 2 aggregates, so a neighbour's coarse cell is an index
+// shift; neighbours outside the interior count as zero), form the residuals,
 // release the stage as soon as their reads are done, and hand each chunk's
-// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a ring of one
-// or two slots.  The recurrence warp owns the
+// rows (residual, x2, cp, c, 1/m) to a recurrence warp through a ring of two
+// slots.  No CTA barrier is taken per chunk.  The recurrence warp owns the
 // tile's column arrays: it runs the forward recurrence chunk by chunk and, at
 // the end of a tile, the backward one, writing each cell's result as soon as
 // it is known; the consumers go on with the next tile meanwhile.  NX1: the
-// iterate x1 is zero (the finest level without pre-smoothing), so its window
-// is neither loaded nor read, and the smaller stage leaves room for a second
-// ring slot.  Same statements per cell as post_tma_kernel, so the results are
-// bit-identical.  Every wait is bounded (on timeout: *err set, the loops run
-// to their end without waiting).
+// iterate x1 is zero (the finest level without pre-smoothing), so its rows are
+// neither loaded nor read.  Three stages: a fourth (measured with x1 zero at
+// 1024x1024x64) made no difference once the per-chunk window and its barrier
+// were gone.  Same statements per cell as post_tma_kernel, so the results are
+// bit-identical.
+// Every wait is bounded (on timeout: *err set, the loops run to their end
+// without waiting).
 // ---------------------------------------------------------------------------
 namespace pt2 {
-constexpr int NR_MAX = 2;                  // ring slots at most
+constexpr int NR = 2;                      // ring slots
+constexpr int NS = 3;                      // stages
 constexpr int RW = pt::KC;                 // recurrence warp
 constexpr int PW = pt::KC + 1;             // producer warp
 constexpr int THREADS = pt::CW + 64;
 constexpr int RING_ROWS = 5;               // residual, x2, cp, c, 1/m
 constexpr int B_SLOT = RING_ROWS * pt::KC * pt::TX * 4;
-constexpr int XW = pt::up128(3 * pt::WK * pt::WX * 4) / 4; // floats per window buffer
-// Stage layout: that of post_tma_kernel, without the x1 window when the iterate
-// is zero (NX1).  Three stages either way: with the x1 window the ring has one
-// slot instead of two, so that two CTAs per SM still fit at nz = 64.
-template <bool NX1> constexpr int ns() { return 3; }
-template <bool NX1> constexpr int nr() { return NX1 ? 2 : 1; }
 template <typename CT, bool NX1> constexpr int o_xc() { return pt::o_x1<CT>() + (NX1 ? 0 : pt::up128(pt::B_X1)); }
 template <typename CT, bool NX1> constexpr int o_r() { return o_xc<CT, NX1>() + pt::up128(pt::B_XC); }
 template <typename TR, typename CT, bool NX1> constexpr int stage_bytes()
@@ -653,10 +652,44 @@ template <typename TR, typename CT, bool NX1> constexpr uint32_t tx_bytes()
 }
 template <typename TR, typename CT, bool NX1> size_t smem_bytes(int nz)
 {
-    return 128 + (size_t)ns<NX1>() * stage_bytes<TR, CT, NX1>() + (size_t)nr<NX1>() * B_SLOT +
-           (size_t)3 * nz * pt::TX * 4 + (size_t)2 * XW * 4 + 2 * (3 + NR_MAX) * 8 + 16;
+    return 128 + (size_t)NS * stage_bytes<TR, CT, NX1>() + (size_t)NR * B_SLOT + (size_t)3 * pt::TX * nz * 4 +
+           2 * (NS + NR) * 8 + 16;
 }
 }  // namespace pt2
+
+// Offsets (dk, dj, di) of the 15 coefficients A..O as compile-time functions
+// (the table c_off, for unrolled loops that need constant indices).
+__host__ __device__ constexpr int off_k(int q)
+{
+    return (q == 1 || q == 7 || q == 8 || q == 11 || q == 12) ? 1 : (q == 2 || q == 9 || q == 10 || q == 13 || q == 14) ? -1 : 0;
+}
+__host__ __device__ constexpr int off_j(int q) { return (q == 5 || q == 11 || q == 13) ? 1 : (q == 6 || q == 12 || q == 14) ? -1 : 0; }
+__host__ __device__ constexpr int off_i(int q) { return (q == 3 || q == 7 || q == 9) ? 1 : (q == 4 || q == 8 || q == 10) ? -1 : 0; }
+constexpr int kOffTable[15][3] = {{0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {0, 0, 1},  {0, 0, -1},
+                                  {0, 1, 0},  {0, -1, 0}, {1, 0, 1},  {1, 0, -1}, {-1, 0, 1},
+                                  {-1, 0, -1}, {1, 1, 0}, {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}};
+constexpr bool off_functions_match(int q = 0)
+{
+    return q == 15 || (off_k(q) == kOffTable[q][0] && off_j(q) == kOffTable[q][1] && off_i(q) == kOffTable[q][2] &&
+                       off_functions_match(q + 1));
+}
+static_assert(off_functions_match(), "off_k/off_j/off_i must restate the coefficient offsets of c_off");
+
+// post_residual with the 15 neighbour values already gathered (same terms, same order).
+__device__ __forceinline__ float post_residual_vals(double rv, const float (&cv)[15], const float (&xv)[15])
+{
+#if HICARW_MG_POST_F32
+    float y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y = fmaf(cv[q], xv[q], y);
+    return (float)(rv - (double)y);
+#else
+    double y = 0.0;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y += (double)cv[q] * (double)xv[q];
+    return (float)(rv - y);
+#endif
+}
 
 template <typename TR, typename TO, typename CT, bool NX1>
 __global__ void __launch_bounds__(pt2::THREADS, 2)
@@ -667,8 +700,7 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                      int *err)
 {
     using namespace pt;
-    constexpr int NR = pt2::nr<NX1>();
-    constexpr int NS = pt2::ns<NX1>();
+    constexpr int NR = pt2::NR, NS = pt2::NS;
     constexpr int SB = pt2::stage_bytes<TR, CT, NX1>();
     constexpr int O_COEF = 0, O_MINV = o_minv<CT>(), O_CP = o_cp<CT>(), O_X1 = o_x1<CT>(),
                   O_XC = pt2::o_xc<CT, NX1>(), O_R = pt2::o_r<CT, NX1>();
@@ -680,12 +712,11 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     float *s_d = ring + NR * SLOT; // recurrence warp: forward results, then the column solution
     float *s_cp = s_d + nz * TX;
     float *s_x2c = s_cp + nz * TX;
-    float *s_x2w = s_x2c + nz * TX; // two window buffers of pt2::XW floats
-    uint64_t *full = (uint64_t *)(s_x2w + 2 * pt2::XW);
-    uint64_t *empty = full + 3;
-    uint64_t *rfull = empty + 3;
-    uint64_t *rempty = rfull + pt2::NR_MAX;
-    int *s_skip = (int *)(rempty + pt2::NR_MAX);
+    uint64_t *full = (uint64_t *)(s_x2c + nz * TX);
+    uint64_t *empty = full + NS;
+    uint64_t *rfull = empty + NS;
+    uint64_t *rempty = rfull + NR;
+    int *s_skip = (int *)(rempty + NR);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
@@ -801,8 +832,12 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
     bool ok = true;
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1;
-        const bool col = i0 + lane <= d.nx;
+        const int bx = tile % ntx, j = tile / ntx + 1, i0 = bx * TX + 1, i = i0 + lane;
+        const bool col = i <= d.nx;
+        // which x-y neighbours lie inside the interior (x2 is zero on the lateral ring)
+        const bool im = i >= 2, ip = i + 1 <= d.nx, jm = j >= 2, jp = j + 1 <= d.ny;
+        // staged coarse row of fine row j (row j - 1 is coarse row 0, row j + 1 coarse row 1)
+        const int jc = ((j + 1) >> 1) - (j >> 1);
         for (int ch = 0; ch < nch; ch++, it++) {
             const int s = it % NS, q = it % NR;
             const unsigned char *st = base + s * SB;
@@ -810,33 +845,33 @@ __global__ void __launch_bounds__(pt2::THREADS, 2)
                 atomicExch(err, 1);
                 ok = false;
             }
-            const int k0 = 1 + ch * KC;
-            // x2 = x1 + s P xc on the chunk's window, zero outside the interior
-            float *xw = s_x2w + (it & 1) * pt2::XW;
-            const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
-            for (int e = tid; e < 3 * WK * WX; e += CW) {
-                const int cc = e % WX, kw = (e / WX) % WK, jj = e / (WX * WK);
-                const int ii = i0 - 1 + cc, kq = k0 - 1 + kw, jq = j - 1 + jj;
-                float a = 0.0f;
-                if (ii >= 1 && ii <= d.nx && jq >= 1 && jq <= d.ny && kq >= 1 && kq <= nz) {
-                    if (!NX1) a = sx1[(jj * WK + kw) * X1W + cc + 3];
-                    a += cscale * sxc[((((j + jj) >> 1) - (j >> 1)) * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
-                }
-                xw[e] = a;
-            }
-            // every consumer has finished the previous chunk (whose window buffer the next chunk reuses)
-            tc::named_sync(1, CW);
-            const int k = k0 + warp;
+            const int k = 1 + ch * KC + warp;
             float res = 0.0f, x2c = 0.0f, cpv = 0.0f, ccv = 0.0f, mv = 0.0f;
             if (k <= nz && col) {
+                const bool km = k >= 2, kp = k + 1 <= nz;
+                const float *sx1 = (const float *)(st + O_X1), *sxc = (const float *)(st + O_XC);
                 const CT *sco = (const CT *)(st + O_COEF);
-                float cv[15];
+                float cv[15], xv[15];
 #pragma unroll
                 for (int qq = 0; qq < 15; qq++) cv[qq] = coef_val(sco[(qq * KC + warp) * TX + lane]);
-                const float *xs = xw + (WK + warp + 1) * WX + lane + 1;
+                // x2 of the 15 neighbours: x1 row jj = dj + 1, level kw = warp + 1 + dk, column
+                // cc = lane + 1 + di of the staged window (i0 - 1 .. i0 + TX), zero outside the interior
+#pragma unroll
+                for (int qq = 0; qq < 15; qq++) {
+                    const int dk = off_k(qq), dj = off_j(qq), di = off_i(qq);
+                    const bool in = (di < 0 ? im : di > 0 ? ip : true) && (dj < 0 ? jm : dj > 0 ? jp : true) &&
+                                    (dk < 0 ? km : dk > 0 ? kp : true);
+                    const int kw = warp + 1 + dk, cc = lane + 1 + di, cr = dj < 0 ? 0 : dj > 0 ? 1 : jc;
+                    float a = 0.0f;
+                    if (in) {
+                        if (!NX1) a = sx1[((dj + 1) * WK + kw) * X1W + cc + 3];
+                        a += cscale * sxc[(cr * WK + kw) * XCW + ((cc + 1) >> 1) + 3];
+                    }
+                    xv[qq] = a;
+                }
                 const double rv = (double)((const TR *)(st + O_R))[warp * TX + lane];
-                res = post_residual<WK * WX, WX>(rv, cv, xs);
-                x2c = xs[0];
+                res = post_residual_vals(rv, cv, xv);
+                x2c = xv[0];
                 cpv = ((const float *)(st + O_CP))[warp * TX + lane];
                 mv = ((const float *)(st + O_MINV))[warp * TX + lane];
                 ccv = k > 1 ? cv[CC] : 0.0f;
@@ -1409,12 +1444,35 @@ static void post_t(const MgLevel &L, const CT *coef, const TR *r, const MgLevel 
     dim3 g((L.d.nx + TX - 1) / TX, (L.d.ny + TY - 1) / TY);
     size_t smem = ((size_t)4 * TX * TY * L.d.nz + (size_t)(TX + 2) * (TY + 2) * (L.d.nz + 2)) * sizeof(float);
     set_smem(post_kernel<TR, TO, TX, TY, CT>, smem);
-    launch_mg(TX == 2 && TY == 2, post_kernel<TR, TO, TX, TY, CT>, g, smem, s, L.d, coef, (const float *)L.cp,
+    launch_mg(TX * TY <= 8, post_kernel<TR, TO, TX, TY, CT>, g, smem, s, L.d, coef, (const float *)L.cp,
               (const float *)L.minv, r, (const float *)L.x1, C.d, (const float *)C.x3, out, omega, cscale, gate);
 }
 
 static std::atomic<long long> g_tma_posts{0};
 long long mg_tma_posts() { return g_tma_posts.load(); }
+
+// Column tile of the small levels' restriction and post-smoothing kernels:
+// 2 x 2 columns, or with HICARW_MG_SMALL_TILE=4 / 8 in the environment a row
+// of 4 / 8 columns (the children's fine rows then span whole 32-byte sectors).
+// The tile does not change any cell's arithmetic.  Read once.
+static int small_tile()
+{
+    static const int t = [] {
+        const char *e = getenv("HICARW_MG_SMALL_TILE");
+        return e && e[0] == '4' ? 4 : e && e[0] == '8' ? 8 : 2;
+    }();
+    return t;
+}
+
+template <typename TR, typename TO, typename CT>
+static void post_small(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
+                       float cscale, const SolveState *gate, cudaStream_t s)
+{
+    const int t = small_tile();
+    if (t == 4) post_t<TR, TO, 4, 1>(L, coef, r, C, out, omega, cscale, gate, s);
+    else if (t == 8) post_t<TR, TO, 8, 1>(L, coef, r, C, out, omega, cscale, gate, s);
+    else post_t<TR, TO, 2, 2>(L, coef, r, C, out, omega, cscale, gate, s);
+}
 
 static int sm_count()
 {
@@ -1549,10 +1607,10 @@ static void launch_post(const MgLevel &L, int level, const TR *r, const MgLevel 
     ProfScope ps_(kLevelName[1][level],
                   (sizeof(TR) + sizeof(TO) + (coefh ? 30.0 : 60.0) + (skip ? 0.0 : 4.0) + 1.0 + 8.0) * N, s);
     if (coefh) {
-        if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, coefh, r, C, out, omega, cscale, gate, s);
+        if (small_level(L.d, 32)) post_small<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, s);
         else if (!(use_tma && post_tma<TR, TO>(L, coefh, r, C, out, omega, cscale, gate, err, s, v2, x1z)))
             post_t<TR, TO, 32, 1>(L, coefh, r, C, out, omega, cscale, gate, s);
-    } else if (small_level(L.d, 32)) post_t<TR, TO, 2, 2>(L, L.coef, r, C, out, omega, cscale, gate, s);
+    } else if (small_level(L.d, 32)) post_small<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, s);
     else if (!(use_tma && post_tma<TR, TO>(L, L.coef, r, C, out, omega, cscale, gate, err, s, v2, x1z)))
         post_t<TR, TO, 32, 1>(L, L.coef, r, C, out, omega, cscale, gate, s);
     count_launch(1);
@@ -1566,7 +1624,7 @@ static void restrict_t(const MgLevel &F, const TR *r, const MgLevel &C, float *o
     size_t smem = ((size_t)4 * TX * TY * C.d.nz + (NOX ? 0 : (size_t)(2 * TX + 2) * (2 * TY + 2) * (C.d.nz + 2))) *
                   sizeof(float);
     set_smem(restrict_pre_kernel<TR, TX, TY, NOX>, smem);
-    launch_mg(TX == 2 && TY == 2, restrict_pre_kernel<TR, TX, TY, NOX>, g, smem, s, F.d, (const float *)F.coef, r,
+    launch_mg(TX * TY <= 8, restrict_pre_kernel<TR, TX, TY, NOX>, g, smem, s, F.d, (const float *)F.coef, r,
               (const float *)F.x1, C.d, (const float *)C.coef, (const float *)C.cp, (const float *)C.minv, C.r, out,
               omega, gate);
 }
@@ -1579,7 +1637,14 @@ static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C,
     const double N = (double)F.d.nx * F.d.ny * F.d.nz, Nc = (double)C.d.nx * C.d.ny * C.d.nz;
     ProfScope ps_(kLevelName[2][clevel], nox ? sizeof(TR) * N + 20.0 * Nc : (60.0 + sizeof(TR) + 4.0) * N, s);
     if (small_level(C.d, 16)) {
-        if (nox) restrict_t<TR, 2, 2, true>(F, r, C, out, omega, gate, s);
+        const int t = small_tile();
+        if (t == 4) {
+            if (nox) restrict_t<TR, 4, 1, true>(F, r, C, out, omega, gate, s);
+            else restrict_t<TR, 4, 1, false>(F, r, C, out, omega, gate, s);
+        } else if (t == 8) {
+            if (nox) restrict_t<TR, 8, 1, true>(F, r, C, out, omega, gate, s);
+            else restrict_t<TR, 8, 1, false>(F, r, C, out, omega, gate, s);
+        } else if (nox) restrict_t<TR, 2, 2, true>(F, r, C, out, omega, gate, s);
         else restrict_t<TR, 2, 2, false>(F, r, C, out, omega, gate, s);
     } else {
         if (nox) restrict_t<TR, 16, 1, true>(F, r, C, out, omega, gate, s);

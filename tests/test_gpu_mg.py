@@ -179,6 +179,36 @@ def test_tma_post_smoother_matches_register_path(shape, monkeypatch):
     assert not y[:, :, 0].any() and not y[:, :, -1].any()
 
 
+@pytest.mark.parametrize("shape", [(131, 75, 21), (128, 96, 16)])
+def test_tma_post_smoother_zero_iterate_matches_register_path(shape, monkeypatch):
+    """V(0,1) on the finest level (its iterate zero, x2 = s P xc read straight
+    from the staged coarse rows): the tensor-copy post-smoother against the
+    register-fed kernel, bit-identical, on a ragged grid (odd nx and ny, so the
+    last aggregate of a row has one column; nz not a multiple of the 8-level
+    chunk) and a regular one."""
+    from hicar_b200 import wind_iterative as wi
+    nx, ny, nz = shape
+    case = cases.build_case(nx, ny, nz, seed=17, adv_den=True, n_hills=12)
+    lib = _capi.load()
+    rng = np.random.default_rng(23)
+    x = np.zeros((ny + 2, nz + 2, nx + 2))
+    x[1:-1, 1:-1, 1:-1] = rng.standard_normal((ny, nz, nx))
+    out = {}
+    for tma in ("0", "2"):
+        dom, _, _, _ = _fresh_handle(case, monkeypatch, tma)
+        h = wi.handle(dom.nest_indx)
+        wi.set_options(wi.WindOptions(mg_skip_fine_presmooth=True, mg_omega=1.0, mg_coarse_scale=1.35))
+        n0 = lib.hicarw_mg_tma_launches()
+        y = np.empty_like(x)
+        _capi.check(lib.hicarw_apply_precond(h, x.ctypes.data, y.ctypes.data, 0, _capi.MEM_HOST, None), h)
+        out[tma] = (y, lib.hicarw_mg_tma_launches() - n0)
+    assert out["0"][1] == 0 and out["2"][1] >= 1
+    np.testing.assert_array_equal(out["2"][0], out["0"][0])
+    y = out["2"][0]
+    assert not y[0].any() and not y[-1].any() and not y[:, 0].any() and not y[:, -1].any()
+    assert not y[:, :, 0].any() and not y[:, :, -1].any()
+
+
 def test_tma_post_smoother_solve_identical(monkeypatch):
     """A whole multigrid-preconditioned solve (BiCGStab, CUDA graphs of
     iterations) with and without the tensor-copy post-smoother: the same
