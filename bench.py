@@ -65,11 +65,11 @@ REF_ITERS = {"plain512": 912, "cpu64": 78, "mid256": None, "mixed1024": 1245, "l
 # ncu capture on a smaller case (the kernel reads and writes each cell's data
 # once, so its traffic scales with the cells of the workload), keyed by the
 # kernel and whether the Krylov vectors it reads and writes are FP64:
-# mg_post_l0 with FP32 vectors, 256.79 MB per launch at 256x256x48 (3145728
+# mg_post_l0 with FP32 vectors, 255.41 MB per launch at 256x256x48 (3145728
 # cells).  None for the FP64-vector form and the register-fed smoother
 # (HICARW_MG_TMA=0), which were not captured in their current form.
 TRAFFIC_PER_CELL = {} if os.environ.get("HICARW_MG_TMA", "2")[:1] in ("0", "1") else {
-    ("mg_post_l0", False): (245.396992e6 + 11.395328e6) / (256 * 256 * 48)}
+    ("mg_post_l0", False): (245.309696e6 + 10.103296e6) / (256 * 256 * 48)}
 TOL = 1.0e-6
 MG_COARSE_SCALE = None  # --mg-coarse-scale
 MG_OMEGA = None  # --mg-omega

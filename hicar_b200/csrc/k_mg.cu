@@ -1305,8 +1305,8 @@ int mg_build(Mg &mg, const Dims &fine, const float *fine_coef, cudaStream_t s)
         cudaMemsetAsync(mg.lev[0].x1, 0, (size_t)mg.lev[0].d.npad * sizeof(float), s);
     const char *tma = getenv("HICARW_MG_TMA");
     mg.use_tma = tma && tma[0] == '0' ? 0 : tma && tma[0] == '1' ? 1 : 2;
-    if (mg.use_tma) { // device queries and the encoder lookup here, never inside a stream capture
-        sm_count();
+    sm_count(); // device queries and the encoder lookup here, never inside a stream capture
+    if (mg.use_tma) {
         smem_optin();
         smem_per_sm();
         if (!tensor_map_encoder()) mg.use_tma = 0;
@@ -1451,24 +1451,31 @@ static void post_t(const MgLevel &L, const CT *coef, const TR *r, const MgLevel 
 static std::atomic<long long> g_tma_posts{0};
 long long mg_tma_posts() { return g_tma_posts.load(); }
 
-// Column tile of the small levels' restriction and post-smoothing kernels:
-// 2 x 2 columns, or with HICARW_MG_SMALL_TILE=4 / 8 in the environment a row
-// of 4 / 8 columns (the children's fine rows then span whole 32-byte sectors).
-// The tile does not change any cell's arithmetic.  Read once.
-static int small_tile()
+// Column tile of the small levels' restriction and post-smoothing kernels
+// (level d: the level whose columns the tiles cover): a row of 8 columns where
+// that still gives two CTAs per SM, else a row of 4.  A row of 4 or 8 columns
+// reads whole 32-byte sectors of the (fine) rows; 2 x 2 tiles read half or a
+// quarter of each.  Measured at 1024x1024x64 (us per launch, 2 x 2 / 4 x 1 /
+// 8 x 1): restriction into 64 x 64 columns 50.7 / 36.3 / 32.8, into 32 x 32
+// 19.2 / 15.7 / 16.5, into 16 x 16 15.0 / 13.1 / 15.4; post-smoothing of 64 x 64
+// 29.9 / 26.4 / 22.2, of 32 x 32 13.3 / 12.8 / 13.4.  HICARW_MG_SMALL_TILE=2, 4
+// or 8 in the environment fixes the tile (for measurement; read once).  The
+// tile does not change any cell's arithmetic.
+static int small_tile(const Dims &d)
 {
-    static const int t = [] {
+    static const int forced = [] {
         const char *e = getenv("HICARW_MG_SMALL_TILE");
-        return e && e[0] == '4' ? 4 : e && e[0] == '8' ? 8 : 2;
+        return e && e[0] == '2' ? 2 : e && e[0] == '4' ? 4 : e && e[0] == '8' ? 8 : 0;
     }();
-    return t;
+    if (forced) return forced;
+    return (long long)d.nx * d.ny >= 8LL * 2 * sm_count() ? 8 : 4;
 }
 
 template <typename TR, typename TO, typename CT>
 static void post_small(const MgLevel &L, const CT *coef, const TR *r, const MgLevel &C, TO *out, float omega,
                        float cscale, const SolveState *gate, cudaStream_t s)
 {
-    const int t = small_tile();
+    const int t = small_tile(L.d);
     if (t == 4) post_t<TR, TO, 4, 1>(L, coef, r, C, out, omega, cscale, gate, s);
     else if (t == 8) post_t<TR, TO, 8, 1>(L, coef, r, C, out, omega, cscale, gate, s);
     else post_t<TR, TO, 2, 2>(L, coef, r, C, out, omega, cscale, gate, s);
@@ -1637,7 +1644,7 @@ static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C,
     const double N = (double)F.d.nx * F.d.ny * F.d.nz, Nc = (double)C.d.nx * C.d.ny * C.d.nz;
     ProfScope ps_(kLevelName[2][clevel], nox ? sizeof(TR) * N + 20.0 * Nc : (60.0 + sizeof(TR) + 4.0) * N, s);
     if (small_level(C.d, 16)) {
-        const int t = small_tile();
+        const int t = small_tile(C.d);
         if (t == 4) {
             if (nox) restrict_t<TR, 4, 1, true>(F, r, C, out, omega, gate, s);
             else restrict_t<TR, 4, 1, false>(F, r, C, out, omega, gate, s);
