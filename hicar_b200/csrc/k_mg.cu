@@ -229,7 +229,8 @@ __device__ __forceinline__ double stencil_regs(const float (&cv)[15], const floa
 // tensor-copy kernels and the fused coarse cycle's post steps, which must agree
 // bit for bit).  HICARW_MG_POST_F32 = 1 (the default): FP32 products and sums in
 // the fixed term order (fmaf), one rounding of the difference; 0: exact
-// products summed in FP64 (the restriction's sums stay FP64 either way).
+// products summed in FP64 (the restriction has its own switch,
+// HICARW_MG_RESTRICT_F32).
 // Measured at 1024x1024x64 with the benchmark's cycle: the same 10 iterations,
 // the level-0 post-smoother 1.59 -> 1.41 ms per launch.
 #ifndef HICARW_MG_POST_F32
@@ -245,6 +246,29 @@ __device__ __forceinline__ float post_residual(double rv, const float (&cv)[15],
     return (float)(rv - (double)y);
 #else
     return (float)(rv - stencil_regs<SX, SP>(cv, xs));
+#endif
+}
+
+// The restriction's fine residual r - A x1 of one cell, in FP64 for the sum
+// over the children (restrict_pre_kernel and the fused coarse cycle's
+// restriction steps, which must agree bit for bit).  HICARW_MG_RESTRICT_F32 = 1
+// (the default): FP32 products and sums in the fixed term order (fmaf), the
+// difference in FP64; 0: exact products summed in FP64.  The FP64 form converts
+// all 30 operands of a cell to FP64, whose conversion rate, not the bytes, then
+// bounds the wide levels' restrictions.
+#ifndef HICARW_MG_RESTRICT_F32
+#define HICARW_MG_RESTRICT_F32 1
+#endif
+template <int SX, int SP>
+__device__ __forceinline__ double restrict_residual(double rv, const float (&cv)[15], const float *xs)
+{
+#if HICARW_MG_RESTRICT_F32
+    float y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y = fmaf(cv[q], xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]], y);
+    return rv - (double)y;
+#else
+    return rv - stencil_regs<SX, SP>(cv, xs);
 #endif
 }
 
@@ -946,8 +970,8 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
                 r1 = (double)r_f[o1];
             }
             const float *xs0 = s_x + k * FP + (2 * lY + pj + 1) * FX + (2 * lX + 1);
-            acc += r0 - stencil_regs<FX, FP>(cv0, xs0);
-            if (has1) acc += r1 - stencil_regs<FX, FP>(cv1, xs0 + 1);
+            acc += restrict_residual<FX, FP>(r0, cv0, xs0);
+            if (has1) acc += restrict_residual<FX, FP>(r1, cv1, xs0 + 1);
         }
         float rc = (float)acc;
         r_c[oc] = rc;
@@ -1032,6 +1056,18 @@ __device__ __forceinline__ double stencil_regs_rt(const float (&cv)[15], const f
     for (int q = 0; q < 15; q++) y += (double)cv[q] * (double)xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]];
     return y;
 }
+__device__ __forceinline__ double restrict_residual_rt(double rv, const float (&cv)[15], const float *xs, int SX,
+                                                       int SP)
+{
+#if HICARW_MG_RESTRICT_F32
+    float y = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 15; q++) y = fmaf(cv[q], xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]], y);
+    return rv - (double)y;
+#else
+    return rv - stencil_regs_rt(cv, xs, SX, SP);
+#endif
+}
 __device__ __forceinline__ float post_residual_rt(double rv, const float (&cv)[15], const float *xs, int SX, int SP)
 {
 #if HICARW_MG_POST_F32
@@ -1105,8 +1141,8 @@ __device__ void fused_restrict(const CoarseStep &p, int bx, int by, float *sm)
                 r1 = (double)__ldcg(p.r_f + o1);
             }
             const float *xs0 = s_x + k * FP + (2 * lY + pj + 1) * FX + (2 * lX + 1);
-            acc += r0 - stencil_regs_rt(cv0, xs0, FX, FP);
-            if (has1) acc += r1 - stencil_regs_rt(cv1, xs0 + 1, FX, FP);
+            acc += restrict_residual_rt(r0, cv0, xs0, FX, FP);
+            if (has1) acc += restrict_residual_rt(r1, cv1, xs0 + 1, FX, FP);
         }
         const float rc = (float)acc;
         p.r_c[oc] = rc;
