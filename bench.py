@@ -702,6 +702,8 @@ def run_ours(args, wl):
             cycle = {"chosen": MG_CYCLE, **MG_CYCLES[MG_CYCLE], **extra}
         if cycle is not None:
             cycle = {k: (list(v) if isinstance(v, tuple) else v) for k, v in cycle.items()}
+    if args.spmv_levels:  # z-march depth of the operator kernels (measurement; results do not depend on it)
+        _capi.check(lib.hicarw_set_kernel_tuning(h, args.spmv_levels, -1), h)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -889,6 +891,7 @@ def run_ours(args, wl):
             "data": "synthetic",
             "config": {"workload": workload_name(args, wl),
                        "solver": args.solver, "mg_cycle_name": (cycle or {}).get("chosen"), "mg_cycle": cycle,
+                       "spmv_levels": args.spmv_levels or None,
                        "tol_rel": TOL, "fields": "f32", "krylov": krylov_desc(opt),
                        "preconditioner_precision": ("bf16 coefficients in the finest level's smoother, f32 elsewhere"
                                                     if opt.mg_precision else "f32"),
@@ -1138,6 +1141,8 @@ def main():
                     help="skip the learned+mixed FGMRES report (run only when trained parameters are shipped)")
     ap.add_argument("--parity-tol", type=float, default=1e-9,
                     help="also time the solve at this tolerance and report its accuracy (0: off)")
+    ap.add_argument("--spmv-levels", type=int, default=0,
+                    help="levels per work item of the float4 operator kernels (0: the library's default)")
     ap.add_argument("--ncu-range", default="none", choices=["none", "step", "profile"],
                     help="bracket the first timed step or the per-kernel profiling pass with "
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off)")

@@ -1012,10 +1012,12 @@ constexpr int MG_FUSE_COLS = 256;   // first fused level: nx * ny at most this (
 constexpr int MG_FUSE_STEPS = 128;  // longest recorded chain (else the per-level launches run); 128 steps
                                     // of 232 bytes keep the kernel parameter under 32 KB
 constexpr int MG_FUSE_THREADS = 512;
+constexpr int MG_FUSE_ONE_CTA = 16;  // levels of at most this many columns: one tile per step (one CTA)
 
 struct CoarseStep {
     int kind;   // 0: restriction of level f + pre-smoothing of level c; 1: post-smoothing of level f
     int tx, ty; // tile in columns: of level c (kind 0) or of level f (kind 1)
+    int cta_sync; // this step and the next are one tile each, both on CTA 0: no cluster barrier between them
     float omega, cscale;
     Dims f, c;
     const float *coef_f, *cp_f, *minv_f, *r_f, *x1_f; // level f (x1_f: the iterate restricted / corrected)
@@ -1247,8 +1249,10 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) coarse_cycle_kernel(const __g
             if (p.kind == 0) fused_restrict(p, t % ntx, t / ntx, sm);
             else fused_post(p, t % ntx, t / ntx, sm);
         }
-        __threadfence();
-        cluster_barrier();
+        // cta_sync: the next step runs on this CTA alone, after the CTA barrier that ends each tile.
+        // Otherwise the cluster barrier: its release / acquire at cluster scope makes every CTA's
+        // global writes of this step visible to the loads (through L2) of the next.
+        if (!p.cta_sync) cluster_barrier();
     }
 }
 
@@ -1714,9 +1718,12 @@ static size_t fused_step_smem(int kind, int tx, int ty, int nz)
 static bool fused_tile(int kind, const Dims &td, int nz, int cn, size_t cap, int *tx, int *ty, size_t *smem)
 {
     static const int cand[7][2] = {{1, 1}, {2, 1}, {2, 2}, {4, 2}, {4, 4}, {8, 4}, {8, 8}};
+    // levels of at most MG_FUSE_ONE_CTA columns: one tile, so that consecutive steps on them run on one
+    // CTA without cluster barriers between them
+    const long long lim = (long long)td.nx * td.ny <= MG_FUSE_ONE_CTA ? 1 : cn;
     int q = 6;
     for (int c = 0; c < 7; c++)
-        if ((long long)((td.nx + cand[c][0] - 1) / cand[c][0]) * ((td.ny + cand[c][1] - 1) / cand[c][1]) <= cn) {
+        if ((long long)((td.nx + cand[c][0] - 1) / cand[c][0]) * ((td.ny + cand[c][1] - 1) / cand[c][1]) <= lim) {
             q = c;
             break;
         }
@@ -1857,6 +1864,14 @@ static bool launch_fused(const Mg &mg, int l, const SolveState *gate, cudaStream
         const double N = (double)p.f.nx * p.f.ny * p.f.nz;
         bytes += p.kind == 0 ? (60.0 + 4.0 + 4.0) * N : (4.0 + 4.0 + 60.0 + 4.0 + 1.0 + 8.0) * N;
     }
+    // consecutive one-tile steps: CTA 0 runs both, a CTA barrier between them (the last step keeps
+    // the cluster barrier)
+    auto one_tile = [](const CoarseStep &p) {
+        const Dims &td = p.kind == 0 ? p.c : p.f;
+        return (td.nx + p.tx - 1) / p.tx == 1 && (td.ny + p.ty - 1) / p.ty == 1;
+    };
+    for (int q = 0; q < prog.n; q++)
+        prog.step[q].cta_sync = q + 1 < prog.n && one_tile(prog.step[q]) && one_tile(prog.step[q + 1]);
     ProfScope ps_(kFusedName[l], bytes, s);
     raise_smem((const void *)coarse_cycle_kernel, smem);
     cudaLaunchAttribute at[1];
