@@ -4,7 +4,7 @@ CPU oracle on identical seeded inputs.
 Bars: bit-exact where both sides run the same FP32 statements (divergence,
 analytic and probed coefficients); 1e-13 relative for the FP64 operator and
 preconditioner (FMA contraction on the device); lambda and u/v/w within 1e-5
-relative L2 (the north-star parity bar).  BiCGStab on this operator amplifies
+relative L2 (the solver parity bar).  BiCGStab on this operator amplifies
 FP64 rounding differences (summation order of the reductions, FMA): changing
 only the order of a grid reduction moves the 512x512x48 iteration count from
 719 to 894, and the 64x64x20 analytic-operator count between 147 and 171.  So

@@ -152,8 +152,9 @@ def test_headline_options_match_oracle_on_mixed_generator(oracle_mod):
 
 
 def test_plain_bicgstab_512_matches_oracle(oracle_mod):
-    """BASELINE's plain-GPU configuration: 512x512x48, 20 hills, alpha 1, density
-    advected, the reference's method and schedule against the oracle's."""
+    """The plain-GPU configuration of the solver comparison: 512x512x48, 20
+    hills, alpha 1, density advected, the reference's method and schedule
+    against the oracle's."""
     case = cases.build_case(512, 512, 48, 250.0, 20, seed=1, adv_den=True, alpha="const")
     ref = OracleSolve(oracle_mod, case, "ref")
     lam_r6, w_r6, div_r6, true_r6 = ref.solve_to(1e-6)
