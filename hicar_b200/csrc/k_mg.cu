@@ -995,229 +995,6 @@ __global__ void __launch_bounds__(MG_THREADS, 3) restrict_pre_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Restriction of a level whose iterate is zero (the finest level of a V(0,1)
-// cycle) fused with the pre-smoothing of level c, fed by tensor copies:
-// r_c = R^T r_f and out_c = w T_c^-1 r_c with the statements of
-// restrict_pre_kernel<TR, TX, TY, true> per cell, so the results are
-// bit-identical.  Persistent CTAs walk tiles of 16 coarse columns of one coarse
-// row J (the 32 fine columns of the fine rows 2J-1 and 2J) in chunks of 16
-// levels.  A producer warp streams each chunk's two fine r rows and the coarse
-// (C, 1/m, cp) rows into a four-stage ring with cp.async.bulk.tensor (no
-// multicast; x coordinates 32 bx + 8 and 16 bx + 8, multiples of 4 floats);
-// eight consumer warps sum the four children of one coarse cell each, store
-// r_c, release the stage and hand (r_c, C, 1/m, cp) to a recurrence warp
-// through a two-slot ring; the recurrence warp runs the column solves (forward
-// chunk by chunk, backward at the end of the tile) and stores out_c.  Every
-// wait is bounded (on timeout: *err set, the loops run to their end without
-// waiting).
-// ---------------------------------------------------------------------------
-namespace rn {
-constexpr int TXC = 16;               // coarse columns per tile
-constexpr int TXF = 2 * TXC;          // fine columns per tile
-constexpr int KC = 16;                // levels per chunk
-constexpr int NS = 4;                 // ring stages
-constexpr int NR = 2;                 // recurrence ring slots
-constexpr int CW = KC * TXC;          // consumer threads: one coarse cell of the chunk each
-constexpr int RW = CW / 32;           // recurrence warp
-constexpr int PW = RW + 1;            // producer warp
-constexpr int THREADS = CW + 64;
-constexpr int ROWS = 4;               // recurrence ring rows: r_c, C, 1/m, cp
-constexpr int SLOT = ROWS * KC * TXC; // floats per ring slot
-// stage: fine r rows of j = 2J-1 and 2J (KC x TXF each), then the coarse C, 1/m and cp rows (KC x TXC each)
-template <typename TR> constexpr int o_r1() { return KC * TXF * (int)sizeof(TR); }
-template <typename TR> constexpr int o_cc() { return 2 * o_r1<TR>(); }
-template <typename TR> constexpr int stage_bytes() { return o_cc<TR>() + 3 * KC * TXC * 4; }
-static_assert(o_r1<float>() % 128 == 0 && (KC * TXC * 4) % 128 == 0 && stage_bytes<float>() % 128 == 0 &&
-                  stage_bytes<double>() % 128 == 0,
-              "stage offsets must stay 128-byte aligned");
-template <typename TR> size_t smem_bytes(int nz)
-{
-    return 128 + (size_t)NS * stage_bytes<TR>() + (size_t)NR * SLOT * 4 + (size_t)2 * nz * TXC * 4 +
-           2 * (NS + NR) * 8 + 16;
-}
-}  // namespace rn
-
-template <typename TR>
-__global__ void __launch_bounds__(rn::THREADS, 4)
-    restrict_nox_tma_kernel(const __grid_constant__ CUtensorMap tm_r, const __grid_constant__ CUtensorMap tm_cc,
-                            const __grid_constant__ CUtensorMap tm_minv, const __grid_constant__ CUtensorMap tm_cp,
-                            Dims f, Dims dc, float *__restrict__ r_c, float *__restrict__ out_c, float omega, int ntx,
-                            int ntiles, const SolveState *gate, int *err)
-{
-    using namespace rn;
-    constexpr int SB = stage_bytes<TR>(), O_R1 = o_r1<TR>(), O_CC = o_cc<TR>(), O_M = O_CC + KC * TXC * 4,
-                  O_CP = O_M + KC * TXC * 4;
-    extern __shared__ unsigned char rn_smem[];
-    unsigned char *base = (unsigned char *)(((uintptr_t)rn_smem + 127) & ~(uintptr_t)127);
-    const int nz = dc.nz, nch = (nz + KC - 1) / KC;
-    float *ring = (float *)(base + NS * SB);
-    float *s_d = ring + NR * SLOT; // recurrence warp: forward results of the tile's columns
-    float *s_cp = s_d + nz * TXC;
-    uint64_t *full = (uint64_t *)(s_cp + nz * TXC);
-    uint64_t *empty = full + NS;
-    uint64_t *rfull = empty + NS;
-    uint64_t *rempty = rfull + NR;
-    int *s_skip = (int *)(rempty + NR);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        s_skip[0] = gate ? (*(volatile const int *)&gate->stop && !gate->profile) : 0;
-        for (int q = 0; q < NS; q++) {
-            tc::mbar_init(&full[q], 1);
-            tc::mbar_init(&empty[q], CW / 32); // one arrival per consumer warp
-        }
-        for (int q = 0; q < NR; q++) {
-            tc::mbar_init(&rfull[q], CW / 32);
-            tc::mbar_init(&rempty[q], 1);
-        }
-        tc::mbar_fence_init();
-    }
-    __syncthreads();
-    if (s_skip[0]) return; // the same value for every thread
-
-    if (warp == PW) { // ---- producer ----
-        if (lane != 0) return;
-        bool ok = true;
-        int it = 0;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int bx = tile % ntx, J = tile / ntx + 1;
-            const int x_f = bx * TXF + 1 + XO, x_c = bx * TXC + 1 + XO;
-            for (int ch = 0; ch < nch; ch++, it++) {
-                const int s = it % NS;
-                if (it >= NS && !tc::mbar_wait(&empty[s], ((it / NS) - 1) & 1)) {
-                    atomicExch(err, 1);
-                    ok = false;
-                    break;
-                }
-                unsigned char *st = base + s * SB;
-                const int k0 = 1 + ch * KC;
-                tc::mbar_expect_tx(&full[s], (uint32_t)SB);
-                tc::tma_load_2d(st, &tm_r, x_f, (2 * J - 1) * f.mz + k0, &full[s]);
-                tc::tma_load_2d(st + O_R1, &tm_r, x_f, 2 * J * f.mz + k0, &full[s]);
-                tc::tma_load_2d(st + O_CC, &tm_cc, x_c, J * dc.mz + k0, &full[s]);
-                tc::tma_load_2d(st + O_M, &tm_minv, x_c, J * dc.mz + k0, &full[s]);
-                tc::tma_load_2d(st + O_CP, &tm_cp, x_c, J * dc.mz + k0, &full[s]);
-            }
-        }
-        // no copy may still be in flight when the CTA ends: wait for the last stages issued
-        for (int q = it > NS ? it - NS : 0; q < it; q++)
-            if (!tc::mbar_wait(&full[q % NS], (q / NS) & 1)) atomicExch(err, 1);
-        return;
-    }
-
-    if (warp == RW) { // ---- recurrence warp: lane = coarse column ----
-        bool ok = true;
-        int it = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            const int bx = tile % ntx, J = tile / ntx + 1, I = bx * TXC + 1 + lane;
-            const bool col = lane < TXC && I <= dc.nx;
-            float dprev = 0.0f;
-            for (int ch = 0; ch < nch; ch++, it++) {
-                const int q = it % NR;
-                if (ok && !tc::mbar_wait(&rfull[q], (it / NR) & 1)) {
-                    atomicExch(err, 1);
-                    ok = false;
-                }
-                const float *rs = ring + q * SLOT;
-                const int k0 = 1 + ch * KC;
-                if (col) {
-#pragma unroll
-                    for (int h = 0; h < KC; h += THOMAS_U) {
-                        float rv[THOMAS_U], cv[THOMAS_U], mv[THOMAS_U], pv[THOMAS_U];
-#pragma unroll
-                        for (int u = 0; u < THOMAS_U; u++) {
-                            rv[u] = rs[(0 * KC + h + u) * TXC + lane];
-                            cv[u] = rs[(1 * KC + h + u) * TXC + lane];
-                            mv[u] = rs[(2 * KC + h + u) * TXC + lane];
-                            pv[u] = rs[(3 * KC + h + u) * TXC + lane];
-                        }
-#pragma unroll
-                        for (int u = 0; u < THOMAS_U; u++) {
-                            if (k0 + h + u > nz) break;
-                            dprev = (rv[u] - cv[u] * dprev) * mv[u];
-                            const int t = (k0 + h + u - 1) * TXC + lane;
-                            s_d[t] = dprev;
-                            s_cp[t] = pv[u];
-                        }
-                    }
-                }
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&rempty[q]);
-            }
-            if (col) { // backward recurrence, each level's result stored as soon as it is known
-                float y = 0.0f;
-                int k = nz - 1;
-                for (; k + 1 >= THOMAS_U; k -= THOMAS_U) {
-                    float rv[THOMAS_U], pv[THOMAS_U];
-#pragma unroll
-                    for (int u = 0; u < THOMAS_U; u++) {
-                        rv[u] = s_d[(k - u) * TXC + lane];
-                        pv[u] = s_cp[(k - u) * TXC + lane];
-                    }
-#pragma unroll
-                    for (int u = 0; u < THOMAS_U; u++) {
-                        y = rv[u] - pv[u] * y;
-                        out_c[kidx(dc, I, k - u + 1, J)] = omega * y;
-                    }
-                }
-                for (; k >= 0; k--) {
-                    y = s_d[k * TXC + lane] - s_cp[k * TXC + lane] * y;
-                    out_c[kidx(dc, I, k + 1, J)] = omega * y;
-                }
-            }
-        }
-        return;
-    }
-
-    // ---- consumers: thread = (level kk, coarse column c) of the chunk ----
-    bool ok = true;
-    int it = 0;
-    const int kk = tid / TXC, c = tid % TXC;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int bx = tile % ntx, J = tile / ntx + 1, I = bx * TXC + 1 + c;
-        const bool col = I <= dc.nx, has1 = 2 * I <= f.nx, row1 = 2 * J <= f.ny;
-        for (int ch = 0; ch < nch; ch++, it++) {
-            const int s = it % NS, q = it % NR;
-            const unsigned char *st = base + s * SB;
-            if (ok && !tc::mbar_wait(&full[s], (it / NS) & 1)) {
-                atomicExch(err, 1);
-                ok = false;
-            }
-            const int k = 1 + ch * KC + kk;
-            float rc = 0.0f, vc = 0.0f, vm = 0.0f, vp = 0.0f;
-            if (k <= nz && col) {
-                // the children (2I-1, j) and (2I, j) of rows j = 2J-1 and 2J, in restrict_pre_kernel's order
-                const TR *r0 = (const TR *)st + kk * TXF + 2 * c, *r1 = (const TR *)(st + O_R1) + kk * TXF + 2 * c;
-                double acc = 0.0;
-                acc += (double)r0[0];
-                if (has1) acc += (double)r0[1];
-                if (row1) {
-                    acc += (double)r1[0];
-                    if (has1) acc += (double)r1[1];
-                }
-                rc = (float)acc;
-                vc = k > 1 ? ((const float *)(st + O_CC))[kk * TXC + c] : 0.0f;
-                vm = ((const float *)(st + O_M))[kk * TXC + c];
-                vp = ((const float *)(st + O_CP))[kk * TXC + c];
-                r_c[kidx(dc, I, k, J)] = rc;
-            }
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&empty[s]); // this warp's reads of the stage are done
-            if (ok && it >= NR && !tc::mbar_wait(&rempty[q], ((it / NR) - 1) & 1)) {
-                atomicExch(err, 1);
-                ok = false;
-            }
-            float *rs = ring + q * SLOT;
-            rs[(0 * KC + kk) * TXC + c] = rc;
-            rs[(1 * KC + kk) * TXC + c] = vc;
-            rs[(2 * KC + kk) * TXC + c] = vm;
-            rs[(3 * KC + kk) * TXC + c] = vp;
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&rfull[q]);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Fused coarse cycle.  Below a level of at most MG_FUSE_COLS columns the
 // cycle is a chain of restriction and post-smoothing steps on tiny levels
 // whose time is set by launch and memory latency (10-15 us per launch for a
@@ -1235,12 +1012,10 @@ constexpr int MG_FUSE_COLS = 256;   // first fused level: nx * ny at most this (
 constexpr int MG_FUSE_STEPS = 128;  // longest recorded chain (else the per-level launches run); 128 steps
                                     // of 232 bytes keep the kernel parameter under 32 KB
 constexpr int MG_FUSE_THREADS = 512;
-constexpr int MG_FUSE_ONE_CTA = 16;  // levels of at most this many columns: one tile per step (one CTA)
 
 struct CoarseStep {
     int kind;   // 0: restriction of level f + pre-smoothing of level c; 1: post-smoothing of level f
     int tx, ty; // tile in columns: of level c (kind 0) or of level f (kind 1)
-    int cta_sync; // this step and the next are one tile each, both on CTA 0: no cluster barrier between them
     float omega, cscale;
     Dims f, c;
     const float *coef_f, *cp_f, *minv_f, *r_f, *x1_f; // level f (x1_f: the iterate restricted / corrected)
@@ -1472,10 +1247,8 @@ __global__ void __launch_bounds__(MG_FUSE_THREADS) coarse_cycle_kernel(const __g
             if (p.kind == 0) fused_restrict(p, t % ntx, t / ntx, sm);
             else fused_post(p, t % ntx, t / ntx, sm);
         }
-        // cta_sync: the next step runs on this CTA alone, after the CTA barrier that ends each tile.
-        // Otherwise the cluster barrier: its release / acquire at cluster scope makes every CTA's
-        // global writes of this step visible to the loads (through L2) of the next.
-        if (!p.cta_sync) cluster_barrier();
+        __threadfence();
+        cluster_barrier();
     }
 }
 
@@ -1899,42 +1672,10 @@ static void restrict_t(const MgLevel &F, const TR *r, const MgLevel &C, float *o
               omega, gate);
 }
 
-// restrict_nox_tma_kernel on a wide level; false (nothing launched) when its
-// conditions do not hold: shared memory for nz levels, 16-byte aligned arrays
-// and row pitches.  Box x coordinates 32 bx + 8 (fine) and 16 bx + 8 (coarse).
-template <typename TR>
-static bool restrict_nox_tma(const MgLevel &F, const TR *r, const MgLevel &C, float *out, float omega,
-                             const SolveState *gate, int *err, cudaStream_t s)
-{
-    using namespace rn;
-    const Dims &f = F.d, &dc = C.d;
-    const size_t smem = smem_bytes<TR>(dc.nz);
-    if (!err || smem > (size_t)smem_optin() || dc.mz != f.mz) return false;
-    const cuuint64_t dfr[2] = {(cuuint64_t)f.P, (cuuint64_t)f.my * f.mz}, sfr[1] = {(cuuint64_t)f.P * sizeof(TR)};
-    const cuuint64_t dcr[2] = {(cuuint64_t)dc.P, (cuuint64_t)dc.my * dc.mz}, scr[1] = {(cuuint64_t)dc.P * 4};
-    const cuuint32_t bf[2] = {TXF, KC}, bc[2] = {TXC, KC};
-    const CUtensorMapDataType f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const CUtensorMapDataType fr = sizeof(TR) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    CUtensorMap m[4];
-    if (!make_map(&m[0], fr, 2, r, dfr, sfr, bf) || !make_map(&m[1], f32, 2, C.coef + (size_t)CC * dc.npad, dcr, scr, bc) ||
-        !make_map(&m[2], f32, 2, C.minv, dcr, scr, bc) || !make_map(&m[3], f32, 2, C.cp, dcr, scr, bc))
-        return false;
-    const int ntx = (dc.nx + TXC - 1) / TXC, ntiles = ntx * dc.ny;
-    const int grid = std::min(ntiles, 4 * sm_count());
-    int *e = gate ? const_cast<int *>(&gate->err) : err;
-    raise_smem((const void *)restrict_nox_tma_kernel<TR>, smem);
-    restrict_nox_tma_kernel<TR><<<grid, THREADS, smem, s>>>(m[0], m[1], m[2], m[3], f, dc, C.r, out, omega, ntx,
-                                                            ntiles, gate, e);
-    g_tma_posts++;
-    return true;
-}
-
-// nox: level f was not pre-smoothed (its x1 is zero): restrict r_f alone (on a
-// wide level with tensor copies when use_tma allows).
+// nox: level f was not pre-smoothed (its x1 is zero): restrict r_f alone.
 template <typename TR>
 static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C, int clevel, float *out, float omega,
-                                const SolveState *gate, cudaStream_t s, bool nox = false, int use_tma = 0,
-                                int *err = nullptr)
+                                const SolveState *gate, cudaStream_t s, bool nox = false)
 {
     const double N = (double)F.d.nx * F.d.ny * F.d.nz, Nc = (double)C.d.nx * C.d.ny * C.d.nz;
     ProfScope ps_(kLevelName[2][clevel], nox ? sizeof(TR) * N + 20.0 * Nc : (60.0 + sizeof(TR) + 4.0) * N, s);
@@ -1948,10 +1689,10 @@ static void launch_restrict_pre(const MgLevel &F, const TR *r, const MgLevel &C,
             else restrict_t<TR, 8, 1, false>(F, r, C, out, omega, gate, s);
         } else if (nox) restrict_t<TR, 2, 2, true>(F, r, C, out, omega, gate, s);
         else restrict_t<TR, 2, 2, false>(F, r, C, out, omega, gate, s);
-    } else if (nox) {
-        if (!(use_tma && restrict_nox_tma<TR>(F, r, C, out, omega, gate, err, s)))
-            restrict_t<TR, 16, 1, true>(F, r, C, out, omega, gate, s);
-    } else restrict_t<TR, 16, 1, false>(F, r, C, out, omega, gate, s);
+    } else {
+        if (nox) restrict_t<TR, 16, 1, true>(F, r, C, out, omega, gate, s);
+        else restrict_t<TR, 16, 1, false>(F, r, C, out, omega, gate, s);
+    }
     count_launch(1);
 }
 
@@ -1973,12 +1714,9 @@ static size_t fused_step_smem(int kind, int tx, int ty, int nz)
 static bool fused_tile(int kind, const Dims &td, int nz, int cn, size_t cap, int *tx, int *ty, size_t *smem)
 {
     static const int cand[7][2] = {{1, 1}, {2, 1}, {2, 2}, {4, 2}, {4, 4}, {8, 4}, {8, 8}};
-    // levels of at most MG_FUSE_ONE_CTA columns: one tile, so that consecutive steps on them run on one
-    // CTA without cluster barriers between them
-    const long long lim = (long long)td.nx * td.ny <= MG_FUSE_ONE_CTA ? 1 : cn;
     int q = 6;
     for (int c = 0; c < 7; c++)
-        if ((long long)((td.nx + cand[c][0] - 1) / cand[c][0]) * ((td.ny + cand[c][1] - 1) / cand[c][1]) <= lim) {
+        if ((long long)((td.nx + cand[c][0] - 1) / cand[c][0]) * ((td.ny + cand[c][1] - 1) / cand[c][1]) <= cn) {
             q = c;
             break;
         }
@@ -2119,14 +1857,6 @@ static bool launch_fused(const Mg &mg, int l, const SolveState *gate, cudaStream
         const double N = (double)p.f.nx * p.f.ny * p.f.nz;
         bytes += p.kind == 0 ? (60.0 + 4.0 + 4.0) * N : (4.0 + 4.0 + 60.0 + 4.0 + 1.0 + 8.0) * N;
     }
-    // consecutive one-tile steps: CTA 0 runs both, a CTA barrier between them (the last step keeps
-    // the cluster barrier)
-    auto one_tile = [](const CoarseStep &p) {
-        const Dims &td = p.kind == 0 ? p.c : p.f;
-        return (td.nx + p.tx - 1) / p.tx == 1 && (td.ny + p.ty - 1) / p.ty == 1;
-    };
-    for (int q = 0; q < prog.n; q++)
-        prog.step[q].cta_sync = q + 1 < prog.n && one_tile(prog.step[q]) && one_tile(prog.step[q + 1]);
     ProfScope ps_(kFusedName[l], bytes, s);
     raise_smem((const void *)coarse_cycle_kernel, smem);
     cudaLaunchAttribute at[1];
@@ -2183,7 +1913,7 @@ void mg_apply(const Mg &mg, const V *in, V *out, const SolveState *gate, cudaStr
     const MgLevel &F = mg.lev[0];
     const MgLevel &C = mg.lev[1];
     const bool last = L == 2;
-    launch_restrict_pre<V>(F, in, C, 1, last ? C.x3 : C.x1, last ? 1.0f : w, gate, s, !mg.pre0, mg.use_tma, mg.err);
+    launch_restrict_pre<V>(F, in, C, 1, last ? C.x3 : C.x1, last ? 1.0f : w, gate, s, !mg.pre0);
     MgLevel Cr = C;
     Cr.x3 = const_cast<float *>(coarse_cycle(mg, 1, gate, s));
     launch_post<V, V>(F, 0, in, Cr, out, w, mg.cscale, gate, mg.use_tma, mg.err, s,

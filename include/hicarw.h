@@ -352,12 +352,10 @@ int hicarw_batch_autotune(hicarw_batch *b, const hicarw_batch_item *items, int a
 
 /* Number of kernels this library has launched since load (graph nodes included). */
 long long hicarw_kernel_launches(void);
-/* Multigrid launches enqueued through the tensor-copy (TMA) kernels since load
- * (a launch captured into a CUDA graph counts once): the wide levels'
- * post-smoothers and, with V(0,1) on the finest level, the restriction of its
- * right-hand side to a wide level 1.  They run unless the environment sets
- * HICARW_MG_TMA=0 as the V-cycle is built (then the register-fed kernels run;
- * both give bit-identical results). */
+/* Multigrid post-smoother launches enqueued through the tensor-copy (TMA) kernel
+ * since load (a launch captured into a CUDA graph counts once).  Wide levels use
+ * it unless the environment sets HICARW_MG_TMA=0 as the V-cycle is built (then
+ * the register-fed kernel runs; both give bit-identical results). */
 long long hicarw_mg_tma_launches(void);
 
 /* ---- the steps either side of the solve in update_winds (wind.F90) ----

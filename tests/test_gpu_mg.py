@@ -185,9 +185,8 @@ def test_tma_post_smoother_zero_iterate_matches_register_path(shape, monkeypatch
     from the staged coarse rows): the tensor-copy post-smoother against the
     register-fed kernel, bit-identical, on ragged grids (odd nx and ny, so the
     last aggregate of a row has one column; nz not a multiple of the 8-level
-    chunk) and a regular one.  On 161 x 131 level 1 is wide enough (81 x 66
-    columns) for the tensor-copy restriction of the finest level's right-hand
-    side, compared here with the per-tile kernel (HICARW_MG_TMA=0)."""
+    chunk) and a regular one; on 161 x 131 level 1 (81 x 66 columns) takes
+    the wide restriction tiles."""
     from hicar_b200 import wind_iterative as wi
     nx, ny, nz = shape
     case = cases.build_case(nx, ny, nz, seed=17, adv_den=True, n_hills=12)
