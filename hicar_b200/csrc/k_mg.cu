@@ -182,23 +182,6 @@ __device__ __forceinline__ void thomas_column(float *s_res, const float *s_c, co
 constexpr int MG_THREADS = 256;
 constexpr int MG_BATCH = 8; // independent loads in flight per thread in the staging loops
 
-// 15-point stencil sum at padded offset o: coefficients walked with a pointer
-// increment of npad through the read-only path, neighbours read from a staged
-// shared-memory window.
-template <int SX, int SP>
-__device__ __forceinline__ double stencil_smem(const float *__restrict__ coef, long long npad, long long o,
-                                               const float *xs)
-{
-    const float *cq = coef + o;
-    double y = 0.0;
-#pragma unroll
-    for (int q = 0; q < 15; q++) {
-        y += (double)__ldg(cq) * (double)xs[c_off[q][0] * SP + c_off[q][1] * SX + c_off[q][2]];
-        cq += npad;
-    }
-    return y;
-}
-
 // The 15 coefficients of a row, loaded together (independent loads in flight);
 // FP32 or BF16 storage (the finest level's smoother coefficients in BF16).
 __device__ __forceinline__ float coef_val(float v) { return v; }
