@@ -20,11 +20,6 @@ namespace hw {
 // ---------------------------------------------------------------------------
 // calc_divergence, one thread per cell (i, k, j).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float rho_at(const float *rho, const Dims &d, int i, int k, int j, int adv_den)
-{
-    return adv_den ? rho[cidx(d, i, k, j)] : 1.0f;
-}
-
 __device__ __forceinline__ float u_met(const Dims &d, const Metrics &m, const float *u, const float *rho, int i, int k,
                                        int j, int adv_den, int use_dqdt)
 {

@@ -64,8 +64,6 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // Make generic-proxy shared-memory writes visible to the async proxy (tensor core).
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 // 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32(w%4)..+31).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 {
