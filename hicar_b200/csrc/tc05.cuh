@@ -63,7 +63,6 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t base, uint32_t ncols)
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Make generic-proxy shared-memory writes visible to the async proxy (tensor core).
 // 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32(w%4)..+31).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 {
